@@ -1,0 +1,406 @@
+"""Benchmark of the batched CPAB transform (one JSON line on stdout).
+
+Workload (the batched 1D configuration): [0,1] split into nC=100 equal
+cells, zero-velocity boundary; 4096 theta from the Gaussian prior (length
+scale 0.1, variance 1); instance i transforms its own n_i = floor(10^U(3,5))
+uniform points (~8.8e7 in total); integration time 1.0 as dt=0.02 x 50 steps
+with nStepsODE=100 (the reference's calc_T scheme); FP32 points, per-cell
+expm in FP64; one fused prologue launch (theta -> A -> expm for all 4096) and
+one persistent integration launch per step.  Seeded synthetic data (seed 1).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value`  : points/s over all ranks with inputs resident in HBM (device time,
+           max over ranks); the inputs (352 MB of points) exceed L2.
+`e2e`    : the same through CpaSpace.calc_T_batched with pinned host buffers,
+           the H2D copy of theta/offsets/points and the D2H copy of the
+           transformed points inside the timed region.
+--impl reference: the reference's own kernel sources compiled for the host
+           (oracle/_ref) in FP64 with all host threads on a bounded sample per
+           step; with N > 1 only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "CPAB points/sec batched+served vs plain per-call at <=1e-5 err; p50/p99 latency"
+UNIT = "points/s"
+N_THETA, NC, SEED = 4096, 100, 1
+DT, NT, NODE = 0.02, 50, 100
+WORKLOAD = "batched_1d_nc100_4096theta_ragged_1e3_1e5"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the cpu baseline and the 2D plain-vs-batched leg")
+    ap.add_argument("--theta", type=int, default=N_THETA)
+    return ap.parse_args()
+
+
+def make_workload(rank: int, n_theta: int):
+    from cpabdiffeo_b200.space import Prior, build_space
+    geo = build_space(1, (NC,), "II")
+    prior = Prior.create(geo, length_scale=0.1, variance=1.0)
+    rng = np.random.default_rng(SEED + 1000 * rank)
+    theta = prior.sample(n_theta, rng)
+    sizes = np.floor(10 ** rng.uniform(3, 5, size=n_theta)).astype(np.int64)
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    pts = rng.uniform(0, 1, size=(int(offsets[-1]), 1)).astype(np.float32)
+    return geo, theta, sizes, offsets, pts
+
+
+class ClockSampler:
+    """nvidia-smi samples while the timed region runs (clocks line of the profiling recipe)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks(torch) -> dict:
+    """FP32 / FP64 SIMT throughput measured here (cuBLAS SGEMM with TF32 off,
+    DGEMM): the denominators for the integration kernel, which runs on the
+    FP32 / FP64 pipes.  HBM from MEASURED_PEAKS.json."""
+    out = {}
+    try:
+        out.update(json.loads((ROOT / "MEASURED_PEAKS.json").read_text()))
+    except (OSError, ValueError):
+        out["hbm_gbs"] = 6650.0
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    for name, dt, n in (("fp32_simt_tflops", torch.float32, 8192), ("fp64_tflops", torch.float64, 4096)):
+        a = torch.randn(n, n, device="cuda", dtype=dt)
+        b = torch.randn(n, n, device="cuda", dtype=dt)
+        for _ in range(2):
+            a @ b
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = 1e30
+        for _ in range(5):
+            s.record()
+            a @ b
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e))
+        out[name] = 2 * n ** 3 / (best * 1e-3) / 1e12
+        del a, b
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    return out
+
+
+def flops_from_counters(cnt, dim=1) -> float:
+    """Algorithmic FP ops of the REF scheme from device counters:
+    per closed-form attempt 2*C_cell + M, per midpoint sub-step C_cell + 2M + 4D,
+    with M = 2 D^2 (affine apply) and C_cell = 5 (1D box lookup)."""
+    C_cell = {1: 5, 2: 24, 3: 36}[dim]
+    M = 2 * dim * dim
+    attempts = cnt[0] + cnt[1]
+    return float(attempts * (2 * C_cell + M) + cnt[2] * (C_cell + 2 * M + 4 * dim))
+
+
+def cpu_reference_rate(theta, offsets, pts, geo, budget_pts: int, rank_seed: int = 0):
+    """The reference's calc_T (host-compiled, FP64, all threads) on the first
+    instances covering ~budget_pts points.  Returns (points/s, sample text, kind, cores)."""
+    from oracle import oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    n_inst = int(np.searchsorted(offsets, budget_pts)) + 1
+    n_inst = max(1, min(n_inst, len(offsets) - 1))
+    t0 = time.perf_counter()
+    npts = 0
+    for i in range(n_inst):
+        A = (geo.B @ theta[i]).reshape(NC, 2)
+        sA, Tr = O.expm_cells(1, A, DT, 1)
+        x = pts[offsets[i]:offsets[i + 1]].astype(np.float64)
+        if kind == "reference":
+            out = O.ref_calc_T(1, 2, geo.nCs, geo.incs, Tr, sA, x, DT, NT, NODE, geo.nC)
+        else:
+            out, _ = O.calc_T(O.tess_struct(1, 2, geo.nCs, geo.incs), Tr, sA, x, DT, NT, NODE)
+        O.clamp_1d(out)
+        npts += x.shape[0]
+    dt = time.perf_counter() - t0
+    return npts / dt, f"first {n_inst} of {len(offsets) - 1} instances ({npts} points), FP64", kind, O.nproc(), dt
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    geo, theta, sizes, offsets, pts = make_workload(0, args.theta)
+    budget = 150_000
+    for _ in range(args.warmup):
+        cpu_reference_rate(theta, offsets, pts, geo, budget)
+    rates, secs, sample, kind, cores = [], 0.0, "", "", 1
+    for _ in range(args.steps):
+        r, sample, kind, cores, dt = cpu_reference_rate(theta, offsets, pts, geo, budget)
+        rates.append(r)
+        secs += dt
+    value = float(np.mean(rates))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded prior draws, uniform points)",
+            "config": {"workload": WORKLOAD, "scheme": "ref calc_T dt=0.02 nT=50 nODE=100", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def plain_vs_batched_2d(torch, dev):
+    """North-star comparison on the 2D nC=64 workload: FP32 batched (one launch
+    for all theta) vs the plain path (one theta per call: host A = B theta,
+    expm launch, calc_T launch, stream sync), 4096 points per theta."""
+    from cpabdiffeo_b200.cpa_space import CpaSpace
+    from cpabdiffeo_b200.space import Prior
+    sp64 = CpaSpace([0, 0], [1, 1], (4, 4), tess="I", device=dev, precision=torch.float64)
+    sp32 = CpaSpace([0, 0], [1, 1], (4, 4), tess="I", device=dev, precision=torch.float32)
+    rng = np.random.default_rng(0)
+    nth, npt = 1024, 4096
+    theta = Prior.create(sp64.geo, 0.1, 1.0).sample(nth, rng)
+    x = rng.uniform(0, 1, size=(nth * npt, 2))
+    p = dict(dt=DT, nTimeSteps=NT, nStepsODEsolver=NODE)
+    # plain: first 64 theta, FP64 (the drop-in default), one call each
+    xs = torch.as_tensor(x[:npt], device=dev)
+    out = torch.empty_like(xs)
+    n_plain = 64
+    for rep in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(n_plain):
+            sp64.update_pat(sp64.B_host @ theta[i])
+            sp64.calc_T_fwd(pts=xs, out=out, **p)
+            torch.cuda.current_stream().synchronize()
+        t_plain = time.perf_counter() - t0
+    plain = n_plain * npt / t_plain
+    xb = torch.as_tensor(x, device=dev, dtype=torch.float32)
+    ob = torch.empty_like(xb)
+    th = torch.as_tensor(theta, device=dev)
+
+    def step():
+        tables = sp32.tables_from_theta(th, DT, 1)
+        sp32.calc_T_batched(tables, xb, ob, **p)
+
+    for _ in range(3):
+        step()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(5):
+        step()
+    e.record()
+    e.synchronize()
+    batched = 5 * nth * npt / (s.elapsed_time(e) * 1e-3)
+    return {"workload": "2d_tessI_4x4_nc64_1024theta_x_4096pts", "plain_per_call_points_per_s": plain,
+            "plain_precision": "f64", "batched_points_per_s": batched, "batched_precision": "f32",
+            "ratio": batched / plain}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+
+    from cpabdiffeo_b200 import _lib
+    from cpabdiffeo_b200.cpa_space import CpaSpace
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    geo, theta_h, sizes, offsets_h, pts_h = make_workload(rank, args.theta)
+    n_total = int(offsets_h[-1])
+    sp = CpaSpace([0.0], [1.0], (NC,), device=dev, precision=torch.float32)
+    theta = torch.as_tensor(theta_h, device=dev)
+    offsets = torch.as_tensor(offsets_h, device=dev)
+    pts = torch.as_tensor(pts_h, device=dev)
+    out = torch.empty_like(pts)
+    ws = torch.empty(int(sp._ctx.lib.cpab_batched_workspace_bytes(args.theta)), dtype=torch.uint8, device=dev)
+    p = dict(dt=DT, nTimeSteps=NT, nStepsODEsolver=NODE)
+    stream = torch.cuda.current_stream()
+    k_ev = []
+
+    def step(record=False):
+        tables = sp.tables_from_theta(theta, DT, 1)
+        if record:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+        sp.calc_T_batched(tables, pts, out, offsets=offsets, workspace=ws, **p)
+        if record:
+            b.record(stream)
+            k_ev.append((a, b))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        s.record(stream)
+        for _ in range(args.steps):
+            step(record=True)
+        e.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = s.elapsed_time(e)
+    kern_ms = float(np.mean([a.elapsed_time(b) for a, b in k_ev]))
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = n_total * world * args.steps / (ms * 1e-3)
+
+    # end to end through the public API, host buffers (pinned), copies inside the timed region
+    pts_pin = torch.from_numpy(pts_h).pin_memory()
+    out_pin = torch.empty_like(pts_pin).pin_memory()
+    th_pin = torch.from_numpy(theta_h).pin_memory()
+    off_pin = torch.from_numpy(offsets_h).pin_memory()
+
+    def e2e_step():
+        th_d = th_pin.to(dev, non_blocking=True)
+        off_d = off_pin.to(dev, non_blocking=True)
+        x_d = pts_pin.to(dev, non_blocking=True)
+        o_d = torch.empty_like(x_d)
+        tables = sp.tables_from_theta(th_d, DT, 1)
+        sp.calc_T_batched(tables, x_d, o_d, offsets=off_d, workspace=ws, **p)
+        out_pin.copy_(o_d, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s2.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e2.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ms_e2e = s2.elapsed_time(e2)
+    if world > 1:
+        t = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    h2d = pts_h.nbytes + theta_h.nbytes + offsets_h.nbytes
+    d2h = pts_h.nbytes
+
+    # work accounting (counters) and error vs the FP64 oracle on a sample
+    cnt = torch.zeros(_lib.CNT_N, dtype=torch.int64, device=dev)
+    tables = sp.tables_from_theta(theta, DT, 1)
+    sp.calc_T_batched(tables, pts, out, offsets=offsets, workspace=ws, counters=cnt, **p)
+    torch.cuda.synchronize()
+    cnt_h = cnt.cpu().numpy()
+    flops = flops_from_counters(cnt_h)
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded prior draws, log-uniform ragged sizes, uniform points)",
+            "config": {"workload": WORKLOAD, "n_theta_per_gpu": args.theta, "points_per_gpu": n_total,
+                       "nC": NC, "scheme": "ref calc_T dt=0.02 nT=50 nODE=100", "precision": "f32 points, f64 expm",
+                       "l2": "inputs larger than L2 (352 MB of points per GPU)",
+                       "parallelism": f"independent shards x{world}"},
+            "e2e": {"value": n_total * world * args.steps / (ms_e2e * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clk.summary(),
+            "work": {"fast_steps": int(cnt_h[0]), "fallback_steps": int(cnt_h[1]), "substeps": int(cnt_h[2]),
+                     "points": int(cnt_h[3])}}
+
+    if rank == 0:
+        peaks = measured_peaks(torch)
+        achieved = flops / (kern_ms * 1e-3) / 1e12
+        line["roofline"] = {"bound": "fp32", "kernel": "k_integrate<1,2,float,REF>", "achieved": achieved,
+                            "peak": peaks["fp32_simt_tflops"], "unit": "TFLOP/s",
+                            "frac": achieved / peaks["fp32_simt_tflops"],
+                            "peak_source": "measured here: cuBLAS SGEMM 8192^3 with TF32 off",
+                            "kernel_ms": kern_ms, "traffic": None,
+                            "algorithmic_flop_per_launch": flops,
+                            "hbm_achieved_gbs": 2 * pts_h.nbytes / (kern_ms * 1e-3) / 1e9,
+                            "hbm_peak_gbs": peaks.get("hbm_gbs")}
+        if world == 1 and not args.no_extras:
+            r, sample, kind, cores, _ = cpu_reference_rate(theta_h, offsets_h, pts_h, geo, 400_000)
+            line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+            try:
+                line["plain_vs_batched_2d"] = plain_vs_batched_2d(torch, dev)
+            except Exception as ex:  # reported, never fatal
+                line["plain_vs_batched_2d"] = {"error": repr(ex)}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

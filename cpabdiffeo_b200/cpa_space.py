@@ -1,0 +1,331 @@
+"""CpaSpace: the reference's transform API on torch CUDA tensors.
+
+Mirrors cpab/cpaNd/_CpaSpace.py (method names, argument order, the sign
+convention of calc_T_fwd / calc_T_inv, the caller-allocated `out`, the
+1D boundary clamp) with torch.Tensor in place of CpuGpuArray.  Every call
+runs hand-written sm_100a kernels from libcpab_b200.so through the C ABI;
+there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from .space import TESS_I, TESS_II, Prior, SpaceGeometry, build_space
+
+_DT = {torch.float64: _lib.CPAB_F64, torch.float32: _lib.CPAB_F32}
+
+
+def default_params_flow_int(dim: int) -> dict:
+    """Defaults of cpab/cpa{1,2,3}d/calcs/_default_params_flow_int.py."""
+    if dim == 1:
+        return dict(dt=0.01, nTimeSteps=100, nStepsODEsolver=10)
+    return dict(dt=0.0001, nTimeSteps=10, nStepsODEsolver=10)
+
+
+class _Ctx:
+    """Owns one cpab_ctx handle."""
+
+    def __init__(self, geo: SpaceGeometry):
+        lib = _lib.load()
+        h = C.c_void_p()
+        nCs = (C.c_int * 3)(*(list(geo.nCs) + [1] * (3 - geo.dim)))
+        incs = (C.c_double * 3)(*(list(geo.incs) + [1.0] * (3 - geo.dim)))
+        _lib.check(lib.cpab_ctx_create(C.byref(h), geo.dim, geo.tess_code, nCs, incs))
+        self.h = h
+        self.lib = lib
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.lib.cpab_ctx_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def check(self, status: int) -> None:
+        _lib.check(status, self.h)
+
+
+class PAT:
+    """Piecewise-affine transformation of one space: the per-cell matrices
+    (Avees, device float64 [D]) plus cached signed matrices and exponentials
+    (cpab/cpaNd/_PAT.py:48-59)."""
+
+    def __init__(self, space: "CpaSpace", Avees: torch.Tensor | None = None):
+        self.space = space
+        self.nC = space.nC
+        self.Avees = torch.zeros(space.D, dtype=torch.float64, device=space.device)
+        self._cache: dict = {}
+        if Avees is not None:
+            self.update(Avees)
+
+    def update(self, Avees) -> None:
+        a = torch.as_tensor(Avees, dtype=torch.float64, device=self.space.device).reshape(-1)
+        if a.numel() != self.space.D:
+            raise ValueError(a.shape, self.space.D)
+        self.Avees.copy_(a)
+        self._cache.clear()
+
+    @property
+    def As(self) -> torch.Tensor:
+        return self.Avees.view(self.nC, self.space.dim, self.space.dim + 1)
+
+    def signed_tables(self, dt: float, sign: int, stream=None):
+        key = (float(dt), int(sign))
+        hit = self._cache.get(key)
+        if hit is None:
+            sA = torch.empty(self.space.D, dtype=torch.float64, device=self.space.device)
+            Tr = torch.empty_like(sA)
+            ctx = self.space._ctx
+            ctx.check(ctx.lib.cpab_expm(ctx.h, _lib.ptr(self.Avees), 1, float(dt), int(sign),
+                                        _lib.ptr(sA), _lib.ptr(Tr), _lib.stream_ptr(stream)))
+            hit = (sA, Tr)
+            self._cache[key] = hit
+        return hit
+
+
+class CpaSpace:
+    """A CPA space over [XMINS, XMAXS] (XMINS must be 0, as in the reference,
+    cpab/cpa2d/calcs/_CpaCalcs.py:38-39)."""
+
+    def __init__(self, XMINS: Sequence[float], XMAXS: Sequence[float], nCs: Sequence[int],
+                 zero_v_across_bdry: Sequence[bool] | None = None, vol_preserve: bool = False,
+                 tess: str = TESS_II, valid_outside: bool | None = None, device=None,
+                 precision: torch.dtype = torch.float64):
+        dim = len(nCs)
+        if vol_preserve:
+            raise NotImplementedError("volume-preserving spaces are outside the built path")
+        if tess == TESS_I and dim == 2 and valid_outside:
+            raise NotImplementedError("valid_outside=True is outside the built path")
+        if any(float(x) != 0.0 for x in XMINS):
+            raise ValueError("XMINS must be 0 (the cell lookup assumes it)")
+        if precision not in _DT:
+            raise TypeError(precision)
+        self.dim = self.dim_domain = self.dim_range = dim
+        self.tess = tess
+        self.XMINS = np.asarray(XMINS, dtype=np.float64)
+        self.XMAXS = np.asarray(XMAXS, dtype=np.float64)
+        self.zero_v_across_bdry = tuple(zero_v_across_bdry if zero_v_across_bdry is not None else (True,) * dim)
+        self.geo = build_space(dim, tuple(int(n) for n in nCs), tess, tuple(self.XMINS), tuple(self.XMAXS),
+                               self.zero_v_across_bdry)
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.precision = precision
+        self.nCs = self.geo.nCs
+        self.nC = self.geo.nC
+        self.incs = self.geo.incs
+        self.nHomoCoo = dim + 1
+        self.lengthAvee = self.geo.lengthAvee
+        self.Ashape = (dim, dim + 1)
+        self.D = self.geo.D
+        self.d = self.geo.d
+        self.B_host = self.geo.B
+        self.B = torch.as_tensor(np.ascontiguousarray(self.geo.B), device=self.device)
+        self._ctx = _Ctx(self.geo)
+        if dim == 1 and self.zero_v_across_bdry[0]:
+            # threshold_krnl clamp of cpab/cpaNd/_CpaSpace.py:655-664
+            self._ctx.check(self._ctx.lib.cpab_set_clamp(self._ctx.h, 1, float(self.XMINS[0]),
+                                                         float(self.XMAXS[0])))
+        self.pat = PAT(self)
+        self.Avees = self.pat.Avees
+
+    # ------------------------------------------------------------------ parameters
+    def get_zeros_theta(self) -> np.ndarray:
+        return np.zeros(self.d)
+
+    def get_zeros_PA(self) -> np.ndarray:
+        return np.zeros(self.D)
+
+    def theta2Avees(self, theta, Avees=None):
+        """A = B theta (cpab/cpaNd/_CpaSpace.py:366-376)."""
+        th = torch.as_tensor(theta, dtype=torch.float64, device=self.device)
+        res = self.B @ th
+        if Avees is None:
+            self.Avees.copy_(res)
+            return self.Avees
+        Avees.copy_(res) if isinstance(Avees, torch.Tensor) else np.copyto(Avees, res.cpu().numpy())
+        return Avees
+
+    def Avees2theta(self, Avees=None):
+        a = self.Avees if Avees is None else torch.as_tensor(Avees, dtype=torch.float64, device=self.device)
+        return self.B.T @ a
+
+    def Avees2As(self, Avees=None):
+        a = self.Avees if Avees is None else Avees
+        return a.reshape(self.nC, *self.Ashape)
+
+    def update_pat(self, Avees=None) -> None:
+        self.pat.update(self.Avees if Avees is None else Avees)
+
+    def create_prior(self, length_scale: float = 0.1, variance: float = 1.0, **kw) -> Prior:
+        return Prior.create(self.geo, length_scale=length_scale, variance=variance, **kw)
+
+    # ------------------------------------------------------------------ checks
+    def _check_pts(self, pts: torch.Tensor, name: str = "pts") -> None:
+        if not isinstance(pts, torch.Tensor):
+            raise TypeError(type(pts))
+        if pts.device.type != "cuda":
+            raise ValueError(f"{name} must be a CUDA tensor")
+        if pts.ndim != 2 or pts.shape[1] != self.dim:
+            raise ValueError(f"{name}.shape = {tuple(pts.shape)}, expected (nPts, {self.dim})")
+        if not pts.is_contiguous():
+            raise ValueError(f"{name} must be C-contiguous")
+        if pts.dtype not in _DT:
+            raise ValueError(f"{name}.dtype = {pts.dtype}")
+
+    def _flow(self, params: dict) -> tuple[float, int, int]:
+        p = default_params_flow_int(self.dim)
+        p.update(params)
+        return float(p["dt"]), int(p["nTimeSteps"]), int(p["nStepsODEsolver"])
+
+    # ------------------------------------------------------------------ transforms
+    def calc_cell_idx(self, pts: torch.Tensor, cell_idx: torch.Tensor) -> torch.Tensor:
+        """cpab/cpaNd/_CpaSpace.py:567 -> _CpaCalcs.calc_cell_idx (:59-88)."""
+        self._check_pts(pts)
+        if pts.dtype != torch.float64:
+            raise ValueError(pts.dtype)
+        if cell_idx.dtype != torch.int32 or cell_idx.numel() != pts.shape[0] or not cell_idx.is_contiguous():
+            raise ValueError("cell_idx must be a contiguous int32 tensor with one entry per point")
+        c = self._ctx
+        c.check(c.lib.cpab_calc_cell_idx(c.h, _lib.ptr(pts), _lib.ptr(cell_idx), pts.shape[0], _lib.stream_ptr()))
+        return cell_idx
+
+    def calc_v(self, pat: PAT | None = None, pts: torch.Tensor | None = None, out: torch.Tensor | None = None,
+               do_checks: bool = True) -> torch.Tensor:
+        """v(x) = A_c [x; 1] (cpab/cpaNd/_CpaSpace.py:573-587)."""
+        pat = pat or self.pat
+        if pts is None:
+            raise ValueError("Pts cannot be None")
+        if out is None:
+            raise ValueError("out Can't have None")
+        self._check_pts(pts)
+        self._check_pts(out, "out")
+        if pts.dtype != torch.float64 or out.dtype != torch.float64 or out.shape != pts.shape:
+            raise ValueError("calc_v works on float64 points with out.shape == pts.shape")
+        c = self._ctx
+        c.check(c.lib.cpab_calc_v(c.h, _lib.ptr(pat.Avees), _lib.ptr(pts), _lib.ptr(out), pts.shape[0],
+                                  _lib.stream_ptr()))
+        return out
+
+    def _calc_T(self, pat, pts, mysign, out, scheme=_lib.SCHEME_REF, counters=None, **params_flow_int):
+        pat = pat or self.pat
+        if pts is None:
+            raise ValueError
+        if out is None:
+            raise ValueError("You must pass the OUT argument")
+        self._check_pts(pts)
+        self._check_pts(out, "out")
+        if out.dtype != pts.dtype or out.shape != pts.shape:
+            raise ValueError("out must match pts in shape and dtype")
+        if pts.data_ptr() == out.data_ptr():
+            raise ValueError("pts and out cannot point to the same memory")
+        dt, nT, nODE = self._flow(params_flow_int)
+        sA, Tr = pat.signed_tables(dt, mysign)
+        c = self._ctx
+        c.check(c.lib.cpab_calc_T(c.h, _lib.ptr(sA), _lib.ptr(Tr), _lib.ptr(pts), _lib.ptr(out), pts.shape[0],
+                                  _DT[pts.dtype], scheme, dt, nT, nODE, _lib.ptr(counters), _lib.stream_ptr()))
+        return out
+
+    def calc_T_fwd(self, pat=None, pts=None, do_checks=True, out=None, **params_flow_int):
+        """T(x) (cpab/cpaNd/_CpaSpace.py:626-627)."""
+        return self._calc_T(pat, pts, 1, out, **params_flow_int)
+
+    def calc_T_inv(self, pat=None, pts=None, do_checks=True, out=None, **params_flow_int):
+        """T^{-1}(x): the flow of -v (cpab/cpaNd/_CpaSpace.py:629-630)."""
+        return self._calc_T(pat, pts, -1, out, **params_flow_int)
+
+    def calc_T_simple(self, pat=None, pts=None, mysign=1, do_checks=True, out=None, **params_flow_int):
+        """Midpoint-only integration (cpab/cpaNd/_CpaSpace.py:590-624)."""
+        return self._calc_T(pat, pts, mysign, out, scheme=_lib.SCHEME_SIMPLE, **params_flow_int)
+
+    def calc_T_exact(self, pat=None, pts=None, mysign=1, out=None, **params_flow_int):
+        """Closed-form 1D flow across cells for time dt*nTimeSteps
+        (cpab/cpa1d/calcs/ClosedFormInt.py:64-165)."""
+        if self.dim != 1:
+            raise NotImplementedError("the exact scheme is built for 1D spaces")
+        return self._calc_T(pat, pts, mysign, out, scheme=_lib.SCHEME_EXACT, **params_flow_int)
+
+    def calc_trajectory(self, pat=None, pts=None, mysign=1, **params_flow_int) -> torch.Tensor:
+        """[(1+nTimeSteps), nPts, dim] positions, row 0 = pts
+        (cpab/cpaNd/_CpaSpace.py:688-703, _CpaCalcs.py:795-871)."""
+        pat = pat or self.pat
+        if pts is None:
+            raise ValueError("pts cannot be None")
+        self._check_pts(pts)
+        if pts.dtype != torch.float64:
+            raise ValueError(pts.dtype)
+        dt, nT, nODE = self._flow(params_flow_int)
+        sA, Tr = pat.signed_tables(dt, mysign)
+        traj = torch.empty((nT + 1, pts.shape[0], self.dim), dtype=torch.float64, device=self.device)
+        c = self._ctx
+        c.check(c.lib.cpab_calc_trajectory(c.h, _lib.ptr(sA), _lib.ptr(Tr), _lib.ptr(pts), _lib.ptr(traj),
+                                           pts.shape[0], dt, nT, nODE, _lib.stream_ptr()))
+        return traj
+
+    # ------------------------------------------------------------------ batches
+    def tables_from_theta(self, theta: torch.Tensor, dt: float, mysign: int = 1, A_out: torch.Tensor | None = None):
+        """signed A and Trel for a batch theta [N, d] (one fused launch)."""
+        th = theta.to(device=self.device, dtype=torch.float64).contiguous()
+        if th.ndim != 2 or th.shape[1] != self.d:
+            raise ValueError(th.shape)
+        N = th.shape[0]
+        sA = torch.empty((N, self.D), dtype=torch.float64, device=self.device)
+        Tr = torch.empty_like(sA)
+        c = self._ctx
+        c.check(c.lib.cpab_theta_to_trels(c.h, _lib.ptr(self.B), self.d, _lib.ptr(th), N, float(dt), int(mysign),
+                                          _lib.ptr(A_out), _lib.ptr(sA), _lib.ptr(Tr), _lib.stream_ptr()))
+        return sA, Tr
+
+    def tables_from_A(self, A: torch.Tensor, dt: float, mysign: int = 1):
+        """signed A and Trel for a batch of matrices A [N, D]."""
+        A = A.to(device=self.device, dtype=torch.float64).contiguous()
+        N = A.shape[0]
+        sA = torch.empty((N, self.D), dtype=torch.float64, device=self.device)
+        Tr = torch.empty_like(sA)
+        c = self._ctx
+        c.check(c.lib.cpab_expm(c.h, _lib.ptr(A), N, float(dt), int(mysign), _lib.ptr(sA), _lib.ptr(Tr),
+                                _lib.stream_ptr()))
+        return sA, Tr
+
+    def calc_T_batched(self, tables, pts: torch.Tensor, out: torch.Tensor, offsets: torch.Tensor | None = None,
+                       scheme: int = _lib.SCHEME_REF, counters: torch.Tensor | None = None,
+                       workspace: torch.Tensor | None = None, **params_flow_int) -> torch.Tensor:
+        """N transforms in one persistent launch.  tables = (signedA, Trels)
+        [N, D] from tables_from_theta / tables_from_A with the same dt and sign.
+        Points of instance i: pts[offsets[i]:offsets[i+1]] (offsets: CUDA
+        int64 [N+1]) or, without offsets, N equal slices of pts."""
+        sA, Tr = tables
+        N = sA.shape[0]
+        self._check_pts(pts)
+        self._check_pts(out, "out")
+        if out.dtype != pts.dtype or out.shape != pts.shape:
+            raise ValueError("out must match pts")
+        dt, nT, nODE = self._flow(params_flow_int)
+        c = self._ctx
+        if offsets is None:
+            if pts.shape[0] % max(N, 1):
+                raise ValueError("without offsets, nPts must be a multiple of N")
+            n_uniform, ws, ws_bytes = pts.shape[0] // max(N, 1), None, 0
+        else:
+            if offsets.dtype != torch.int64 or offsets.numel() != N + 1 or offsets.device.type != "cuda":
+                raise ValueError("offsets must be a CUDA int64 tensor of N+1 entries")
+            n_uniform = 0
+            ws_bytes = int(c.lib.cpab_batched_workspace_bytes(N))
+            if workspace is None or workspace.numel() * workspace.element_size() < ws_bytes:
+                workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=self.device)
+            ws = workspace
+        c.check(c.lib.cpab_calc_T_batched(c.h, _lib.ptr(sA), _lib.ptr(Tr), _lib.ptr(pts), _lib.ptr(out), N,
+                                          _lib.ptr(offsets), n_uniform, _lib.ptr(ws), ws_bytes, _DT[pts.dtype],
+                                          scheme, dt, nT, nODE, _lib.ptr(counters), _lib.stream_ptr()))
+        return out
+
+    def set_launch(self, block: int = 0, ctas_per_sm: int = 0, tile_pts: int = 0) -> None:
+        c = self._ctx
+        c.check(c.lib.cpab_set_launch(c.h, block, ctas_per_sm, tile_pts))
+
+    def __repr__(self) -> str:
+        return self.geo.subspace_string

@@ -1,0 +1,309 @@
+// cpab_capi.cu -- the extern "C" boundary declared in include/cpab_b200.h:
+// argument validation, status codes and error strings, launch dispatch.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <new>
+
+#include "../../include/cpab_b200.h"
+#include "cpab_internal.h"
+#include "cpab_launch.h"
+
+using namespace cpab;
+
+struct cpab_ctx {
+    Tess t;
+    int nCs[3];
+    int clamp = 0;
+    double clamp_lo = 0, clamp_hi = 0;
+    LaunchCfg cfg;
+    char err[512] = {0};
+};
+
+static thread_local char g_thread_err[512];
+
+static int fail(cpab_ctx *ctx, int status, const char *fmt, ...)
+{
+    char *buf = ctx ? ctx->err : g_thread_err;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, 512, fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+static int cuda_status(cpab_ctx *ctx, cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return CPAB_OK;
+    return fail(ctx, CPAB_CUDA_ERROR, "%s: %s", what, cudaGetErrorString(e));
+}
+
+static inline int cell_len(const cpab_ctx *c) { return c->t.dim * (c->t.dim + 1); }
+
+static bool overlaps(const void *a, size_t na, const void *b, size_t nb)
+{
+    const char *pa = (const char *)a, *pb = (const char *)b;
+    return pa < pb + nb && pb < pa + na;
+}
+
+static size_t tables_smem(const cpab_ctx *c, int prec)
+{
+    return (size_t)2 * c->t.nC * cell_len(c) * (prec == CPAB_F64 ? 8 : 4);
+}
+
+static int max_smem_optin()
+{
+    static int v = 0;
+    if (v == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || v <= 0)
+            v = 227 * 1024;
+    }
+    return v;
+}
+
+extern "C" {
+
+int cpab_ctx_create(cpab_ctx **out, int dim, int tess, const int *nCs, const double *incs)
+{
+    if (!out) return fail(nullptr, CPAB_BAD_ARG, "out is NULL");
+    *out = nullptr;
+    if (dim < 1 || dim > 3) return fail(nullptr, CPAB_BAD_ARG, "dim must be 1, 2 or 3 (got %d)", dim);
+    if (tess != 1 && tess != 2) return fail(nullptr, CPAB_BAD_ARG, "tess must be 1 (I) or 2 (II) (got %d)", tess);
+    if (dim == 1 && tess == 1)
+        return fail(nullptr, CPAB_BAD_ARG, "1D spaces have type II tessellations only (cpab/cpaNd/_CpaSpace.py:77)");
+    if (!nCs || !incs) return fail(nullptr, CPAB_BAD_ARG, "nCs/incs is NULL");
+    cpab_ctx *c = new (std::nothrow) cpab_ctx();
+    if (!c) return fail(nullptr, CPAB_NO_MEMORY, "out of host memory");
+    if (!make_tess(dim, tess, nCs, incs, c->t)) {
+        delete c;
+        return fail(nullptr, CPAB_BAD_ARG, "invalid nCs/incs (need nCs >= 1, finite incs > 0, at most 2^20 cells)");
+    }
+    for (int k = 0; k < 3; ++k) c->nCs[k] = k < dim ? nCs[k] : 1;
+    *out = c;
+    return CPAB_OK;
+}
+
+int cpab_ctx_destroy(cpab_ctx *ctx)
+{
+    delete ctx;
+    return CPAB_OK;
+}
+
+const char *cpab_last_error_string(const cpab_ctx *ctx) { return ctx ? ctx->err : g_thread_err; }
+
+int cpab_ctx_num_cells(const cpab_ctx *ctx) { return ctx ? ctx->t.nC : -1; }
+int cpab_ctx_cell_len(const cpab_ctx *ctx) { return ctx ? cell_len(ctx) : -1; }
+
+int cpab_set_clamp(cpab_ctx *ctx, int enable, double lo, double hi)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (enable && !(lo <= hi)) return fail(ctx, CPAB_BAD_ARG, "clamp needs lo <= hi");
+    ctx->clamp = enable ? 1 : 0;
+    ctx->clamp_lo = lo;
+    ctx->clamp_hi = hi;
+    return CPAB_OK;
+}
+
+int cpab_set_launch(cpab_ctx *ctx, int block, int ctas_per_sm, int tile_pts)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (block && (block < 32 || block > 256 || block % 32))
+        return fail(ctx, CPAB_BAD_ARG, "block must be a multiple of 32 in [32, 256] (got %d)", block);
+    if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(ctx, CPAB_BAD_ARG, "ctas_per_sm out of range");
+    if (tile_pts < 0) return fail(ctx, CPAB_BAD_ARG, "tile_pts < 0");
+    if (block) ctx->cfg.block = block;
+    if (ctas_per_sm) ctx->cfg.ctas_per_sm = ctas_per_sm;
+    if (tile_pts) ctx->cfg.tile_pts = tile_pts;
+    return CPAB_OK;
+}
+
+int cpab_expm(cpab_ctx *ctx, const double *A, int N, double dt, int sign, double *signedA, double *Trels,
+              void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (N < 0) return fail(ctx, CPAB_BAD_SHAPE, "N < 0");
+    if (N == 0) return CPAB_OK;
+    if (!A || !Trels) return fail(ctx, CPAB_BAD_ARG, "A/Trels is NULL");
+    if (sign != 1 && sign != -1) return fail(ctx, CPAB_BAD_ARG, "sign must be +1 or -1");
+    if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
+    return cuda_status(ctx, launch_expm(ctx->t.dim, A, signedA, Trels, (int64_t)N * ctx->t.nC, dt, (double)sign,
+                                        (cudaStream_t)stream),
+                       "expm launch");
+}
+
+int cpab_theta_to_trels(cpab_ctx *ctx, const double *B, int d, const double *theta, int N, double dt, int sign,
+                        double *A, double *signedA, double *Trels, void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (N < 0 || d < 1) return fail(ctx, CPAB_BAD_SHAPE, "need N >= 0 and d >= 1");
+    if (N == 0) return CPAB_OK;
+    if (!B || !theta || !Trels) return fail(ctx, CPAB_BAD_ARG, "B/theta/Trels is NULL");
+    if (sign != 1 && sign != -1) return fail(ctx, CPAB_BAD_ARG, "sign must be +1 or -1");
+    if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
+    return cuda_status(ctx, launch_theta_to_trels(ctx->t.dim, B, theta, d, ctx->t.nC, N, dt, (double)sign, A,
+                                                  signedA, Trels, (cudaStream_t)stream),
+                       "theta_to_trels launch");
+}
+
+int cpab_calc_cell_idx(cpab_ctx *ctx, const double *pts, int32_t *cell_idx, int64_t nPts, void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (nPts < 0) return fail(ctx, CPAB_BAD_SHAPE, "nPts < 0");
+    if (nPts == 0) return CPAB_OK;
+    if (!pts || !cell_idx) return fail(ctx, CPAB_BAD_ARG, "pts/cell_idx is NULL");
+    return cuda_status(ctx, launch_cell_idx(ctx->t, pts, cell_idx, nPts, (cudaStream_t)stream), "cell_idx launch");
+}
+
+int cpab_calc_v(cpab_ctx *ctx, const double *A, const double *pts, double *vel, int64_t nPts, void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (nPts < 0) return fail(ctx, CPAB_BAD_SHAPE, "nPts < 0");
+    if (nPts == 0) return CPAB_OK;
+    if (!A || !pts || !vel) return fail(ctx, CPAB_BAD_ARG, "A/pts/vel is NULL");
+    size_t bytes = (size_t)nPts * ctx->t.dim * 8;
+    if (overlaps(pts, bytes, vel, bytes)) return fail(ctx, CPAB_ALIAS, "pts and vel overlap");
+    if ((size_t)ctx->t.nC * cell_len(ctx) * 8 > (size_t)max_smem_optin())
+        return fail(ctx, CPAB_UNSUPPORTED, "cell table does not fit in shared memory");
+    return cuda_status(ctx, launch_calc_v(ctx->t, A, pts, vel, nPts, (cudaStream_t)stream), "calc_v launch");
+}
+
+static int check_integrate(cpab_ctx *ctx, const double *signedA, const double *Trels, const void *pts, void *out,
+                           int64_t nPts, int precision, int scheme, double dt, int nTimeSteps, int nStepsODE)
+{
+    if (precision != CPAB_F64 && precision != CPAB_F32)
+        return fail(ctx, CPAB_BAD_DTYPE, "precision must be CPAB_F64 or CPAB_F32");
+    if (scheme != CPAB_SCHEME_REF && scheme != CPAB_SCHEME_SIMPLE && scheme != CPAB_SCHEME_EXACT)
+        return fail(ctx, CPAB_BAD_ARG, "unknown scheme %d", scheme);
+    if (scheme == CPAB_SCHEME_EXACT && ctx->t.dim != 1)
+        return fail(ctx, CPAB_UNSUPPORTED, "the exact scheme is built for 1D spaces");
+    if (nPts < 0) return fail(ctx, CPAB_BAD_SHAPE, "nPts < 0");
+    if (nTimeSteps < 1) return fail(ctx, CPAB_BAD_ARG, "nTimeSteps must be >= 1");
+    if (nStepsODE < 1) return fail(ctx, CPAB_BAD_ARG, "nStepsODE must be >= 1");
+    if ((long long)nTimeSteps * nStepsODE > 0x7fffffffLL)
+        return fail(ctx, CPAB_BAD_ARG, "nTimeSteps * nStepsODE overflows");
+    if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
+    if (!signedA) return fail(ctx, CPAB_BAD_ARG, "signedA is NULL");
+    if (scheme == CPAB_SCHEME_REF && !Trels) return fail(ctx, CPAB_BAD_ARG, "Trels is NULL");
+    if (nPts > 0 && (!pts || !out)) return fail(ctx, CPAB_BAD_ARG, "pts/out is NULL");
+    size_t bytes = (size_t)nPts * ctx->t.dim * (precision == CPAB_F64 ? 8 : 4);
+    if (nPts > 0 && overlaps(pts, bytes, out, bytes))
+        return fail(ctx, CPAB_ALIAS, "pts and out cannot point to the same memory (_CpaCalcs.py:388)");
+    if (tables_smem(ctx, precision) > (size_t)max_smem_optin())
+        return fail(ctx, CPAB_UNSUPPORTED, "cell tables (%zu bytes) exceed shared memory", tables_smem(ctx, precision));
+    return CPAB_OK;
+}
+
+static IntegrateArgs make_args(cpab_ctx *ctx, const double *signedA, const double *Trels, const void *pts,
+                               void *out, double dt, int nTimeSteps, int nStepsODE, uint64_t *counters)
+{
+    IntegrateArgs a;
+    memset(&a, 0, sizeof(a));
+    a.t = ctx->t;
+    a.A = signedA;
+    a.T = Trels;
+    a.pts_in = pts;
+    a.pts_out = out;
+    a.dt = dt;
+    a.nTimeSteps = nTimeSteps;
+    a.nStepsODE = nStepsODE;
+    a.clamp = ctx->clamp;
+    a.clamp_lo = ctx->clamp_lo;
+    a.clamp_hi = ctx->clamp_hi;
+    a.counters = reinterpret_cast<unsigned long long *>(counters);
+    a.max_crossings = 4 * ctx->t.nC + 8;
+    return a;
+}
+
+static int run_integrate(cpab_ctx *ctx, IntegrateArgs &a, int precision, int scheme, int64_t uniform_tiles_total,
+                         cudaStream_t s)
+{
+    LaunchCfg cfg = ctx->cfg;
+    int persistent = num_sms() * cfg.ctas_per_sm;
+    if (uniform_tiles_total > 0 && uniform_tiles_total < persistent) cfg.grid = (int)uniform_tiles_total;
+    cudaError_t e = (scheme == CPAB_SCHEME_EXACT) ? launch_integrate_exact1d(a, precision, cfg, s)
+                                                   : launch_integrate(a, precision, scheme, cfg, s);
+    return cuda_status(ctx, e, "integrate launch");
+}
+
+int cpab_calc_T(cpab_ctx *ctx, const double *signedA, const double *Trels, const void *pts, void *out,
+                int64_t nPts, int precision, int scheme, double dt, int nTimeSteps, int nStepsODE,
+                uint64_t *counters, void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    int st = check_integrate(ctx, signedA, Trels, pts, out, nPts, precision, scheme, dt, nTimeSteps, nStepsODE);
+    if (st != CPAB_OK) return st;
+    if (nPts == 0) return CPAB_OK;
+    IntegrateArgs a = make_args(ctx, signedA, Trels, pts, out, dt, nTimeSteps, nStepsODE, counters);
+    a.batch.N = 1;
+    a.batch.n_uniform = nPts;
+    a.batch.offsets = nullptr;
+    a.batch.tile_prefix = nullptr;
+    a.batch.tile_pts = ctx->cfg.tile_pts;
+    a.batch.tiles_per_inst = (nPts + a.batch.tile_pts - 1) / a.batch.tile_pts;
+    return run_integrate(ctx, a, precision, scheme, a.batch.tiles_per_inst, (cudaStream_t)stream);
+}
+
+size_t cpab_batched_workspace_bytes(int N)
+{
+    if (N < 0) return 0;
+    size_t b = (size_t)(N + 1) * sizeof(int64_t);
+    return (b + 255) & ~(size_t)255;
+}
+
+int cpab_calc_T_batched(cpab_ctx *ctx, const double *signedA, const double *Trels, const void *pts, void *out,
+                        int N, const int64_t *offsets, int64_t n_uniform, void *workspace, size_t workspace_bytes,
+                        int precision, int scheme, double dt, int nTimeSteps, int nStepsODE, uint64_t *counters,
+                        void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (N < 0) return fail(ctx, CPAB_BAD_SHAPE, "N < 0");
+    if (N == 0) return CPAB_OK;
+    if (!offsets && n_uniform < 0) return fail(ctx, CPAB_BAD_SHAPE, "n_uniform < 0");
+    // Overlap is checked on the uniform extent only; ragged extents live on the device.
+    int64_t nchk = offsets ? 0 : (int64_t)N * n_uniform;
+    int st = check_integrate(ctx, signedA, Trels, pts, out, nchk, precision, scheme, dt, nTimeSteps, nStepsODE);
+    if (st != CPAB_OK) return st;
+    if (offsets && (!pts || !out)) return fail(ctx, CPAB_BAD_ARG, "pts/out is NULL");
+    if (offsets && pts == out) return fail(ctx, CPAB_ALIAS, "pts and out are the same buffer");
+    cudaStream_t s = (cudaStream_t)stream;
+    IntegrateArgs a = make_args(ctx, signedA, Trels, pts, out, dt, nTimeSteps, nStepsODE, counters);
+    a.batch.N = N;
+    a.batch.tile_pts = ctx->cfg.tile_pts;
+    int64_t uniform_tiles = 0;
+    if (offsets) {
+        if (!workspace || workspace_bytes < cpab_batched_workspace_bytes(N))
+            return fail(ctx, CPAB_NO_MEMORY, "workspace of %zu bytes needed", cpab_batched_workspace_bytes(N));
+        int64_t *prefix = static_cast<int64_t *>(workspace);
+        cudaError_t e = launch_tile_prefix(offsets, prefix, N, a.batch.tile_pts, s);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "tile_prefix launch");
+        a.batch.offsets = offsets;
+        a.batch.tile_prefix = prefix;
+    } else {
+        if (n_uniform == 0) return CPAB_OK;
+        a.batch.n_uniform = n_uniform;
+        a.batch.tiles_per_inst = (n_uniform + a.batch.tile_pts - 1) / a.batch.tile_pts;
+        uniform_tiles = a.batch.tiles_per_inst * N;
+    }
+    return run_integrate(ctx, a, precision, scheme, uniform_tiles, s);
+}
+
+int cpab_calc_trajectory(cpab_ctx *ctx, const double *signedA, const double *Trels, const double *pts, double *traj,
+                         int64_t nPts, double dt, int nTimeSteps, int nStepsODE, void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (!Trels) return fail(ctx, CPAB_BAD_ARG, "Trels is NULL");
+    int st = check_integrate(ctx, signedA, Trels, pts, traj, 0, CPAB_F64, CPAB_SCHEME_REF, dt, nTimeSteps, nStepsODE);
+    if (st != CPAB_OK) return st;
+    if (nPts < 0) return fail(ctx, CPAB_BAD_SHAPE, "nPts < 0");
+    if (nPts == 0) return CPAB_OK;
+    if (!pts || !traj) return fail(ctx, CPAB_BAD_ARG, "pts/traj is NULL");
+    size_t in_bytes = (size_t)nPts * ctx->t.dim * 8, out_bytes = in_bytes * (size_t)(nTimeSteps + 1);
+    if (overlaps(pts, in_bytes, traj, out_bytes)) return fail(ctx, CPAB_ALIAS, "pts and traj overlap");
+    IntegrateArgs a = make_args(ctx, signedA, Trels, pts, traj, dt, nTimeSteps, nStepsODE, nullptr);
+    return cuda_status(ctx, launch_trajectory(a, nPts, (cudaStream_t)stream), "trajectory launch");
+}
+
+}  // extern "C"

@@ -1,0 +1,182 @@
+// cpab_exact1d.cu -- closed-form 1D integration across cell boundaries.
+//
+// Restates cpab/cpa1d/calcs/ClosedFormInt.py (calc_phi :64-165,
+// find_crossing_time :193-256, calc_affine_phi :171-192) for a batch of
+// instances on the unit interval with nC equal cells and zero-velocity
+// boundary.  Inside cell c the velocity is v(x) = a x + b, so
+//     x(t) = e^{a t} x + b (e^{a t} - 1) / a        (x + t b if a == 0)
+// and the time to reach the cell's exit endpoint xe is
+//     t = log((xe + b/a) / (x + b/a)) / a           ((xe - x)/b if a ~ 0).
+// A point walks from cell to cell, consuming the remaining time, until it
+// stops inside a cell or the velocity cannot carry it over the next
+// endpoint (sign change / zero velocity), with the reference's 1e-16 and
+// 1e-12 nudges at endpoints and its np.allclose(., 0) tests (|.| <= 1e-8).
+//
+// Arithmetic is double in both precisions: the FP32 mode only stores the
+// points in float (hitting times and exponentials stay in double).
+#include <math_constants.h>
+
+#include "cpab_device.cuh"
+#include "cpab_launch.h"
+
+namespace cpab {
+
+struct Exact1D {
+    const double *A;  // [nC, 2] signed (a, b) of the current instance, shared memory
+    int nC;
+    double step;      // 1/nC: vertices x_k = k*step, x_nC = 1 (np.linspace(0,1,nC+1))
+};
+
+__device__ __forceinline__ double vert(const Exact1D &e, int k) { return k == e.nC ? 1.0 : (double)k * e.step; }
+
+__device__ __forceinline__ int cf_cell(const Exact1D &e, double x)
+{
+    double f = floor(x * (double)e.nC);
+    f = fmin(fmax(f, 0.0), (double)(e.nC - 1));
+    return (int)f;
+}
+
+__device__ __forceinline__ double cf_v(const Exact1D &e, double x, int c)
+{
+    if (!(0 <= x && x <= 1)) return 0.0;
+    return e.A[2 * c] * x + e.A[2 * c + 1];
+}
+
+__device__ __forceinline__ bool near0(double v) { return fabs(v) <= 1e-8; }
+
+// find_crossing_time; next = -1 for "never".
+__device__ double cf_crossing(const Exact1D &e, double x, int c, int &next)
+{
+    const double a = e.A[2 * c], b = e.A[2 * c + 1];
+    const double v = cf_v(e, x, c);
+    next = -1;
+    if (near0(v)) return CUDART_INF;
+    const int cn = c + (v > 0 ? 1 : -1);
+    if (!(0 <= cn && cn < e.nC)) return CUDART_INF;
+    double xn = (v > 0) ? vert(e, cn) + 1e-16 : vert(e, c) - 1e-16;
+    const double vn = cf_v(e, xn, cn);
+    if (near0(vn)) return CUDART_INF;
+    if ((v > 0) != (vn > 0)) return CUDART_INF;
+    double t;
+    if (xn == 0 || xn == 1) t = CUDART_INF;
+    else if (near0(a)) t = (xn - x) / b;
+    else t = 1.0 / a * log((xn + b / a) / (x + b / a));
+    next = cn;
+    return t;
+}
+
+__device__ __forceinline__ double cf_phi(const Exact1D &e, int c, double x, double t)
+{
+    double a = e.A[2 * c], b = e.A[2 * c + 1];
+    if (!(0 <= x && x <= 1)) { a = 0; b = 0; }
+    if (a == 0) return x + t * b;
+    const double ea = exp(t * a);
+    return ea * x + b * (ea - 1) / a;
+}
+
+// calc_phi for one point; returns false when the crossing cap is hit
+// (the reference raises ValueError, ClosedFormInt.py:155-160).
+__device__ bool cf_point(const Exact1D &e, double x, double t, int cap, double &out)
+{
+    double x_old = x, x_new = x, t_rem = t;
+    if (0 < x_old && x_old < 1) {
+        // on a vertex with non-positive velocity: start just left of it
+        double u = x_old * (double)e.nC;
+        int k = (int)rint(u);
+        if (k >= 0 && k <= e.nC && vert(e, k) == x_old) {
+            int c = k < e.nC ? k : e.nC - 1;
+            double vk = e.A[2 * c] * x_old + e.A[2 * c + 1];
+            if (!(vk > 0)) x_old = x_old - 1e-16;
+        }
+    }
+    for (int counter = 0;;) {
+        const int c = cf_cell(e, x_old);
+        int cn;
+        double tc = cf_crossing(e, x_old, c, cn);
+        bool crossed = true;
+        if (tc >= t_rem) { tc = t_rem; crossed = false; }
+        if (crossed) x_new = (cn > c) ? vert(e, cn) + 1e-12 : vert(e, c) - 1e-12;
+        else x_new = cf_phi(e, c, x_old, tc);
+        x_new = fmin(1.0, fmax(0.0, x_new));
+        t_rem -= tc;
+        if (!crossed) break;
+        if (++counter >= cap) { out = x_new; return false; }
+        x_old = x_new;
+    }
+    out = x_new;
+    return true;
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sA = reinterpret_cast<double *>(smem_raw);
+    __shared__ TileInfo s_tile;
+    const int nC = a.t.nC;
+    const double T_total = a.dt * (double)a.nTimeSteps;
+    const int64_t ntiles = total_tiles(a.batch);
+    unsigned long long c_pts = 0, c_fail = 0;
+    int loaded = -1;
+    Exact1D e;
+    e.A = sA;
+    e.nC = nC;
+    e.step = 1.0 / (double)nC;
+    // the reference gives up after nC crossings
+    const int cap = nC;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        if (threadIdx.x == 0) s_tile = decode_tile(a.batch, tile);
+        __syncthreads();
+        const TileInfo ti = s_tile;
+        if (ti.inst != loaded) {
+            const double *gA = a.A + (size_t)ti.inst * nC * 2;
+            for (int i = threadIdx.x; i < nC * 2; i += blockDim.x) sA[i] = gA[i];
+            loaded = ti.inst;
+            __syncthreads();
+        }
+        for (int64_t i = ti.start + threadIdx.x; i < ti.end; i += blockDim.x) {
+            Real xin;
+            load_pt<1, Real>(a.pts_in, i, &xin);
+            double y;
+            bool ok = cf_point(e, (double)xin, T_total, cap, y);
+            if (a.clamp) y = clamp_ref(y, a.clamp_lo, a.clamp_hi);
+            Real yo = (Real)y;
+            store_pt<1, Real>(a.pts_out, i, &yo);
+            ++c_pts;
+            c_fail += ok ? 0 : 1;
+        }
+        __syncthreads();
+    }
+    if (a.counters) {
+        c_pts = warp_sum_u64(c_pts);
+        c_fail = warp_sum_u64(c_fail);
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(a.counters + CNT_POINTS, c_pts);
+            atomicAdd(a.counters + CNT_FAILED, c_fail);
+        }
+    }
+}
+
+cudaError_t launch_integrate_exact1d(const IntegrateArgs &a, int prec, const LaunchCfg &cfg, cudaStream_t s)
+{
+    size_t smem = (size_t)a.t.nC * 2 * sizeof(double);
+    int grid = cfg.grid > 0 ? cfg.grid : num_sms() * cfg.ctas_per_sm;
+    if (prec == PREC_F64) {
+        auto kern = k_exact1d<double>;
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        kern<<<grid, cfg.block, smem, s>>>(a);
+    } else {
+        auto kern = k_exact1d<float>;
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        kern<<<grid, cfg.block, smem, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace cpab

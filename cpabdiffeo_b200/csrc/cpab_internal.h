@@ -1,0 +1,53 @@
+// cpab_internal.h -- launch descriptors shared by the kernels and the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "cpab_cell.cuh"
+
+namespace cpab {
+
+enum Precision { PREC_F64 = 0, PREC_F32 = 1 };
+
+// Integration schemes.
+//  REF    : calc_T of cpab/gpu/calc_2Dto2D.cu:348-408 -- per time step a
+//           closed-form step with Trel = expm(dt*A_c), kept when the end
+//           point is still in the start cell, else nStepsODE midpoint steps.
+//  SIMPLE : calc_T_simple, calc_2Dto2D.cu:412-445 -- midpoint steps only.
+//  EXACT  : closed-form flow across cell boundaries with hitting times
+//           (1D; restates cpab/cpa1d/calcs/ClosedFormInt.py:64-256).
+enum Scheme { SCHEME_REF = 0, SCHEME_SIMPLE = 1, SCHEME_EXACT = 2 };
+
+// A batch of N independent transforms ("instances"), each with its own
+// cell tables and its own point range.  Uniform batches have n_uniform
+// points per instance; ragged batches give device offsets[N+1].
+struct Batch {
+    int N;
+    int64_t n_uniform;
+    const int64_t *offsets;      // [N+1] or nullptr
+    const int64_t *tile_prefix;  // [N+1] tiles per instance (prefix) or nullptr
+    int64_t tiles_per_inst;      // uniform batches
+    int tile_pts;                // points per CTA tile
+};
+
+struct IntegrateArgs {
+    Tess t;
+    const double *A;      // [N, nC, ne] signed velocity matrices
+    const double *T;      // [N, nC, ne] Trel = expm(dt * signed A)  (REF)
+    const void *pts_in;   // [nPts, DIM] float64 or float32
+    void *pts_out;        // same layout
+    Batch batch;
+    double dt;
+    int nTimeSteps;
+    int nStepsODE;
+    int clamp;            // 1D zero-velocity boundary: clamp to [lo, hi]
+    double clamp_lo, clamp_hi;
+    unsigned long long *counters;  // [4] or nullptr: fast steps, fallback steps, sub-steps, points
+    int max_crossings;    // EXACT: give up after this many boundary crossings
+};
+
+// Counters slots.
+enum { CNT_FAST = 0, CNT_FALLBACK = 1, CNT_SUBSTEPS = 2, CNT_POINTS = 3, CNT_FAILED = 4, CNT_N = 5 };
+
+}  // namespace cpab

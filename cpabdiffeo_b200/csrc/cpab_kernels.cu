@@ -1,0 +1,576 @@
+// cpab_kernels.cu -- sm_100a kernels of the CPAB transform hot path.
+//
+//   k_theta_to_trels  A = B.theta for a batch of theta, then per cell
+//                     signed A and Trel = expm(dt * signed A)
+//                     (cpab/cpaNd/_CpaSpace.py:366-376 + _CpaCalcs.py:227-372
+//                     + cpab/gpu/expm/expm_affine_by_series_{2D,3D}.py)
+//   k_expm            the same from given A (no basis)
+//   k_integrate       calc_T / calc_T_simple for a batch of instances
+//                     (cpab/gpu/calc_2Dto2D.cu:348-445 and 1D/3D twins)
+//   k_trajectory      calc_trajectory (calc_2Dto2D.cu:499-556)
+//   k_cell_idx        calc_cell_idx (calc_2Dto2D.cu:323-344)
+//   k_calc_v          calc_v (calc_2Dto2D.cu:561-602)
+//   k_tile_prefix     tile bookkeeping for ragged batches
+//
+// Layout in HBM: points row-major [nPts, DIM] (the reference's layout);
+// per-instance tables [N, nC, DIM*(DIM+1)] float64; the current instance's
+// tables are staged in shared memory (converted to float in FP32 mode).
+#include "cpab_device.cuh"
+#include "cpab_launch.h"
+
+namespace cpab {
+
+// ------------------------------------------------------------ arithmetic
+// The double instantiation is the bit-exact family; float is the fast one.
+
+template <int DIM, int TESS>
+__device__ __forceinline__ int cell_of(const Tess &t, const double *p) { return exact_cell<DIM, TESS>(t, p); }
+template <int DIM, int TESS>
+__device__ __forceinline__ int cell_of(const Tess &t, const float *p) { return fast_cell<DIM, TESS>(t, p); }
+
+template <int DIM>
+__device__ __forceinline__ void affine(double *x, const double *A, const double *b) { exact_affine<DIM>(x, A, b); }
+template <int DIM>
+__device__ __forceinline__ void affine(float *x, const float *A, const float *b) { fast_affine<DIM>(x, A, b); }
+
+template <int DIM>
+__device__ __forceinline__ void midpoint(double *p, const double *A, double h) { exact_midpoint<DIM>(p, A, h); }
+template <int DIM>
+__device__ __forceinline__ void midpoint(float *p, const float *A, float h)
+{
+    float v[DIM], pm[DIM];
+    fast_affine<DIM>(v, A, p);
+    const float hh = 0.5f * h;
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) pm[i] = fmaf(hh, v[i], p[i]);
+    fast_affine<DIM>(v, A, pm);
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) p[i] = fmaf(h, v[i], p[i]);
+}
+
+// tile_prefix[i] = sum_{j<i} ceil(n_j / tile_pts); one block, sequential
+// chunks per thread, then a block scan of the chunk sums.
+__global__ void k_tile_prefix(const int64_t *offsets, int64_t *prefix, int N, int tile_pts)
+{
+    __shared__ int64_t part[1024];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int per = (N + nt - 1) / nt;
+    const int b = tid * per, e = min(N, b + per);
+    int64_t s = 0;
+    for (int i = b; i < e; ++i) {
+        int64_t n = offsets[i + 1] - offsets[i];
+        s += n > 0 ? (n + tile_pts - 1) / tile_pts : 0;
+    }
+    part[tid] = s;
+    __syncthreads();
+    if (tid == 0) {
+        int64_t acc = 0;
+        for (int i = 0; i < nt; ++i) { int64_t v = part[i]; part[i] = acc; acc += v; }
+        prefix[N] = acc;
+    }
+    __syncthreads();
+    int64_t acc = part[tid];
+    for (int i = b; i < e; ++i) {
+        prefix[i] = acc;
+        int64_t n = offsets[i + 1] - offsets[i];
+        acc += n > 0 ? (n + tile_pts - 1) / tile_pts : 0;
+    }
+}
+
+// ------------------------------------------------------------ integration
+
+// One warp integrates the points [ws, we).  Every lane owns one point and
+// advances it by one unit per iteration -- a closed-form Trel step or one
+// midpoint sub-step, which cost about the same -- and claims the next
+// unprocessed point of the range as soon as its own is finished.  A point
+// that falls back to 100 sub-steps therefore keeps one lane busy, not the
+// whole warp.  Results do not depend on the schedule: each point follows
+// exactly the reference's sequence of operations.
+template <int DIM, int TESS, typename Real, int SCHEME>
+__device__ __forceinline__ void integrate_range(const IntegrateArgs &a, const Real *sA, const Real *sT,
+                                                int64_t ws, int64_t we, Real h,
+                                                unsigned long long &c_fast, unsigned long long &c_fb,
+                                                unsigned long long &c_sub, unsigned long long &c_pts)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int nT = a.nTimeSteps, nODE = a.nStepsODE;
+    int64_t next = ws + 32;
+    int64_t idx = ws + lane;
+    bool active = idx < we;
+    Real p[DIM];
+    int steps_left = 0, sub_left = 0;
+    if (active) {
+        load_pt<DIM, Real>(a.pts_in, idx, p);
+        steps_left = nT;
+        sub_left = (SCHEME == SCHEME_SIMPLE) ? nT * nODE : 0;
+    }
+    while (__any_sync(FULL, active)) {
+        bool fin = false;
+        if (active) {
+            int c = cell_of<DIM, TESS>(a.t, p);
+            if (SCHEME == SCHEME_REF && sub_left == 0) {
+                Real q[DIM];
+                affine<DIM>(q, sT + c * NE, p);
+                int cq = cell_of<DIM, TESS>(a.t, q);
+                if (cq == c) {
+#pragma unroll
+                    for (int i = 0; i < DIM; ++i) p[i] = q[i];
+                    --steps_left;
+                    ++c_fast;
+                } else {
+                    sub_left = nODE;
+                    ++c_fb;
+                }
+            } else {
+                midpoint<DIM>(p, sA + c * NE, h);
+                --sub_left;
+                ++c_sub;
+                if (sub_left == 0) --steps_left;
+            }
+            fin = (SCHEME == SCHEME_SIMPLE) ? (sub_left == 0) : (steps_left == 0);
+            if (fin) {
+                if (a.clamp) {
+#pragma unroll
+                    for (int i = 0; i < DIM; ++i) p[i] = clamp_ref(p[i], a.clamp_lo, a.clamp_hi);
+                }
+                store_pt<DIM, Real>(a.pts_out, idx, p);
+                ++c_pts;
+            }
+        }
+        unsigned done = __ballot_sync(FULL, fin);
+        if (done) {
+            if (fin) {
+                idx = next + __popc(done & lt);
+                active = idx < we;
+                if (active) {
+                    load_pt<DIM, Real>(a.pts_in, idx, p);
+                    steps_left = nT;
+                    sub_left = (SCHEME == SCHEME_SIMPLE) ? nT * nODE : 0;
+                }
+            }
+            next += __popc(done);
+        }
+    }
+}
+
+template <int DIM, int TESS, typename Real, int SCHEME>
+__global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Real *sA = reinterpret_cast<Real *>(smem_raw);
+    Real *sT = sA + a.t.nC * NE;
+    __shared__ TileInfo s_tile;
+
+    const int nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5;
+    const int tab = a.t.nC * NE;
+    const Real h = (Real)(a.dt / (double)a.nStepsODE);
+    const int64_t ntiles = total_tiles(a.batch);
+    unsigned long long c_fast = 0, c_fb = 0, c_sub = 0, c_pts = 0;
+    int loaded = -1;
+
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        if (threadIdx.x == 0) s_tile = decode_tile(a.batch, tile);
+        __syncthreads();
+        const TileInfo ti = s_tile;
+        if (ti.inst != loaded) {
+            const double *gA = a.A + (size_t)ti.inst * tab;
+            const double *gT = a.T + (size_t)ti.inst * tab;
+            for (int i = threadIdx.x; i < tab; i += blockDim.x) {
+                sA[i] = (Real)gA[i];
+                if (SCHEME == SCHEME_REF) sT[i] = (Real)gT[i];
+            }
+            loaded = ti.inst;
+            __syncthreads();
+        }
+        const int64_t n = ti.end - ti.start;
+        const int64_t per = (n + nwarps - 1) / nwarps;
+        int64_t ws = ti.start + warp * per, we = ws + per;
+        if (we > ti.end) we = ti.end;
+        if (ws < we)
+            integrate_range<DIM, TESS, Real, SCHEME>(a, sA, sT, ws, we, h, c_fast, c_fb, c_sub, c_pts);
+        __syncthreads();
+    }
+    if (a.counters) {
+        c_fast = warp_sum_u64(c_fast);
+        c_fb = warp_sum_u64(c_fb);
+        c_sub = warp_sum_u64(c_sub);
+        c_pts = warp_sum_u64(c_pts);
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(a.counters + CNT_FAST, c_fast);
+            atomicAdd(a.counters + CNT_FALLBACK, c_fb);
+            atomicAdd(a.counters + CNT_SUBSTEPS, c_sub);
+            atomicAdd(a.counters + CNT_POINTS, c_pts);
+        }
+    }
+}
+
+// ------------------------------------------------------------ trajectory
+
+// calc_trajectory: out is [(nTimeSteps+1), nPts, DIM]; row 0 = the input
+// (the reference prepends it on the host, _CpaCalcs.py:866-868).
+template <int DIM, int TESS>
+__global__ void __launch_bounds__(256) k_trajectory(IntegrateArgs a, int64_t nPts)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sA = reinterpret_cast<double *>(smem_raw);
+    double *sT = sA + a.t.nC * NE;
+    const int tab = a.t.nC * NE;
+    for (int i = threadIdx.x; i < tab; i += blockDim.x) {
+        sA[i] = a.A[i];
+        sT[i] = a.T[i];
+    }
+    __syncthreads();
+    const double h = XDIV(a.dt, (double)a.nStepsODE);
+    double *out = static_cast<double *>(a.pts_out);
+    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < nPts;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        double p[DIM], q[DIM];
+        load_pt<DIM, double>(a.pts_in, idx, p);
+        store_pt<DIM, double>(out, idx, p);
+        for (int s = 0; s < a.nTimeSteps; ++s) {
+            int c = exact_cell<DIM, TESS>(a.t, p);
+            exact_affine<DIM>(q, sT + c * NE, p);
+            if (exact_cell<DIM, TESS>(a.t, q) == c) {
+#pragma unroll
+                for (int i = 0; i < DIM; ++i) p[i] = q[i];
+            } else {
+                for (int k = 0; k < a.nStepsODE; ++k) {
+                    int cc = exact_cell<DIM, TESS>(a.t, p);
+                    exact_midpoint<DIM>(p, sA + cc * NE, h);
+                }
+            }
+            store_pt<DIM, double>(out, (int64_t)(s + 1) * nPts + idx, p);
+        }
+    }
+}
+
+// ------------------------------------------------------------ cell index, velocity
+
+template <int DIM, int TESS>
+__global__ void k_cell_idx(Tess t, const double *pts, int32_t *out, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double p[DIM];
+        load_pt<DIM, double>(pts, i, p);
+        out[i] = exact_cell<DIM, TESS>(t, p);
+    }
+}
+
+template <int DIM, int TESS>
+__global__ void __launch_bounds__(256) k_calc_v(Tess t, const double *A, const double *pts, double *out, int64_t n)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sA = reinterpret_cast<double *>(smem_raw);
+    for (int i = threadIdx.x; i < t.nC * NE; i += blockDim.x) sA[i] = A[i];
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double p[DIM], v[DIM];
+        load_pt<DIM, double>(pts, i, p);
+        int c = exact_cell<DIM, TESS>(t, p);
+        exact_affine<DIM>(v, sA + c * NE, p);
+        store_pt<DIM, double>(out, i, v);
+    }
+}
+
+// ------------------------------------------------------------ expm
+
+// expm of the 2x2 linear block, cpab/gpu/expm/expm_affine_by_series_2D.py:28-74
+// (eigenvalue cases: repeated, real, complex).
+__device__ void expm_2x2(double a, double b, double c, double d, double *E)
+{
+    double disc = (a - d) * (a - d) + 4 * b * c;
+    double e = exp((a + d) / 2);
+    double hd = (a - d) / 2;
+    if (disc == 0) {
+        E[0] = (1 + hd) * e;
+        E[1] = b * e;
+        E[2] = c * e;
+        E[3] = (1 - hd) * e;
+    } else {
+        double delta, ch, s;
+        if (disc > 0) {
+            delta = sqrt(disc) / 2;
+            ch = cosh(delta);
+            s = sinh(delta) / delta;
+        } else {
+            delta = sqrt(-disc) / 2;
+            ch = cos(delta);
+            s = sin(delta) / delta;
+        }
+        E[0] = (ch + hd * s) * e;
+        E[1] = b * s * e;
+        E[2] = c * s * e;
+        E[3] = (ch - hd * s) * e;
+    }
+}
+
+// I + sum_{k=1..12} M^k / k! for an affine block with zero last row
+// (expm_affine_by_series_2D.py:156-232, _3D.py:26-220).
+template <int DIM>
+__device__ void expm_taylor12(const double *M, double *T)
+{
+    constexpr int NC = DIM + 1, NE = DIM * NC;
+    double An[NE], Bn[NE];
+#pragma unroll
+    for (int r = 0; r < DIM; ++r)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) T[r * NC + c] = (r == c) ? 1.0 : 0.0;
+#pragma unroll
+    for (int k = 0; k < NE; ++k) { An[k] = M[k]; T[k] += An[k]; }
+    int fact = 1;
+    for (int i = 2; i <= 12; ++i) {
+#pragma unroll
+        for (int k = 0; k < NE; ++k) Bn[k] = An[k];
+        fact *= i;
+        const double inv = 1.0 / (double)fact;
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                double acc = M[r * NC] * Bn[c];
+#pragma unroll
+                for (int m = 1; m < DIM; ++m) acc += M[r * NC + m] * Bn[m * NC + c];
+                An[r * NC + c] = acc;
+            }
+#pragma unroll
+        for (int k = 0; k < NE; ++k) T[k] += An[k] * inv;
+    }
+}
+
+// Trel for one cell from M = dt * signed A.
+template <int DIM>
+__device__ void affine_expm(const double *M, double *T)
+{
+    if (DIM == 1) {
+        // cpab/cpaNd/_CpaCalcs.py:288-292
+        T[0] = exp(M[0]);
+        T[1] = M[1];
+        if (M[0] != 0) T[1] = T[1] * (T[0] - 1) / M[0];
+    } else if (DIM == 2) {
+        double det = M[0] * M[4] - M[1] * M[3];
+        if (det != 0) {
+            double E[4];
+            expm_2x2(M[0], M[1], M[3], M[4], E);
+            T[0] = E[0]; T[1] = E[1]; T[3] = E[2]; T[4] = E[3];
+            double i00 = M[4] / det, i11 = M[0] / det, i01 = -M[1] / det, i10 = -M[3] / det;
+            double u = i00 * M[2] + i01 * M[5];
+            double w = i10 * M[2] + i11 * M[5];
+            T[2] = (T[0] - 1) * u + T[1] * w;
+            T[5] = T[3] * u + (T[4] - 1) * w;
+        } else {
+            expm_taylor12<2>(M, T);
+        }
+    } else {
+        expm_taylor12<3>(M, T);
+    }
+}
+
+// signed A and Trel for n_cells = N*nC cells from A.
+template <int DIM>
+__global__ void k_expm(const double *A, double *signedA, double *T, int64_t n_cells, double dt, double sign)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n_cells;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        double sA[NE], M[NE], Tr[NE];
+#pragma unroll
+        for (int k = 0; k < NE; ++k) {
+            sA[k] = sign < 0 ? -A[c * NE + k] : A[c * NE + k];
+            M[k] = sA[k] * dt;
+        }
+        affine_expm<DIM>(M, Tr);
+#pragma unroll
+        for (int k = 0; k < NE; ++k) {
+            if (signedA) signedA[c * NE + k] = sA[k];
+            T[c * NE + k] = Tr[k];
+        }
+    }
+}
+
+// A = B.theta (theta row-major [N, d], B row-major [D_A, d]) fused with the
+// per-cell expm: one thread per (instance, cell).  A is optional output.
+template <int DIM>
+__global__ void k_theta_to_trels(const double *B, const double *theta, int d, int nC, int N,
+                                 double dt, double sign, double *A, double *signedA, double *T)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    const int64_t total = (int64_t)N * nC;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        const int n = (int)(g / nC), c = (int)(g - (int64_t)n * nC);
+        const double *th = theta + (int64_t)n * d;
+        const double *Bc = B + (int64_t)c * NE * d;
+        double a[NE], M[NE], Tr[NE];
+#pragma unroll
+        for (int k = 0; k < NE; ++k) a[k] = 0.0;
+        for (int j = 0; j < d; ++j) {
+            const double tj = th[j];
+#pragma unroll
+            for (int k = 0; k < NE; ++k) a[k] = fma(Bc[k * d + j], tj, a[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < NE; ++k) {
+            if (A) A[g * NE + k] = a[k];
+            double s = sign < 0 ? -a[k] : a[k];
+            if (signedA) signedA[g * NE + k] = s;
+            M[k] = s * dt;
+        }
+        affine_expm<DIM>(M, Tr);
+#pragma unroll
+        for (int k = 0; k < NE; ++k) T[g * NE + k] = Tr[k];
+    }
+}
+
+// ------------------------------------------------------------ launchers
+
+static int g_num_sms = 0;
+int num_sms()
+{
+    if (g_num_sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+        if (g_num_sms <= 0) g_num_sms = 148;
+    }
+    return g_num_sms;
+}
+
+static int grid_for(int64_t n, int block, int per_sm = 8)
+{
+    int64_t g = (n + block - 1) / block;
+    int64_t cap = (int64_t)num_sms() * per_sm;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+template <int DIM, int TESS, typename Real, int SCHEME>
+static cudaError_t launch_integrate_t(const IntegrateArgs &a, const LaunchCfg &cfg, cudaStream_t s)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    size_t smem = (size_t)2 * a.t.nC * NE * sizeof(Real);
+    auto kern = k_integrate<DIM, TESS, Real, SCHEME>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    int grid = cfg.grid > 0 ? cfg.grid : num_sms() * cfg.ctas_per_sm;
+    kern<<<grid, cfg.block, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int DIM, int TESS>
+static cudaError_t launch_integrate_dt(const IntegrateArgs &a, int prec, int scheme, const LaunchCfg &cfg,
+                                       cudaStream_t s)
+{
+    if (prec == PREC_F64) {
+        if (scheme == SCHEME_REF) return launch_integrate_t<DIM, TESS, double, SCHEME_REF>(a, cfg, s);
+        return launch_integrate_t<DIM, TESS, double, SCHEME_SIMPLE>(a, cfg, s);
+    }
+    if (scheme == SCHEME_REF) return launch_integrate_t<DIM, TESS, float, SCHEME_REF>(a, cfg, s);
+    return launch_integrate_t<DIM, TESS, float, SCHEME_SIMPLE>(a, cfg, s);
+}
+
+cudaError_t launch_integrate(const IntegrateArgs &a, int prec, int scheme, const LaunchCfg &cfg, cudaStream_t s)
+{
+    const int dim = a.t.dim, tess = a.t.tess;
+    if (dim == 1) return launch_integrate_dt<1, 2>(a, prec, scheme, cfg, s);
+    if (dim == 2) return tess == 1 ? launch_integrate_dt<2, 1>(a, prec, scheme, cfg, s)
+                                   : launch_integrate_dt<2, 2>(a, prec, scheme, cfg, s);
+    return tess == 1 ? launch_integrate_dt<3, 1>(a, prec, scheme, cfg, s)
+                     : launch_integrate_dt<3, 2>(a, prec, scheme, cfg, s);
+}
+
+cudaError_t launch_tile_prefix(const int64_t *offsets, int64_t *prefix, int N, int tile_pts, cudaStream_t s)
+{
+    k_tile_prefix<<<1, 1024, 0, s>>>(offsets, prefix, N, tile_pts);
+    return cudaGetLastError();
+}
+
+template <int DIM, int TESS>
+static cudaError_t launch_traj_t(const IntegrateArgs &a, int64_t nPts, cudaStream_t s)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    size_t smem = (size_t)2 * a.t.nC * NE * sizeof(double);
+    auto kern = k_trajectory<DIM, TESS>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<grid_for(nPts, 256, 4), 256, smem, s>>>(a, nPts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trajectory(const IntegrateArgs &a, int64_t nPts, cudaStream_t s)
+{
+    const int dim = a.t.dim, tess = a.t.tess;
+    if (dim == 1) return launch_traj_t<1, 2>(a, nPts, s);
+    if (dim == 2) return tess == 1 ? launch_traj_t<2, 1>(a, nPts, s) : launch_traj_t<2, 2>(a, nPts, s);
+    return tess == 1 ? launch_traj_t<3, 1>(a, nPts, s) : launch_traj_t<3, 2>(a, nPts, s);
+}
+
+cudaError_t launch_cell_idx(const Tess &t, const double *pts, int32_t *out, int64_t n, cudaStream_t s)
+{
+    int g = grid_for(n, 256);
+    if (t.dim == 1) k_cell_idx<1, 2><<<g, 256, 0, s>>>(t, pts, out, n);
+    else if (t.dim == 2) {
+        if (t.tess == 1) k_cell_idx<2, 1><<<g, 256, 0, s>>>(t, pts, out, n);
+        else k_cell_idx<2, 2><<<g, 256, 0, s>>>(t, pts, out, n);
+    } else {
+        if (t.tess == 1) k_cell_idx<3, 1><<<g, 256, 0, s>>>(t, pts, out, n);
+        else k_cell_idx<3, 2><<<g, 256, 0, s>>>(t, pts, out, n);
+    }
+    return cudaGetLastError();
+}
+
+template <int DIM, int TESS>
+static cudaError_t launch_v_t(const Tess &t, const double *A, const double *pts, double *out, int64_t n,
+                              cudaStream_t s)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    size_t smem = (size_t)t.nC * NE * sizeof(double);
+    auto kern = k_calc_v<DIM, TESS>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<grid_for(n, 256, 4), 256, smem, s>>>(t, A, pts, out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_calc_v(const Tess &t, const double *A, const double *pts, double *out, int64_t n, cudaStream_t s)
+{
+    if (t.dim == 1) return launch_v_t<1, 2>(t, A, pts, out, n, s);
+    if (t.dim == 2) return t.tess == 1 ? launch_v_t<2, 1>(t, A, pts, out, n, s) : launch_v_t<2, 2>(t, A, pts, out, n, s);
+    return t.tess == 1 ? launch_v_t<3, 1>(t, A, pts, out, n, s) : launch_v_t<3, 2>(t, A, pts, out, n, s);
+}
+
+cudaError_t launch_expm(int dim, const double *A, double *signedA, double *T, int64_t n_cells, double dt, double sign,
+                        cudaStream_t s)
+{
+    int g = grid_for(n_cells, 128);
+    if (dim == 1) k_expm<1><<<g, 128, 0, s>>>(A, signedA, T, n_cells, dt, sign);
+    else if (dim == 2) k_expm<2><<<g, 128, 0, s>>>(A, signedA, T, n_cells, dt, sign);
+    else k_expm<3><<<g, 128, 0, s>>>(A, signedA, T, n_cells, dt, sign);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_theta_to_trels(int dim, const double *B, const double *theta, int d, int nC, int N, double dt,
+                                  double sign, double *A, double *signedA, double *T, cudaStream_t s)
+{
+    int64_t total = (int64_t)N * nC;
+    int g = grid_for(total, 128);
+    if (dim == 1) k_theta_to_trels<1><<<g, 128, 0, s>>>(B, theta, d, nC, N, dt, sign, A, signedA, T);
+    else if (dim == 2) k_theta_to_trels<2><<<g, 128, 0, s>>>(B, theta, d, nC, N, dt, sign, A, signedA, T);
+    else k_theta_to_trels<3><<<g, 128, 0, s>>>(B, theta, d, nC, N, dt, sign, A, signedA, T);
+    return cudaGetLastError();
+}
+
+}  // namespace cpab

@@ -1,0 +1,32 @@
+// cpab_launch.h -- host-side launchers of cpab_kernels.cu / cpab_remap.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "cpab_internal.h"
+
+namespace cpab {
+
+// Launch shape of the integration kernel (chosen by the autotuner).
+struct LaunchCfg {
+    int block = 256;       // threads per CTA (multiple of 32, <= 256)
+    int ctas_per_sm = 4;   // persistent grid = SMs * ctas_per_sm
+    int grid = 0;          // explicit grid (0 = persistent default)
+    int tile_pts = 2048;   // points per CTA tile
+};
+
+int num_sms();
+
+cudaError_t launch_integrate(const IntegrateArgs &a, int prec, int scheme, const LaunchCfg &cfg, cudaStream_t s);
+cudaError_t launch_integrate_exact1d(const IntegrateArgs &a, int prec, const LaunchCfg &cfg, cudaStream_t s);
+cudaError_t launch_tile_prefix(const int64_t *offsets, int64_t *prefix, int N, int tile_pts, cudaStream_t s);
+cudaError_t launch_trajectory(const IntegrateArgs &a, int64_t nPts, cudaStream_t s);
+cudaError_t launch_cell_idx(const Tess &t, const double *pts, int32_t *out, int64_t n, cudaStream_t s);
+cudaError_t launch_calc_v(const Tess &t, const double *A, const double *pts, double *out, int64_t n, cudaStream_t s);
+cudaError_t launch_expm(int dim, const double *A, double *signedA, double *T, int64_t n_cells, double dt,
+                        double sign, cudaStream_t s);
+cudaError_t launch_theta_to_trels(int dim, const double *B, const double *theta, int d, int nC, int N, double dt,
+                                  double sign, double *A, double *signedA, double *T, cudaStream_t s);
+
+}  // namespace cpab

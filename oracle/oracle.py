@@ -1,0 +1,254 @@
+"""Python access to the CPU parity oracle.  TEST INFRASTRUCTURE ONLY.
+
+Two libraries, both built by oracle/Makefile:
+  * liboracle.so      -- this repository's C restatement (cpab_oracle.c),
+                         the checker every GPU parity test uses;
+  * _ref/libcpab_ref.so -- the reference's own kernel sources compiled as host
+                         code (ref_kernels.cpp, ref_expm.cpp); present only where
+                         the reference checkout existed at build time.  It pins
+                         the restatement (tests/golden/make_golden.py) and serves
+                         as the CPU baseline of bench.py when available.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module; the product package never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+REF_SO = HERE / "_ref" / "libcpab_ref.so"
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+
+
+class OracleTess(C.Structure):
+    _fields_ = [("dim", C.c_int), ("tess", C.c_int), ("nC0", C.c_int), ("nC1", C.c_int), ("nC2", C.c_int),
+                ("inc_x", C.c_double), ("inc_y", C.c_double), ("inc_z", C.c_double)]
+
+
+def build(quiet: bool = True) -> None:
+    """Run the oracle Makefile (liboracle.so; _ref only if the reference exists)."""
+    r = subprocess.run(["make", "-C", str(HERE)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
+    if not quiet:
+        print(r.stdout)
+
+
+_ora = None
+_ref = None
+
+
+def lib() -> C.CDLL:
+    global _ora
+    if _ora is None:
+        if not ORACLE_SO.exists():
+            build()
+        L = C.CDLL(str(ORACLE_SO))
+        L.oracle_cell_idx.restype = C.c_int
+        L.oracle_calc_T.restype = C.c_int64
+        L.oracle_closed_form_1d.restype = C.c_int64
+        L.oracle_remap_ssd.restype = C.c_double
+        _ora = L
+    return _ora
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def ref_lib() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        if not REF_SO.exists():
+            raise FileNotFoundError(f"{REF_SO} (built only where the reference sources exist)")
+        _ref = C.CDLL(str(REF_SO))
+    return _ref
+
+
+def _d(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _c64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def tess_struct(dim: int, tess: int, nCs, incs) -> OracleTess:
+    n = list(nCs) + [0] * (3 - len(nCs))
+    i = list(incs) + [1.0] * (3 - len(incs))
+    return OracleTess(dim, tess, n[0], n[1], n[2], i[0], i[1], i[2])
+
+
+# ------------------------------------------------------------------ restatement
+
+
+def calc_cell_idx(t: OracleTess, pts) -> np.ndarray:
+    pts = _c64(pts)
+    out = np.empty(pts.shape[0], dtype=np.int32)
+    lib().oracle_calc_cell_idx(C.byref(t), _d(pts), out.ctypes.data_as(_ip), C.c_int64(pts.shape[0]))
+    return out
+
+
+def calc_v(t: OracleTess, As, pts) -> np.ndarray:
+    pts, As = _c64(pts), _c64(As)
+    out = np.empty_like(pts)
+    lib().oracle_calc_v(C.byref(t), _d(As), _d(pts), _d(out), C.c_int64(pts.shape[0]))
+    return out
+
+
+def expm_cells(dim: int, A, dt: float, sign: int):
+    """(signedA, Trels) for cells A [..., ne]."""
+    A = _c64(A)
+    ne = dim * (dim + 1)
+    n = A.size // ne
+    sA = np.empty_like(A)
+    Tr = np.empty_like(A)
+    lib().oracle_expm_cells(C.c_int(dim), _d(A), C.c_int64(n), C.c_double(dt), C.c_int(sign), _d(sA), _d(Tr))
+    return sA, Tr
+
+
+def calc_T(t: OracleTess, Trels, sA, pts, dt, nT, nODE):
+    """Returns (out, number of fallback steps)."""
+    pts = _c64(pts)
+    out = np.empty_like(pts)
+    nfb = lib().oracle_calc_T(C.byref(t), _d(_c64(Trels)), _d(_c64(sA)), _d(pts), _d(out),
+                              C.c_int64(pts.shape[0]), C.c_double(dt), C.c_int(nT), C.c_int(nODE))
+    return out, int(nfb)
+
+
+def calc_T_simple(t: OracleTess, sA, pts, dt, nT, nODE):
+    pts = _c64(pts)
+    out = np.empty_like(pts)
+    lib().oracle_calc_T_simple(C.byref(t), _d(_c64(sA)), _d(pts), _d(out), C.c_int64(pts.shape[0]),
+                               C.c_double(dt), C.c_int(nT), C.c_int(nODE))
+    return out
+
+
+def calc_trajectory(t: OracleTess, Trels, sA, pts, dt, nT, nODE):
+    pts = _c64(pts)
+    traj = np.empty((nT + 1,) + pts.shape)
+    lib().oracle_calc_trajectory(C.byref(t), _d(_c64(Trels)), _d(_c64(sA)), _d(pts), _d(traj),
+                                 C.c_int64(pts.shape[0]), C.c_double(dt), C.c_int(nT), C.c_int(nODE))
+    return traj
+
+
+def closed_form_1d(sA, nC: int, pts, t_total: float):
+    """ClosedFormInt.calc_phi per point on [0,1]; returns (out, n_failed)."""
+    sA = _c64(sA).reshape(nC, 2)
+    x_tess = np.linspace(0.0, 1.0, nC + 1)
+    vel = np.empty(nC + 1)
+    for k in range(nC + 1):
+        c = min(k, nC - 1)
+        vel[k] = sA[c, 0] * x_tess[k] + sA[c, 1]
+    pts = _c64(pts).reshape(-1)
+    out = np.empty_like(pts)
+    nf = lib().oracle_closed_form_1d(_d(sA), _d(x_tess), _d(vel), C.c_int(nC), _d(pts), _d(out),
+                                     C.c_int64(pts.size), C.c_double(t_total))
+    return out, int(nf)
+
+
+def clamp_1d(x, lo=0.0, hi=1.0):
+    """threshold_krnl (cpab/cpaNd/_CpaSpace.py:35-43)."""
+    y = np.array(x, dtype=np.float64, copy=True)
+    y[y < lo] = lo
+    y[y > hi] = hi
+    return y
+
+
+# ------------------------------------------------------------------ reference (host-compiled)
+
+
+def _ref_fn(name):
+    return getattr(ref_lib(), name)
+
+
+def ref_calc_cell_idx(dim: int, tess: int, nCs, incs, pts, nC: int) -> np.ndarray:
+    pts = _c64(pts).copy()
+    out = np.empty(pts.shape[0], dtype=np.int32)
+    n = list(nCs) + [0] * (3 - len(nCs))
+    i = list(incs) + [1.0] * (3 - len(incs))
+    _ref_fn(f"ref_d{dim}_t{tess}_calc_cell_idx")(_d(pts), out.ctypes.data_as(_ip), C.c_int(pts.shape[0]),
+                                                 C.c_int(n[0]), C.c_int(n[1]), C.c_int(n[2]),
+                                                 C.c_double(i[0]), C.c_double(i[1]), C.c_double(i[2]), C.c_int(nC))
+    return out
+
+
+def ref_calc_v(dim, tess, nCs, incs, As, pts, nC):
+    pts = _c64(pts).copy()
+    As = _c64(As).copy()
+    vel = np.zeros_like(pts)
+    n = list(nCs) + [0] * (3 - len(nCs))
+    i = list(incs) + [1.0] * (3 - len(incs))
+    _ref_fn(f"ref_d{dim}_t{tess}_calc_v")(_d(pts), _d(vel), _d(As), C.c_int(pts.shape[0]),
+                                          C.c_int(n[0]), C.c_int(n[1]), C.c_int(n[2]),
+                                          C.c_double(i[0]), C.c_double(i[1]), C.c_double(i[2]), C.c_int(nC))
+    return vel
+
+
+def ref_calc_T(dim, tess, nCs, incs, Trels, sA, pts, dt, nT, nODE, nC, simple=False):
+    pts = _c64(pts).copy()
+    out = np.zeros_like(pts)
+    n = list(nCs) + [0] * (3 - len(nCs))
+    i = list(incs) + [1.0] * (3 - len(incs))
+    common = [C.c_double(dt), C.c_int(nT), C.c_int(nODE), C.c_int(pts.shape[0]),
+              C.c_int(n[0]), C.c_int(n[1]), C.c_int(n[2]),
+              C.c_double(i[0]), C.c_double(i[1]), C.c_double(i[2]), C.c_int(nC)]
+    if simple:
+        _ref_fn(f"ref_d{dim}_t{tess}_calc_T_simple")(_d(pts), _d(out), _d(_c64(sA).copy()), *common)
+    else:
+        _ref_fn(f"ref_d{dim}_t{tess}_calc_T")(_d(pts), _d(out), _d(_c64(Trels).copy()), _d(_c64(sA).copy()),
+                                              *common)
+    return out
+
+
+def ref_calc_trajectory(dim, tess, nCs, incs, Trels, sA, pts, dt, nT, nODE, nC):
+    pts = _c64(pts)
+    nP = pts.shape[0]
+    pos = np.zeros((nT * nP, dim))
+    pos[:nP] = pts
+    n = list(nCs) + [0] * (3 - len(nCs))
+    i = list(incs) + [1.0] * (3 - len(incs))
+    _ref_fn(f"ref_d{dim}_t{tess}_calc_trajectory")(_d(pos), _d(_c64(Trels).copy()), _d(_c64(sA).copy()),
+                                                   C.c_double(dt), C.c_int(nT), C.c_int(nODE), C.c_int(nP),
+                                                   C.c_int(n[0]), C.c_int(n[1]), C.c_int(n[2]),
+                                                   C.c_double(i[0]), C.c_double(i[1]), C.c_double(i[2]),
+                                                   C.c_int(nC))
+    return np.concatenate([pts[None], pos.reshape(nT, nP, dim)], axis=0)
+
+
+def ref_expm(dim: int, M) -> np.ndarray:
+    """The reference's gpu_expm kernel (p=12) on dt-scaled signed matrices M [n, ne]."""
+    M = _c64(M).copy()
+    ne = dim * (dim + 1)
+    n = M.size // ne
+    T = np.zeros_like(M)
+    _ref_fn(f"ref_expm{dim}d")(_d(M), _d(T), C.c_int(n), C.c_int(12))
+    return T
+
+
+def ref_expm_1d(M) -> np.ndarray:
+    """The reference's 1D closed form (cpab/cpaNd/_CpaCalcs.py:285-292), numpy as there."""
+    M = _c64(M).reshape(-1, 2)
+    T = np.empty_like(M)
+    np.exp(M[:, 0], out=T[:, 0])
+    T[:, 1] = M[:, 1]
+    idx = M[:, 0] != 0
+    T[idx, 1] = T[idx, 1] * (T[idx, 0] - 1) / M[idx, 0]
+    return T
+
+
+def nproc() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1

@@ -1,0 +1,60 @@
+"""libcpab_b200.so loads and exports every function include/cpab_b200.h declares;
+no compute calls (no GPU needed).  Also checks host-side argument validation
+paths that return before any CUDA call."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+from cpabdiffeo_b200 import _lib
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names |= set(re.findall(r"\b(cpab_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    assert "cpab_calc_T" in names and "cpab_ctx_create" in names
+    assert len(names) >= 15
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_bindings_cover_header():
+    assert set(declared()) <= set(_lib.SIGNATURES)
+
+
+def test_ctx_create_validation():
+    lib = _lib.load()
+    h = C.c_void_p()
+    nCs = (C.c_int * 3)(4, 4, 1)
+    incs = (C.c_double * 3)(0.25, 0.25, 1.0)
+    assert lib.cpab_ctx_create(C.byref(h), 4, 1, nCs, incs) == 1          # bad dim
+    assert b"dim" in lib.cpab_last_error_string(None)
+    assert lib.cpab_ctx_create(C.byref(h), 1, 1, nCs, incs) == 1          # 1D tess I
+    bad = (C.c_double * 3)(0.0, 0.25, 1.0)
+    assert lib.cpab_ctx_create(C.byref(h), 2, 1, nCs, bad) == 1           # inc 0
+    assert lib.cpab_ctx_create(C.byref(h), 2, 1, nCs, incs) == 0
+    assert lib.cpab_ctx_num_cells(h) == 64 and lib.cpab_ctx_cell_len(h) == 6
+    # argument checks that return before any CUDA call
+    assert lib.cpab_calc_T(h, None, None, None, None, 10, 0, 0, 0.02, 50, 100, None, None) == 1
+    assert lib.cpab_calc_T(h, 8, 8, 16, 16, 10, 5, 0, 0.02, 50, 100, None, None) == 3   # dtype
+    assert lib.cpab_calc_T(h, 8, 8, 16, 16, 10, 0, 0, 0.02, 50, 0, None, None) == 1     # nStepsODE
+    # pts and out overlap -> ALIAS (reference raises, cpab/cpaNd/_CpaCalcs.py:388)
+    assert lib.cpab_calc_T(h, 8, 8, 4096, 4096 + 64, 10, 0, 0, 0.02, 50, 100, None, None) == 4
+    assert b"same memory" in lib.cpab_last_error_string(h)
+    assert lib.cpab_calc_T(h, 8, 8, 16, 16, 10, 0, 2, 0.02, 50, 100, None, None) == 10  # exact needs 1D
+    assert lib.cpab_set_launch(h, 48, 0, 0) == 1
+    assert lib.cpab_ctx_destroy(h) == 0

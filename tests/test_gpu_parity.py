@@ -1,0 +1,271 @@
+"""GPU parity: libcpab_b200.so (through the C ABI) against the golden fixtures
+made by the reference's own kernel sources and against the oracle restatement.
+
+Tolerances (stated per result):
+  * cell indices, FP64 REF / SIMPLE / trajectory given the same tables: bit-exact
+  * per-cell expm (CUDA vs host libm): 1e-14 absolute
+  * theta -> T(x) end to end in FP64 (tables computed on the GPU): 1e-12 absolute
+  * FP32 mode vs the FP64 oracle: 1e-5 * max(1, |x|)
+  * 1D closed form, FP64: 1e-12 absolute; FP32 storage: 1e-6 absolute
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+from cpabdiffeo_b200 import _lib
+from cpabdiffeo_b200.cpa_space import CpaSpace
+from cpabdiffeo_b200.space import Prior, pixel_centers
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted((Path(__file__).resolve().parent / "golden").glob("*.npz"))
+TESS = {1: "I", 2: "II"}
+DEV = "cuda:0"
+
+
+def load(path):
+    with np.load(path) as z:
+        return {k: z[k] for k in z.files}
+
+
+def space_for(g, precision=torch.float64):
+    dim = int(g["dim"])
+    return CpaSpace([0.0] * dim, [1.0] * dim, list(g["nCs"]), tess=TESS[int(g["tess"])], device=DEV,
+                    precision=precision)
+
+
+def cuda(a, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=DEV)
+
+
+@pytest.fixture(params=GOLDEN, ids=[p.stem for p in GOLDEN])
+def g(request):
+    return load(request.param)
+
+
+def test_cell_idx_bit_exact(g):
+    sp = space_for(g)
+    pts = cuda(g["pts_wide"])
+    out = torch.empty(pts.shape[0], dtype=torch.int32, device=DEV)
+    sp.calc_cell_idx(pts, out)
+    np.testing.assert_array_equal(out.cpu().numpy(), g["cell_idx"])
+
+
+def test_calc_v_bit_exact(g):
+    sp = space_for(g)
+    sp.update_pat(g["A"].reshape(-1))
+    pts = cuda(g["pts"])
+    v = torch.empty_like(pts)
+    sp.calc_v(pts=pts, out=v)
+    np.testing.assert_array_equal(v.cpu().numpy(), g["v"])
+
+
+@pytest.mark.parametrize("tag,sign", [("fwd", 1), ("inv", -1)])
+def test_expm(g, tag, sign):
+    sp = space_for(g)
+    sA, Tr = sp.tables_from_A(cuda(g["A"].reshape(1, -1)), float(g["dt"]), sign)
+    np.testing.assert_array_equal(sA.cpu().numpy().reshape(g["A"].shape), -g["A"] if sign < 0 else g["A"])
+    np.testing.assert_allclose(Tr.cpu().numpy().reshape(g["A"].shape), g[f"Trels_{tag}"], rtol=0, atol=1e-14)
+
+
+def _run_T(sp, g, tag, sign, pts, scheme=_lib.SCHEME_REF, dtype=torch.float64, counters=None):
+    sA = cuda((-g["A"] if sign < 0 else g["A"]).reshape(-1))
+    Tr = cuda(g[f"Trels_{tag}"].reshape(-1))
+    x = cuda(pts, dtype)
+    out = torch.empty_like(x)
+    c = sp._ctx
+    c.check(c.lib.cpab_calc_T(c.h, _lib.ptr(sA), _lib.ptr(Tr), _lib.ptr(x), _lib.ptr(out), x.shape[0],
+                              _lib.CPAB_F64 if dtype == torch.float64 else _lib.CPAB_F32, scheme,
+                              float(g["dt"]), int(g["nT"]), int(g["nODE"]), _lib.ptr(counters), _lib.stream_ptr()))
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("tag,sign", [("fwd", 1), ("inv", -1)])
+def test_calc_T_ref_bit_exact(g, tag, sign):
+    """Same tables as the reference -> identical points, including the 1D clamp."""
+    sp = space_for(g)
+    out = _run_T(sp, g, tag, sign, g["pts"])
+    np.testing.assert_array_equal(out, g[f"T_{tag}"])
+
+
+def test_calc_T_simple_bit_exact(g):
+    sp = space_for(g)
+    out = _run_T(sp, g, "fwd", 1, g["pts"][:500], scheme=_lib.SCHEME_SIMPLE)
+    np.testing.assert_array_equal(out, g["T_simple"])
+
+
+def test_trajectory_bit_exact(g):
+    sp = space_for(g)
+    sA = cuda(g["A"].reshape(-1))
+    Tr = cuda(g["Trels_fwd"].reshape(-1))
+    x = cuda(g["pts"][:200])
+    traj = torch.empty((int(g["nT"]) + 1, 200, int(g["dim"])), dtype=torch.float64, device=DEV)
+    c = sp._ctx
+    c.check(c.lib.cpab_calc_trajectory(c.h, _lib.ptr(sA), _lib.ptr(Tr), _lib.ptr(x), _lib.ptr(traj), 200,
+                                       float(g["dt"]), int(g["nT"]), int(g["nODE"]), _lib.stream_ptr()))
+    np.testing.assert_array_equal(traj.cpu().numpy(), g["traj"])
+
+
+def test_fallback_counter_matches_oracle(g, oracle_mod):
+    O = oracle_mod
+    sp = space_for(g)
+    cnt = torch.zeros(_lib.CNT_N, dtype=torch.int64, device=DEV)
+    _run_T(sp, g, "fwd", 1, g["pts"], counters=cnt)
+    t = O.tess_struct(int(g["dim"]), int(g["tess"]), list(g["nCs"]), list(g["incs"]))
+    _, nfb = O.calc_T(t, g["Trels_fwd"], g["A"], g["pts"], float(g["dt"]), int(g["nT"]), int(g["nODE"]))
+    cnt = cnt.cpu().numpy()
+    n, nT = g["pts"].shape[0], int(g["nT"])
+    assert cnt[_lib.CNT_FALLBACK] == nfb
+    assert cnt[_lib.CNT_FAST] + cnt[_lib.CNT_FALLBACK] == n * nT
+    assert cnt[_lib.CNT_SUBSTEPS] == nfb * int(g["nODE"])
+    assert cnt[_lib.CNT_POINTS] == n
+
+
+def test_fp32_within_tolerance(g):
+    """FP32 mode against the FP64 reference result: 1e-5 * max(1, |x|)."""
+    sp = space_for(g, torch.float32)
+    out = _run_T(sp, g, "fwd", 1, g["pts"].astype(np.float32), dtype=torch.float32)
+    ref = g["T_fwd"]
+    err = np.abs(out.astype(np.float64) - ref) / np.maximum(1.0, np.abs(ref))
+    inside = np.all((g["pts"] >= 0) & (g["pts"] <= 1), axis=1)
+    print("fp32 max err", err[inside].max())
+    assert err[inside].max() < 1e-5
+
+
+# ---------------------------------------------------------------- end to end
+
+
+def _prior_space(dim, nCs, tess, seed, precision=torch.float64):
+    sp = CpaSpace([0.0] * dim, [1.0] * dim, nCs, tess=tess, device=DEV, precision=precision)
+    rng = np.random.default_rng(seed)
+    theta = Prior.create(sp.geo, 0.1, 1.0).sample(4, rng)
+    return sp, theta, rng
+
+
+@pytest.mark.parametrize("dim,nCs,tess", [(1, (100,), "II"), (2, (4, 4), "I"), (3, (4, 4, 4), "I")])
+def test_theta_end_to_end(oracle_mod, dim, nCs, tess):
+    """theta -> A -> expm -> T(x) on the GPU vs the oracle with its own tables."""
+    O = oracle_mod
+    sp, theta, rng = _prior_space(dim, nCs, tess, 21)
+    dt, nT, nODE = 0.02, 50, 100
+    sA, Tr = sp.tables_from_theta(torch.as_tensor(theta, device=DEV), dt, 1)
+    x = rng.uniform(0, 1, size=(20000, dim))
+    t = O.tess_struct(dim, sp.geo.tess_code, nCs, sp.incs)
+    for i in range(theta.shape[0]):
+        A = sp.B_host @ theta[i]
+        np.testing.assert_allclose(sA[i].cpu().numpy(), A, rtol=1e-13, atol=1e-14)
+        osA, oTr = O.expm_cells(dim, A, dt, 1)
+        np.testing.assert_allclose(Tr[i].cpu().numpy(), oTr.reshape(-1), rtol=0, atol=1e-13)
+        xg = cuda(x)
+        out = torch.empty_like(xg)
+        c = sp._ctx
+        c.check(c.lib.cpab_calc_T(c.h, _lib.ptr(sA[i]), _lib.ptr(Tr[i]), _lib.ptr(xg), _lib.ptr(out), x.shape[0],
+                                  _lib.CPAB_F64, _lib.SCHEME_REF, dt, nT, nODE, None, _lib.stream_ptr()))
+        ref, _ = O.calc_T(t, oTr, osA, x, dt, nT, nODE)
+        if dim == 1:
+            ref = O.clamp_1d(ref)
+        diff = np.abs(out.cpu().numpy() - ref).max(axis=1)
+        # tables differ by ulps (CUDA vs libm exp): a point within ~1e-15 of a cell
+        # boundary may take the other branch ("flip"); count them, bound the rest
+        flips = int((diff > 1e-12).sum())
+        print(f"instance {i}: max diff {diff.max():.3e}, flips {flips}")
+        assert flips <= max(2, x.shape[0] // 5000)
+        assert np.median(diff) < 1e-14
+
+
+def test_calc_T_fwd_inv_api_round_trip():
+    sp, theta, rng = _prior_space(2, (4, 4), "I", 5)
+    sp.theta2Avees(theta[0])
+    sp.update_pat()
+    x = cuda(pixel_centers(128, 128))
+    y = torch.empty_like(x)
+    z = torch.empty_like(x)
+    p = dict(dt=0.02, nTimeSteps=50, nStepsODEsolver=100)
+    sp.calc_T_fwd(pts=x, out=y, **p)
+    sp.calc_T_inv(pts=y, out=z, **p)
+    assert (z - x).abs().max().item() < 1e-3
+    with pytest.raises(ValueError):
+        sp.calc_T_fwd(pts=x, out=x, **p)
+
+
+@pytest.mark.parametrize("precision", [torch.float64, torch.float32])
+def test_batched_uniform_and_ragged(oracle_mod, precision):
+    O = oracle_mod
+    sp, theta, rng = _prior_space(2, (4, 4), "I", 8, precision)
+    dt, nT, nODE = 0.02, 50, 100
+    tables = sp.tables_from_theta(torch.as_tensor(theta, device=DEV), dt, 1)
+    sA, Tr = (t.cpu().numpy() for t in tables)
+    t = O.tess_struct(2, 1, (4, 4), sp.incs)
+    sizes = [0, 1, 4097, 12345]          # an empty instance, a single point, ragged tails
+    offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    x = rng.uniform(0, 1, size=(offs[-1], 2))
+    xg = cuda(x, precision)
+    out = torch.empty_like(xg)
+    sp.calc_T_batched(tables, xg, out, offsets=torch.as_tensor(offs, device=DEV), dt=dt, nTimeSteps=nT,
+                      nStepsODEsolver=nODE)
+    got = out.cpu().numpy().astype(np.float64)
+    for i in range(4):
+        sl = slice(offs[i], offs[i + 1])
+        ref, _ = O.calc_T(t, Tr[i], sA[i], x[sl], dt, nT, nODE)
+        if precision == torch.float64:
+            np.testing.assert_array_equal(got[sl], ref)
+        else:
+            assert np.abs(got[sl] - ref).max(initial=0) < 1e-5
+    # uniform batch: 4 x 3000
+    xu = rng.uniform(0, 1, size=(4 * 3000, 2))
+    xg = cuda(xu, precision)
+    out = torch.empty_like(xg)
+    sp.calc_T_batched(tables, xg, out, dt=dt, nTimeSteps=nT, nStepsODEsolver=nODE)
+    got = out.cpu().numpy().astype(np.float64)
+    for i in range(4):
+        sl = slice(3000 * i, 3000 * (i + 1))
+        ref, _ = O.calc_T(t, Tr[i], sA[i], xu[sl], dt, nT, nODE)
+        if precision == torch.float64:
+            np.testing.assert_array_equal(got[sl], ref)
+        else:
+            assert np.abs(got[sl] - ref).max() < 1e-5
+
+
+@pytest.mark.parametrize("precision,tol", [(torch.float64, 1e-12), (torch.float32, 1e-6)])
+def test_exact_1d_vs_closed_form_oracle(oracle_mod, precision, tol):
+    O = oracle_mod
+    sp, theta, rng = _prior_space(1, (100,), "II", 13, precision)
+    sA, Tr = sp.tables_from_theta(torch.as_tensor(theta, device=DEV), 0.02, 1)
+    x = rng.uniform(0, 1, size=(50000, 1))
+    xg = cuda(x, precision)
+    for i in range(theta.shape[0]):
+        out = torch.empty_like(xg)
+        cnt = torch.zeros(_lib.CNT_N, dtype=torch.int64, device=DEV)
+        c = sp._ctx
+        c.check(c.lib.cpab_calc_T(c.h, _lib.ptr(sA[i]), _lib.ptr(Tr[i]), _lib.ptr(xg), _lib.ptr(out), x.shape[0],
+                                  _lib.CPAB_F64 if precision == torch.float64 else _lib.CPAB_F32, _lib.SCHEME_EXACT,
+                                  0.02, 50, 100, _lib.ptr(cnt), _lib.stream_ptr()))
+        xin = xg.cpu().numpy().astype(np.float64)[:, 0]
+        ref, nf = O.closed_form_1d(sA[i].cpu().numpy(), 100, xin, 1.0)
+        assert cnt[_lib.CNT_FAILED].item() == nf == 0
+        err = np.abs(out.cpu().numpy().astype(np.float64)[:, 0] - ref)
+        assert err.max() < tol, err.max()
+
+
+def test_full_size_c0_properties():
+    """2D nC=64, all 512x512 pixel centres: cell indices bit-exact to the
+    oracle, trajectory end == calc_T, inverse(forward) ~ identity."""
+    from oracle import oracle as O
+    sp, theta, rng = _prior_space(2, (4, 4), "I", 0)
+    x = pixel_centers(512, 512)
+    xg = cuda(x)
+    ci = torch.empty(x.shape[0], dtype=torch.int32, device=DEV)
+    sp.calc_cell_idx(xg, ci)
+    t = O.tess_struct(2, 1, (4, 4), sp.incs)
+    np.testing.assert_array_equal(ci.cpu().numpy(), O.calc_cell_idx(t, x))
+    sp.update_pat(sp.B @ torch.as_tensor(theta[0], device=DEV))
+    p = dict(dt=0.02, nTimeSteps=50, nStepsODEsolver=100)
+    y = torch.empty_like(xg)
+    sp.calc_T_fwd(pts=xg, out=y, **p)
+    traj = sp.calc_trajectory(pts=xg, **p)
+    torch.testing.assert_close(traj[-1], y, rtol=0, atol=0)
+    z = torch.empty_like(xg)
+    sp.calc_T_inv(pts=y, out=z, **p)
+    assert (z - xg).abs().max().item() < 1e-3
