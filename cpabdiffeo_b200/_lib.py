@@ -50,7 +50,9 @@ SIGNATURES = {
     "cpab_batched_workspace_bytes": (_sz, [_i]),
     "cpab_calc_T_batched": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _vp, _i64, _vp, _sz, _i, _i, _d, _i, _i, _vp, _vp]),
     "cpab_calc_trajectory": (_i, [_vp, _vp, _vp, _vp, _vp, _i64, _d, _i, _i, _vp]),
+    "cpab_calc_T_batched_noalloc": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _vp, _i64, _i, _i, _d, _i, _i, _vp, _vp]),
 }
+NOALLOC_MAX_INSTANCES = 65536
 
 _lib = None
 

@@ -307,3 +307,69 @@ int cpab_calc_trajectory(cpab_ctx *ctx, const double *signedA, const double *Tre
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free ragged batch (cpab_calc_T_batched_noalloc).
+//
+// Some callers cannot allocate device memory: a host application that owns
+// the whole device pool and hands plugins only their inputs and outputs, or a
+// latency-critical loop that must not pay for cudaMalloc's implicit
+// synchronisation.  For them the tile bookkeeping of a ragged batch lives in
+// this fixed array, compiled into the library.  Every GPU that loads the
+// library holds it (CPAB_NOALLOC_MAX_INSTANCES + 1 int64, 512 KiB) until the
+// process exits.  All calls share it and it keeps the last call's contents;
+// each call rewrites every entry it reads, so nothing needs clearing, but two
+// calls whose work overlaps on the GPU (different streams, or different host
+// threads) race on it.  Host code must not pass the array's name to a kernel:
+// outside device code that name is a host-side stand-in, not a device
+// address.  The device address is looked up once per device, with that device
+// current, on the first call made on it.
+#include <mutex>
+
+static __device__ __align__(256) int64_t g_noalloc_tile_prefix[CPAB_NOALLOC_MAX_INSTANCES + 1];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+int64_t *g_noalloc_addr[kNoallocMaxDevices] = {nullptr};
+}  // namespace
+
+static int noalloc_scratch(cpab_ctx *ctx, int64_t **out)
+{
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "cudaGetDevice");
+    if (dev < 0 || dev >= kNoallocMaxDevices)
+        return fail(ctx, CPAB_UNSUPPORTED, "device %d: the allocation-free entry point supports devices 0..%d", dev,
+                    kNoallocMaxDevices - 1);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_tile_prefix);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "cudaGetSymbolAddress(g_noalloc_tile_prefix)");
+        g_noalloc_addr[dev] = static_cast<int64_t *>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return CPAB_OK;
+}
+
+extern "C" int cpab_calc_T_batched_noalloc(cpab_ctx *ctx, const double *signedA, const double *Trels,
+                                           const void *pts, void *out, int N, const int64_t *offsets,
+                                           int64_t n_uniform, int precision, int scheme, double dt,
+                                           int nTimeSteps, int nStepsODE, uint64_t *counters, void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (N > CPAB_NOALLOC_MAX_INSTANCES)
+        return fail(ctx, CPAB_BAD_SHAPE,
+                    "cpab_calc_T_batched_noalloc accepts at most %d instances (got %d); "
+                    "use cpab_calc_T_batched with a workspace for larger batches",
+                    CPAB_NOALLOC_MAX_INSTANCES, N);
+    int64_t *scratch = nullptr;
+    if (offsets && N > 0) {
+        int st = noalloc_scratch(ctx, &scratch);
+        if (st != CPAB_OK) return st;
+    }
+    return cpab_calc_T_batched(ctx, signedA, Trels, pts, out, N, offsets, n_uniform, scratch,
+                               scratch ? sizeof(g_noalloc_tile_prefix) : 0, precision, scheme, dt, nTimeSteps,
+                               nStepsODE, counters, stream);
+}

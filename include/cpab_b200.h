@@ -144,6 +144,25 @@ int cpab_calc_T_batched(cpab_ctx *ctx, const double *signedA, const double *Trel
                         void *workspace, size_t workspace_bytes, int precision, int scheme,
                         double dt, int nTimeSteps, int nStepsODE, uint64_t *counters, void *stream);
 
+/* Largest N cpab_calc_T_batched_noalloc accepts. */
+#define CPAB_NOALLOC_MAX_INSTANCES 65536
+
+/* cpab_calc_T_batched without caller scratch: for callers that cannot
+ * allocate device memory (a host that owns the whole device pool and gives a
+ * plugin only its inputs and outputs, or a latency-critical loop that must not
+ * pay for cudaMalloc's implicit synchronisation).  The ragged-batch
+ * bookkeeping lives in a fixed device array inside the library (512 KiB per
+ * GPU that loads it, held until exit), so N is limited to
+ * CPAB_NOALLOC_MAX_INSTANCES (larger N -> CPAB_BAD_SHAPE).  Makes no
+ * allocation.  The first call on a device looks up the array's device
+ * address with that device current; make that first call before any stream
+ * capture.  Calls share the array: calls whose work overlaps on the GPU
+ * (other streams, other threads) race.  No counterpart in the reference. */
+int cpab_calc_T_batched_noalloc(cpab_ctx *ctx, const double *signedA, const double *Trels,
+                                const void *pts, void *out, int N, const int64_t *offsets, int64_t n_uniform,
+                                int precision, int scheme, double dt, int nTimeSteps, int nStepsODE,
+                                uint64_t *counters, void *stream);
+
 /* Trajectories (calc_trajectory, cpab/gpu/calc_2Dto2D.cu:499-556; host
  * cpab/cpaNd/_CpaCalcs.py:795-871): traj [(nTimeSteps+1), nPts, dim]
  * float64, row 0 = pts.  The reference supports 2D only; all dims here. */
