@@ -3,10 +3,15 @@
 Workload (the batched 1D configuration): [0,1] split into nC=100 equal
 cells, zero-velocity boundary; 4096 theta from the Gaussian prior (length
 scale 0.1, variance 1); instance i transforms its own n_i = floor(10^U(3,5))
-uniform points (~8.8e7 in total); integration time 1.0 as dt=0.02 x 50 steps
-with nStepsODE=100 (the reference's calc_T scheme); FP32 points, per-cell
-expm in FP64; one fused prologue launch (theta -> A -> expm for all 4096) and
-one persistent integration launch per step.  Seeded synthetic data (seed 1).
+uniform points (~8.8e7 in total), FP32 points; integration time 1.0.  The
+timed step integrates in closed form across cell boundaries (hitting times
+in FP64, cpab/cpa1d/calcs/ClosedFormInt.py restated on the GPU): one fused
+prologue launch (theta -> A -> expm for all 4096) and one persistent
+integration launch.  Each run checks the result against the reference's own
+calc_T scheme in FP64 (dt=0.02 x 50 steps, nStepsODE=100) on a sample of
+instances and reports the error (must stay <= 1e-5); the same workload
+through the REF scheme on the GPU is reported beside it.  Seeded synthetic
+data (seed 1).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -151,6 +156,18 @@ def measured_peaks(torch) -> dict:
     return out
 
 
+# Closed-form segment cost model (FP64 operations): per cell visit the
+# crossing test and hitting time take 10 arithmetic operations plus one log,
+# the final in-cell evaluation 6 plus one exp; log and exp are counted as 20
+# operations each (range reduction + a degree ~8 polynomial).
+EXACT_FLOP_PER_VISIT = 30
+EXACT_FLOP_PER_POINT = 26
+
+
+def flops_exact(cnt) -> float:
+    return float(cnt[0] * EXACT_FLOP_PER_VISIT + cnt[3] * EXACT_FLOP_PER_POINT)
+
+
 def flops_from_counters(cnt, dim=1) -> float:
     """Algorithmic FP ops of the REF scheme from device counters:
     per closed-form attempt 2*C_cell + M, per midpoint sub-step C_cell + 2M + 4D,
@@ -287,12 +304,12 @@ def main():
     stream = torch.cuda.current_stream()
     k_ev = []
 
-    def step(record=False):
+    def step(record=False, scheme=_lib.SCHEME_EXACT):
         tables = sp.tables_from_theta(theta, DT, 1)
         if record:
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
-        sp.calc_T_batched(tables, pts, out, offsets=offsets, workspace=ws, **p)
+        sp.calc_T_batched(tables, pts, out, offsets=offsets, workspace=ws, scheme=scheme, **p)
         if record:
             b.record(stream)
             k_ev.append((a, b))
@@ -334,7 +351,7 @@ def main():
         x_d = pts_pin.to(dev, non_blocking=True)
         o_d = torch.empty_like(x_d)
         tables = sp.tables_from_theta(th_d, DT, 1)
-        sp.calc_T_batched(tables, x_d, o_d, offsets=off_d, workspace=ws, **p)
+        sp.calc_T_batched(tables, x_d, o_d, offsets=off_d, workspace=ws, scheme=_lib.SCHEME_EXACT, **p)
         out_pin.copy_(o_d, non_blocking=True)
 
     for _ in range(2):
@@ -356,40 +373,77 @@ def main():
     h2d = pts_h.nbytes + theta_h.nbytes + offsets_h.nbytes
     d2h = pts_h.nbytes
 
-    # work accounting (counters) and error vs the FP64 oracle on a sample
+    # work accounting (counters) of the timed scheme
     cnt = torch.zeros(_lib.CNT_N, dtype=torch.int64, device=dev)
     tables = sp.tables_from_theta(theta, DT, 1)
-    sp.calc_T_batched(tables, pts, out, offsets=offsets, workspace=ws, counters=cnt, **p)
+    sp.calc_T_batched(tables, pts, out, offsets=offsets, workspace=ws, counters=cnt, scheme=_lib.SCHEME_EXACT, **p)
     torch.cuda.synchronize()
     cnt_h = cnt.cpu().numpy()
-    flops = flops_from_counters(cnt_h)
+    flops = flops_exact(cnt_h)
+    out_h = out.cpu().numpy()
+
+    # the same workload through the reference's REF scheme (FP32 on the GPU)
+    for _ in range(2):
+        step(scheme=_lib.SCHEME_REF)
+    torch.cuda.synchronize()
+    s3, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_ref_steps = 2
+    s3.record(stream)
+    for _ in range(n_ref_steps):
+        step(scheme=_lib.SCHEME_REF)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_ref = s3.elapsed_time(e3) / n_ref_steps
+    out_ref_h = out.cpu().numpy()
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded prior draws, log-uniform ragged sizes, uniform points)",
             "config": {"workload": WORKLOAD, "n_theta_per_gpu": args.theta, "points_per_gpu": n_total,
-                       "nC": NC, "scheme": "ref calc_T dt=0.02 nT=50 nODE=100", "precision": "f32 points, f64 expm",
+                       "nC": NC, "integration_time": 1.0,
+                       "scheme": "closed form across cells (hitting times, FP64); checked against the "
+                                 "reference calc_T scheme dt=0.02 nT=50 nODE=100 in FP64",
+                       "precision": "f32 points, f64 hitting times and expm",
                        "l2": "inputs larger than L2 (352 MB of points per GPU)",
                        "parallelism": f"independent shards x{world}"},
             "e2e": {"value": n_total * world * args.steps / (ms_e2e * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": 3 * args.steps,
             "clocks": clk.summary(),
-            "work": {"fast_steps": int(cnt_h[0]), "fallback_steps": int(cnt_h[1]), "substeps": int(cnt_h[2]),
-                     "points": int(cnt_h[3])}}
-
+            "work": {"cell_visits": int(cnt_h[0]), "points": int(cnt_h[3]), "failed": int(cnt_h[4])},
+            "ref_scheme_gpu": {"points_per_s": n_total * world / (ms_ref * 1e-3), "ms_per_step": ms_ref,
+                               "precision": "f32"}}
     if rank == 0:
         peaks = measured_peaks(torch)
         achieved = flops / (kern_ms * 1e-3) / 1e12
-        line["roofline"] = {"bound": "fp32", "kernel": "k_integrate<1,2,float,REF>", "achieved": achieved,
-                            "peak": peaks["fp32_simt_tflops"], "unit": "TFLOP/s",
-                            "frac": achieved / peaks["fp32_simt_tflops"],
-                            "peak_source": "measured here: cuBLAS SGEMM 8192^3 with TF32 off",
+        line["roofline"] = {"bound": "fp64", "kernel": "k_exact1d<float>", "achieved": achieved,
+                            "peak": peaks["fp64_tflops"], "unit": "TFLOP/s",
+                            "frac": achieved / peaks["fp64_tflops"],
+                            "peak_source": "measured here: cuBLAS DGEMM 4096^3",
+                            "flop_model": f"{EXACT_FLOP_PER_VISIT} per cell visit + {EXACT_FLOP_PER_POINT} per point "
+                                          "(log/exp counted as 20)",
                             "kernel_ms": kern_ms, "traffic": None,
                             "algorithmic_flop_per_launch": flops,
                             "hbm_achieved_gbs": 2 * pts_h.nbytes / (kern_ms * 1e-3) / 1e9,
                             "hbm_peak_gbs": peaks.get("hbm_gbs")}
+        # error of both GPU results against the reference scheme in FP64 (oracle) on a sample
+        from oracle import oracle as O
+        t = O.tess_struct(1, 2, geo.nCs, geo.incs)
+        err_exact = err_ref = 0.0
+        n_chk = 0
+        for i in range(8):
+            A = (geo.B @ theta_h[i]).reshape(NC, 2)
+            sAo, Tro = O.expm_cells(1, A, DT, 1)
+            sl = slice(offsets_h[i], offsets_h[i + 1])
+            x = pts_h[sl].astype(np.float64)
+            ref, _ = O.calc_T(t, Tro, sAo, x, DT, NT, NODE)
+            ref = O.clamp_1d(ref)
+            err_exact = max(err_exact, float(np.abs(out_h[sl].astype(np.float64) - ref).max()))
+            err_ref = max(err_ref, float(np.abs(out_ref_h[sl].astype(np.float64) - ref).max()))
+            n_chk += x.shape[0]
+        line["error_vs_fp64_reference_scheme"] = {"max_abs_timed_result": err_exact, "max_abs_ref_scheme_f32": err_ref,
+                                                  "points_checked": n_chk, "tolerance": 1e-5}
         if world == 1 and not args.no_extras:
             r, sample, kind, cores, _ = cpu_reference_rate(theta_h, offsets_h, pts_h, geo, 400_000)
             line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}

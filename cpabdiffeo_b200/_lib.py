@@ -51,6 +51,16 @@ SIGNATURES = {
     "cpab_calc_T_batched": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _vp, _i64, _vp, _sz, _i, _i, _d, _i, _i, _vp, _vp]),
     "cpab_calc_trajectory": (_i, [_vp, _vp, _vp, _vp, _vp, _i64, _d, _i, _i, _vp]),
     "cpab_calc_T_batched_noalloc": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _vp, _i64, _i, _i, _d, _i, _i, _vp, _vp]),
+    "cpab_remap_workspace_bytes": (_sz, [_i, _i, _i]),
+    "cpab_remap_ssd": (_i, [_vp, _vp, _i, _vp, _vp, _i, _i, _i, _d, _d, _d, _d, _d, _vp, _vp, _vp, _sz, _vp]),
+    "cpab_register_workspace_bytes": (_sz, [_vp, _i, _i, _i]),
+    "cpab_register_ll": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _i, _i, _d, _i, _d, _i, _i, _vp, _vp, _vp, _sz, _vp,
+                              _vp]),
+    "cpab_mcmc_propose": (_i, [_vp, _i, _i, _vp, _vp, _d, C.c_uint64, _vp, _vp, _vp]),
+    "cpab_mcmc_accept": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _d, _vp, _d, _vp, _i, C.c_uint64, _vp, _vp, _vp]),
+    "cpab_grad_workspace_bytes": (_sz, [_vp, _i, _i64, _i, _i]),
+    "cpab_grad_theta": (_i, [_vp, _vp, _i, _vp, _i, _vp, _i64, _vp, _d, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp,
+                             _sz, _vp]),
 }
 NOALLOC_MAX_INSTANCES = 65536
 

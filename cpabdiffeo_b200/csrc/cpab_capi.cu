@@ -1,58 +1,21 @@
 // cpab_capi.cu -- the extern "C" boundary declared in include/cpab_b200.h:
 // argument validation, status codes and error strings, launch dispatch.
-#include <cstdarg>
-#include <cstdio>
-#include <cstring>
 #include <cmath>
 #include <new>
 
-#include "../../include/cpab_b200.h"
-#include "cpab_internal.h"
-#include "cpab_launch.h"
+#include "cpab_ctx.h"
 
 using namespace cpab;
 
-struct cpab_ctx {
-    Tess t;
-    int nCs[3];
-    int clamp = 0;
-    double clamp_lo = 0, clamp_hi = 0;
-    LaunchCfg cfg;
-    char err[512] = {0};
-};
-
-static thread_local char g_thread_err[512];
-
-static int fail(cpab_ctx *ctx, int status, const char *fmt, ...)
-{
-    char *buf = ctx ? ctx->err : g_thread_err;
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(buf, 512, fmt, ap);
-    va_end(ap);
-    return status;
-}
-
-static int cuda_status(cpab_ctx *ctx, cudaError_t e, const char *what)
-{
-    if (e == cudaSuccess) return CPAB_OK;
-    return fail(ctx, CPAB_CUDA_ERROR, "%s: %s", what, cudaGetErrorString(e));
-}
-
-static inline int cell_len(const cpab_ctx *c) { return c->t.dim * (c->t.dim + 1); }
-
-static bool overlaps(const void *a, size_t na, const void *b, size_t nb)
-{
-    const char *pa = (const char *)a, *pb = (const char *)b;
-    return pa < pb + nb && pb < pa + na;
-}
+thread_local char cpab::g_thread_err[512];
 
 static size_t tables_smem(const cpab_ctx *c, int prec)
 {
-    return (size_t)2 * c->t.nC * cell_len(c) * (prec == CPAB_F64 ? 8 : 4);
+    // float64: A and T; float32: A and the (T - I) hi/lo pair
+    return (size_t)c->t.nC * cell_len(c) * (prec == CPAB_F64 ? 2 * 8 : 3 * 4);
 }
 
-static int max_smem_optin()
+int cpab::max_smem_optin()
 {
     static int v = 0;
     if (v == 0) {

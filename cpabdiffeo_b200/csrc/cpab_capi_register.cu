@@ -1,0 +1,295 @@
+// cpab_capi_register.cu -- C ABI of the remap / registration-likelihood
+// kernels (declared in include/cpab_b200.h).
+#include <cmath>
+
+#include "cpab_ctx.h"
+#include "cpab_register.h"
+
+using namespace cpab;
+
+namespace {
+
+constexpr int kRemapTilePx = 2048;
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+struct WsLayout {
+    size_t partials_off, tickets_off, total;
+};
+
+WsLayout ws_layout(int N, int64_t tiles_per_image)
+{
+    WsLayout w;
+    w.partials_off = 0;
+    w.tickets_off = align256((size_t)N * (size_t)tiles_per_image * sizeof(double));
+    w.total = w.tickets_off + align256((size_t)N * sizeof(unsigned));
+    return w;
+}
+
+int64_t tiles_of(int H, int W, int tile_px) { return ((int64_t)H * W + tile_px - 1) / tile_px; }
+
+int check_images(cpab_ctx *ctx, int N, int H, int W)
+{
+    if (N < 0) return fail(ctx, CPAB_BAD_SHAPE, "N < 0");
+    if (H < 1 || W < 1) return fail(ctx, CPAB_BAD_SHAPE, "image size %d x %d", H, W);
+    if ((int64_t)H * W > (int64_t)1 << 31) return fail(ctx, CPAB_BAD_SHAPE, "image too large");
+    return CPAB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t cpab_remap_workspace_bytes(int N, int H, int W)
+{
+    if (N < 0 || H < 1 || W < 1) return 0;
+    return ws_layout(N, tiles_of(H, W, kRemapTilePx)).total;
+}
+
+int cpab_remap_ssd(cpab_ctx *ctx, const void *map, int map_precision, const float *src, const float *dst, int N,
+                   int H, int W, double sx, double ox, double sy, double oy, double sigma, float *warped,
+                   double *ll, void *workspace, size_t workspace_bytes, void *stream)
+{
+    int st = check_images(ctx, N, H, W);
+    if (st != CPAB_OK) return st;
+    if (N == 0) return CPAB_OK;
+    if (map_precision != CPAB_F64 && map_precision != CPAB_F32)
+        return fail(ctx, CPAB_BAD_DTYPE, "map precision must be CPAB_F64 or CPAB_F32");
+    if (!map || !src) return fail(ctx, CPAB_BAD_ARG, "map/src is NULL");
+    if (!dst && !warped) return fail(ctx, CPAB_BAD_ARG, "nothing to compute: dst and warped are both NULL");
+    if (dst && !ll) return fail(ctx, CPAB_BAD_ARG, "ll is NULL (needed with dst)");
+    if (dst && !(sigma > 0) ) return fail(ctx, CPAB_BAD_ARG, "sigma must be positive");
+    if (!std::isfinite(sx) || !std::isfinite(ox) || !std::isfinite(sy) || !std::isfinite(oy))
+        return fail(ctx, CPAB_BAD_ARG, "pixel mapping is not finite");
+    const int64_t tpi = tiles_of(H, W, kRemapTilePx);
+    const WsLayout L = ws_layout(N, tpi);
+    RemapArgs a;
+    memset(&a, 0, sizeof(a));
+    a.map = map;
+    a.src = src;
+    a.dst = dst;
+    a.warped = warped;
+    a.ll = ll;
+    a.N = N;
+    a.H = H;
+    a.W = W;
+    a.tile_px = kRemapTilePx;
+    a.sx = sx;
+    a.ox = ox;
+    a.sy = sy;
+    a.oy = oy;
+    a.sigma = dst ? sigma : 1.0;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dst) {
+        if (!workspace || workspace_bytes < L.total)
+            return fail(ctx, CPAB_NO_MEMORY, "workspace of %zu bytes needed", L.total);
+        char *w = static_cast<char *>(workspace);
+        a.partials = reinterpret_cast<double *>(w + L.partials_off);
+        a.tickets = reinterpret_cast<unsigned *>(w + L.tickets_off);
+        cudaError_t e = cudaMemsetAsync(a.tickets, 0, (size_t)N * sizeof(unsigned), s);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "ticket reset");
+    }
+    return cuda_status(ctx, launch_remap_ssd(a, map_precision == CPAB_F64 ? PREC_F64 : PREC_F32, s),
+                       "remap_ssd launch");
+}
+
+size_t cpab_register_workspace_bytes(const cpab_ctx *ctx, int N, int H, int W)
+{
+    if (!ctx || N < 0 || H < 1 || W < 1) return 0;
+    return ws_layout(N, tiles_of(H, W, ctx->cfg.tile_pts)).total;
+}
+
+int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, int N, const float *src,
+                     const float *dst, int H, int W, double sigma, int precision, double dt, int nTimeSteps,
+                     int nStepsODE, double *ll, float *warped, void *workspace, size_t workspace_bytes,
+                     uint64_t *counters, void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (ctx->t.dim != 2) return fail(ctx, CPAB_UNSUPPORTED, "the registration likelihood is built for 2D spaces");
+    int st = check_images(ctx, N, H, W);
+    if (st != CPAB_OK) return st;
+    if (N == 0) return CPAB_OK;
+    if (precision != CPAB_F64 && precision != CPAB_F32)
+        return fail(ctx, CPAB_BAD_DTYPE, "precision must be CPAB_F64 or CPAB_F32");
+    if (!signedA || !Trels || !src || !dst || !ll) return fail(ctx, CPAB_BAD_ARG, "NULL argument");
+    if (!(sigma > 0)) return fail(ctx, CPAB_BAD_ARG, "sigma must be positive");
+    if (nTimeSteps < 1 || nStepsODE < 1) return fail(ctx, CPAB_BAD_ARG, "nTimeSteps and nStepsODE must be >= 1");
+    if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
+    if ((size_t)ctx->t.nC * 6 * (precision == CPAB_F64 ? 2 * 8 : 3 * 4) > (size_t)max_smem_optin())
+        return fail(ctx, CPAB_UNSUPPORTED, "cell tables exceed shared memory");
+    const int tile_px = ctx->cfg.tile_pts;
+    const WsLayout L = ws_layout(N, tiles_of(H, W, tile_px));
+    if (!workspace || workspace_bytes < L.total)
+        return fail(ctx, CPAB_NO_MEMORY, "workspace of %zu bytes needed", L.total);
+    RegisterArgs a;
+    memset(&a, 0, sizeof(a));
+    a.t = ctx->t;
+    a.A = signedA;
+    a.T = Trels;
+    a.src = src;
+    a.dst = dst;
+    a.warped = warped;
+    a.ll = ll;
+    char *w = static_cast<char *>(workspace);
+    a.partials = reinterpret_cast<double *>(w + L.partials_off);
+    a.tickets = reinterpret_cast<unsigned *>(w + L.tickets_off);
+    a.counters = reinterpret_cast<unsigned long long *>(counters);
+    a.N = N;
+    a.H = H;
+    a.W = W;
+    a.tile_px = tile_px;
+    a.sigma = sigma;
+    a.dt = dt;
+    a.nTimeSteps = nTimeSteps;
+    a.nStepsODE = nStepsODE;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(a.tickets, 0, (size_t)N * sizeof(unsigned), s);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "ticket reset");
+    return cuda_status(ctx, launch_register_ll(a, precision == CPAB_F64 ? PREC_F64 : PREC_F32, ctx->cfg, s),
+                       "register_ll launch");
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched Metropolis-Hastings steps (cpab/cpaNd/inference/Metropolis.py:41-85).
+#include "cpab_mcmc.h"
+
+namespace {
+
+int check_mcmc(cpab_ctx *ctx, int C, int d, const void *theta, const void *theta_prop, const void *step)
+{
+    if (C < 0 || d < 1) return fail(ctx, CPAB_BAD_SHAPE, "need C >= 0 chains and d >= 1");
+    if (C > 0 && (!theta || !theta_prop || !step)) return fail(ctx, CPAB_BAD_ARG, "theta/theta_prop/step is NULL");
+    return CPAB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cpab_mcmc_propose(cpab_ctx *ctx, int C, int d, const double *theta, const double *prop_std, double scale,
+                      uint64_t seed, const int64_t *step, double *theta_prop, void *stream)
+{
+    int st = check_mcmc(ctx, C, d, theta, theta_prop, step);
+    if (st != CPAB_OK) return st;
+    if (C == 0) return CPAB_OK;
+    if (!prop_std) return fail(ctx, CPAB_BAD_ARG, "prop_std is NULL");
+    if (!std::isfinite(scale)) return fail(ctx, CPAB_BAD_ARG, "scale is not finite");
+    McmcArgs a;
+    memset(&a, 0, sizeof(a));
+    a.C = C;
+    a.d = d;
+    a.theta = const_cast<double *>(theta);
+    a.theta_prop = theta_prop;
+    a.prop_std = prop_std;
+    a.scale = scale;
+    a.seed = seed;
+    a.step = const_cast<int64_t *>(step);
+    return cuda_status(ctx, launch_mcmc_propose(a, (cudaStream_t)stream), "mcmc_propose launch");
+}
+
+int cpab_mcmc_accept(cpab_ctx *ctx, int C, int d, double *theta, const double *theta_prop, double *ll,
+                     const double *ll_prop, double inv_npts, const double *prior_prec, double wlp, double *lp,
+                     int rule, uint64_t seed, int64_t *step, int64_t *n_accepted, void *stream)
+{
+    int st = check_mcmc(ctx, C, d, theta, theta_prop, step);
+    if (st != CPAB_OK) return st;
+    if (rule != 0 && rule != 1) return fail(ctx, CPAB_BAD_ARG, "rule must be 0 (reference) or 1 (textbook)");
+    if (prior_prec && !lp) return fail(ctx, CPAB_BAD_ARG, "lp is NULL (needed with prior_prec)");
+    if (C > 0) {
+        if (!ll || !ll_prop) return fail(ctx, CPAB_BAD_ARG, "ll/ll_prop is NULL");
+        McmcArgs a;
+        memset(&a, 0, sizeof(a));
+        a.C = C;
+        a.d = d;
+        a.theta = theta;
+        a.theta_prop = const_cast<double *>(theta_prop);
+        a.ll = ll;
+        a.ll_prop = ll_prop;
+        a.inv_npts = inv_npts;
+        a.prior_prec = prior_prec;
+        a.lp = lp;
+        a.wlp = wlp;
+        a.rule = rule;
+        a.seed = seed;
+        a.step = step;
+        a.n_accepted = n_accepted;
+        cudaError_t e = launch_mcmc_accept(a, (cudaStream_t)stream);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "mcmc_accept launch");
+    }
+    return cuda_status(ctx, step ? launch_mcmc_advance(step, (cudaStream_t)stream) : cudaSuccess,
+                       "mcmc_advance launch");
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Adjoint gradient of the midpoint scheme (cpab/gpu/calc_2Dto2D.cu:202-319,
+// 448-491 computes the same derivative forward; its binding is commented out
+// in cpab/gpu/Calcs.py:196).
+#include "cpab_grad.h"
+
+extern "C" {
+
+size_t cpab_grad_workspace_bytes(const cpab_ctx *ctx, int N, int64_t n_per_inst, int nTimeSteps, int ck)
+{
+    if (!ctx || N < 0 || n_per_inst < 0 || nTimeSteps < 1 || ck < 1) return 0;
+    const int64_t nck = (nTimeSteps + ck - 1) / ck;
+    return align256((size_t)nck * (size_t)N * (size_t)n_per_inst * ctx->t.dim * sizeof(double));
+}
+
+int cpab_grad_theta(cpab_ctx *ctx, const double *B, int d, const double *signedA, int N, const double *pts,
+                    int64_t n_per_inst, const double *grad_out, double dt, int nTimeSteps, int nStepsODE, int sign,
+                    int ck, double *out, double *grad_pts, double *gA, double *dtheta, void *workspace,
+                    size_t workspace_bytes, void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (N < 0 || n_per_inst < 0) return fail(ctx, CPAB_BAD_SHAPE, "N and n_per_inst must be >= 0");
+    if (N > 65535) return fail(ctx, CPAB_BAD_SHAPE, "at most 65535 instances per call (got %d)", N);
+    if (N == 0) return CPAB_OK;
+    if (!signedA || !gA) return fail(ctx, CPAB_BAD_ARG, "signedA/gA is NULL");
+    if (dtheta && (!B || d < 1)) return fail(ctx, CPAB_BAD_ARG, "dtheta needs the basis B and d >= 1");
+    if (n_per_inst > 0 && (!pts || !grad_out)) return fail(ctx, CPAB_BAD_ARG, "pts/grad_out is NULL");
+    if (nTimeSteps < 1 || nStepsODE < 1) return fail(ctx, CPAB_BAD_ARG, "nTimeSteps and nStepsODE must be >= 1");
+    if (nStepsODE > 256) return fail(ctx, CPAB_UNSUPPORTED, "the adjoint replays at most 256 sub-steps per step");
+    if (ck < 1) return fail(ctx, CPAB_BAD_ARG, "checkpoint stride must be >= 1");
+    if (sign != 1 && sign != -1) return fail(ctx, CPAB_BAD_ARG, "sign must be +1 or -1");
+    if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
+    if ((size_t)2 * ctx->t.nC * cell_len(ctx) * 8 > (size_t)max_smem_optin())
+        return fail(ctx, CPAB_UNSUPPORTED, "cell tables exceed shared memory");
+    const size_t need = cpab_grad_workspace_bytes(ctx, N, n_per_inst, nTimeSteps, ck);
+    if (n_per_inst > 0 && (!workspace || workspace_bytes < need))
+        return fail(ctx, CPAB_NO_MEMORY, "workspace of %zu bytes needed", need);
+    cudaStream_t s = (cudaStream_t)stream;
+    const int DA = ctx->t.nC * cell_len(ctx);
+    cudaError_t e = cudaMemsetAsync(gA, 0, (size_t)N * DA * sizeof(double), s);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "gA reset");
+    if (n_per_inst > 0) {
+        GradArgs a;
+        memset(&a, 0, sizeof(a));
+        a.t = ctx->t;
+        a.A = signedA;
+        a.pts = pts;
+        a.grad_out = grad_out;
+        a.out = out;
+        a.grad_in = grad_pts;
+        a.gA = gA;
+        a.ckpt = static_cast<double *>(workspace);
+        a.N = N;
+        a.n_per_inst = n_per_inst;
+        a.dt = dt;
+        a.nTimeSteps = nTimeSteps;
+        a.nStepsODE = nStepsODE;
+        a.ck = ck;
+        e = launch_grad_simple(a, s);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "grad launch");
+    }
+    if (dtheta) {
+        e = launch_bt_times(B, gA, dtheta, DA, d, N, (double)sign, s);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "B^T launch");
+    }
+    return CPAB_OK;
+}
+
+}  // extern "C"

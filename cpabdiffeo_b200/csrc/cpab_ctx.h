@@ -1,0 +1,52 @@
+// cpab_ctx.h -- the context behind the opaque cpab_ctx handle and the
+// error helpers shared by the C ABI files.
+#pragma once
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "../../include/cpab_b200.h"
+#include "cpab_internal.h"
+#include "cpab_launch.h"
+
+struct cpab_ctx {
+    cpab::Tess t;
+    int nCs[3];
+    int clamp = 0;
+    double clamp_lo = 0, clamp_hi = 0;
+    cpab::LaunchCfg cfg;
+    char err[512] = {0};
+};
+
+namespace cpab {
+
+extern thread_local char g_thread_err[512];
+
+inline int fail(cpab_ctx *ctx, int status, const char *fmt, ...)
+{
+    char *buf = ctx ? ctx->err : g_thread_err;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, 512, fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+inline int cuda_status(cpab_ctx *ctx, cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return CPAB_OK;
+    return fail(ctx, CPAB_CUDA_ERROR, "%s: %s", what, cudaGetErrorString(e));
+}
+
+inline int cell_len(const cpab_ctx *c) { return c->t.dim * (c->t.dim + 1); }
+
+inline bool overlaps(const void *a, size_t na, const void *b, size_t nb)
+{
+    const char *pa = (const char *)a, *pb = (const char *)b;
+    return pa < pb + nb && pb < pa + na;
+}
+
+int max_smem_optin();
+
+}  // namespace cpab

@@ -76,7 +76,7 @@ __device__ __forceinline__ double cf_phi(const Exact1D &e, int c, double x, doub
 
 // calc_phi for one point; returns false when the crossing cap is hit
 // (the reference raises ValueError, ClosedFormInt.py:155-160).
-__device__ bool cf_point(const Exact1D &e, double x, double t, int cap, double &out)
+__device__ bool cf_point(const Exact1D &e, double x, double t, int cap, double &out, unsigned long long &visits)
 {
     double x_old = x, x_new = x, t_rem = t;
     if (0 < x_old && x_old < 1) {
@@ -90,6 +90,7 @@ __device__ bool cf_point(const Exact1D &e, double x, double t, int cap, double &
         }
     }
     for (int counter = 0;;) {
+        ++visits;
         const int c = cf_cell(e, x_old);
         int cn;
         double tc = cf_crossing(e, x_old, c, cn);
@@ -116,7 +117,7 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
     const int nC = a.t.nC;
     const double T_total = a.dt * (double)a.nTimeSteps;
     const int64_t ntiles = total_tiles(a.batch);
-    unsigned long long c_pts = 0, c_fail = 0;
+    unsigned long long c_pts = 0, c_fail = 0, c_visits = 0;
     int loaded = -1;
     Exact1D e;
     e.A = sA;
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
             Real xin;
             load_pt<1, Real>(a.pts_in, i, &xin);
             double y;
-            bool ok = cf_point(e, (double)xin, T_total, cap, y);
+            bool ok = cf_point(e, (double)xin, T_total, cap, y, c_visits);
             if (a.clamp) y = clamp_ref(y, a.clamp_lo, a.clamp_hi);
             Real yo = (Real)y;
             store_pt<1, Real>(a.pts_out, i, &yo);
@@ -150,7 +151,9 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
     if (a.counters) {
         c_pts = warp_sum_u64(c_pts);
         c_fail = warp_sum_u64(c_fail);
+        c_visits = warp_sum_u64(c_visits);
         if ((threadIdx.x & 31) == 0) {
+            atomicAdd(a.counters + CNT_FAST, c_visits);  // cell visits (closed-form segments)
             atomicAdd(a.counters + CNT_POINTS, c_pts);
             atomicAdd(a.counters + CNT_FAILED, c_fail);
         }

@@ -15,38 +15,10 @@
 // Layout in HBM: points row-major [nPts, DIM] (the reference's layout);
 // per-instance tables [N, nC, DIM*(DIM+1)] float64; the current instance's
 // tables are staged in shared memory (converted to float in FP32 mode).
-#include "cpab_device.cuh"
+#include "cpab_integrate.cuh"
 #include "cpab_launch.h"
 
 namespace cpab {
-
-// ------------------------------------------------------------ arithmetic
-// The double instantiation is the bit-exact family; float is the fast one.
-
-template <int DIM, int TESS>
-__device__ __forceinline__ int cell_of(const Tess &t, const double *p) { return exact_cell<DIM, TESS>(t, p); }
-template <int DIM, int TESS>
-__device__ __forceinline__ int cell_of(const Tess &t, const float *p) { return fast_cell<DIM, TESS>(t, p); }
-
-template <int DIM>
-__device__ __forceinline__ void affine(double *x, const double *A, const double *b) { exact_affine<DIM>(x, A, b); }
-template <int DIM>
-__device__ __forceinline__ void affine(float *x, const float *A, const float *b) { fast_affine<DIM>(x, A, b); }
-
-template <int DIM>
-__device__ __forceinline__ void midpoint(double *p, const double *A, double h) { exact_midpoint<DIM>(p, A, h); }
-template <int DIM>
-__device__ __forceinline__ void midpoint(float *p, const float *A, float h)
-{
-    float v[DIM], pm[DIM];
-    fast_affine<DIM>(v, A, p);
-    const float hh = 0.5f * h;
-#pragma unroll
-    for (int i = 0; i < DIM; ++i) pm[i] = fmaf(hh, v[i], p[i]);
-    fast_affine<DIM>(v, A, pm);
-#pragma unroll
-    for (int i = 0; i < DIM; ++i) p[i] = fmaf(h, v[i], p[i]);
-}
 
 // tile_prefix[i] = sum_{j<i} ceil(n_j / tile_pts); one block, sequential
 // chunks per thread, then a block scan of the chunk sums.
@@ -79,81 +51,35 @@ __global__ void k_tile_prefix(const int64_t *offsets, int64_t *prefix, int N, in
 
 // ------------------------------------------------------------ integration
 
-// One warp integrates the points [ws, we).  Every lane owns one point and
-// advances it by one unit per iteration -- a closed-form Trel step or one
-// midpoint sub-step, which cost about the same -- and claims the next
-// unprocessed point of the range as soon as its own is finished.  A point
-// that falls back to 100 sub-steps therefore keeps one lane busy, not the
-// whole warp.  Results do not depend on the schedule: each point follows
-// exactly the reference's sequence of operations.
-template <int DIM, int TESS, typename Real, int SCHEME>
-__device__ __forceinline__ void integrate_range(const IntegrateArgs &a, const Real *sA, const Real *sT,
-                                                int64_t ws, int64_t we, Real h,
-                                                unsigned long long &c_fast, unsigned long long &c_fb,
-                                                unsigned long long &c_sub, unsigned long long &c_pts)
-{
-    constexpr int NE = DIM * (DIM + 1);
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    const int nT = a.nTimeSteps, nODE = a.nStepsODE;
-    int64_t next = ws + 32;
-    int64_t idx = ws + lane;
-    bool active = idx < we;
-    Real p[DIM];
-    int steps_left = 0, sub_left = 0;
-    if (active) {
-        load_pt<DIM, Real>(a.pts_in, idx, p);
-        steps_left = nT;
-        sub_left = (SCHEME == SCHEME_SIMPLE) ? nT * nODE : 0;
+template <int DIM>
+struct ArraySrc {
+    const void *base;
+    template <typename Real>
+    __device__ __forceinline__ void load(int64_t i, PState<DIM, Real> &st) const
+    {
+        Real p[DIM];
+        load_pt<DIM, Real>(base, i, p);
+        st.set(p);
     }
-    while (__any_sync(FULL, active)) {
-        bool fin = false;
-        if (active) {
-            int c = cell_of<DIM, TESS>(a.t, p);
-            if (SCHEME == SCHEME_REF && sub_left == 0) {
-                Real q[DIM];
-                affine<DIM>(q, sT + c * NE, p);
-                int cq = cell_of<DIM, TESS>(a.t, q);
-                if (cq == c) {
+};
+
+template <int DIM>
+struct ArraySnk {
+    void *base;
+    int clamp;
+    double lo, hi;
+    template <typename Real>
+    __device__ __forceinline__ void put(int64_t i, const PState<DIM, Real> &st)
+    {
+        Real p[DIM];
+        st.get(p);
+        if (clamp) {
 #pragma unroll
-                    for (int i = 0; i < DIM; ++i) p[i] = q[i];
-                    --steps_left;
-                    ++c_fast;
-                } else {
-                    sub_left = nODE;
-                    ++c_fb;
-                }
-            } else {
-                midpoint<DIM>(p, sA + c * NE, h);
-                --sub_left;
-                ++c_sub;
-                if (sub_left == 0) --steps_left;
-            }
-            fin = (SCHEME == SCHEME_SIMPLE) ? (sub_left == 0) : (steps_left == 0);
-            if (fin) {
-                if (a.clamp) {
-#pragma unroll
-                    for (int i = 0; i < DIM; ++i) p[i] = clamp_ref(p[i], a.clamp_lo, a.clamp_hi);
-                }
-                store_pt<DIM, Real>(a.pts_out, idx, p);
-                ++c_pts;
-            }
+            for (int k = 0; k < DIM; ++k) p[k] = clamp_ref(p[k], lo, hi);
         }
-        unsigned done = __ballot_sync(FULL, fin);
-        if (done) {
-            if (fin) {
-                idx = next + __popc(done & lt);
-                active = idx < we;
-                if (active) {
-                    load_pt<DIM, Real>(a.pts_in, idx, p);
-                    steps_left = nT;
-                    sub_left = (SCHEME == SCHEME_SIMPLE) ? nT * nODE : 0;
-                }
-            }
-            next += __popc(done);
-        }
+        store_pt<DIM, Real>(base, i, p);
     }
-}
+};
 
 template <int DIM, int TESS, typename Real, int SCHEME>
 __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
@@ -170,18 +96,16 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
     const int64_t ntiles = total_tiles(a.batch);
     unsigned long long c_fast = 0, c_fb = 0, c_sub = 0, c_pts = 0;
     int loaded = -1;
+    const ArraySrc<DIM> src{a.pts_in};
+    ArraySnk<DIM> snk{a.pts_out, a.clamp, a.clamp_lo, a.clamp_hi};
 
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         if (threadIdx.x == 0) s_tile = decode_tile(a.batch, tile);
         __syncthreads();
         const TileInfo ti = s_tile;
         if (ti.inst != loaded) {
-            const double *gA = a.A + (size_t)ti.inst * tab;
-            const double *gT = a.T + (size_t)ti.inst * tab;
-            for (int i = threadIdx.x; i < tab; i += blockDim.x) {
-                sA[i] = (Real)gA[i];
-                if (SCHEME == SCHEME_REF) sT[i] = (Real)gT[i];
-            }
+            stage_tables<DIM, Real>(a.A + (size_t)ti.inst * tab, a.T + (size_t)ti.inst * tab, a.t.nC,
+                                    SCHEME == SCHEME_REF, sA, sT);
             loaded = ti.inst;
             __syncthreads();
         }
@@ -190,7 +114,8 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
         int64_t ws = ti.start + warp * per, we = ws + per;
         if (we > ti.end) we = ti.end;
         if (ws < we)
-            integrate_range<DIM, TESS, Real, SCHEME>(a, sA, sT, ws, we, h, c_fast, c_fb, c_sub, c_pts);
+            integrate_range<DIM, TESS, Real, SCHEME>(a.t, a.nTimeSteps, a.nStepsODE, sA, sT, ws, we, h, src, snk,
+                                                     c_fast, c_fb, c_sub, c_pts);
         __syncthreads();
     }
     if (a.counters) {
@@ -455,7 +380,7 @@ template <int DIM, int TESS, typename Real, int SCHEME>
 static cudaError_t launch_integrate_t(const IntegrateArgs &a, const LaunchCfg &cfg, cudaStream_t s)
 {
     constexpr int NE = DIM * (DIM + 1);
-    size_t smem = (size_t)2 * a.t.nC * NE * sizeof(Real);
+    size_t smem = (size_t)(1 + TableLayout<Real>::kTParts) * a.t.nC * NE * sizeof(Real);
     auto kern = k_integrate<DIM, TESS, Real, SCHEME>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

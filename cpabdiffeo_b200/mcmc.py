@@ -1,0 +1,103 @@
+"""Batched Metropolis-Hastings image registration: C independent chains,
+each with its own (src, dst) image pair, advanced in lock-step on the GPU.
+
+One step per chain (cpab/cpaNd/inference/Metropolis.py:41-85,
+cpab/cpaNd/inference/Proposal.py:29-64):
+  theta' = theta + scale * sqrt(diag Sigma_CPA) * z
+  ll'    = registration log-likelihood of theta' (fused kernel, map never stored)
+  log_ratio = (ll' - ll) / nPts  [+ wlp * (lp' - lp)]
+  accept if log_ratio > 0, else by u ~ U(0,1) with the reference's own test
+  log(u) > log_ratio (rule="reference", the default) or the textbook test
+  log(u) < log_ratio (rule="standard").
+State (theta, ll, lp, acceptance counts, the step counter) stays on the GPU;
+several steps can be captured in one CUDA graph and replayed.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from .cpa_space import CpaSpace
+from .registration import GaussianLogLikelihood
+
+
+class BatchedMetropolis:
+    def __init__(self, ll: GaussianLogLikelihood, theta0: torch.Tensor, prop_std: np.ndarray, scale: float = 0.05,
+                 seed: int = 0, rule: str = "reference", use_ave_ll: bool = True,
+                 prior_precision: np.ndarray | None = None, wlp: float = 1.0):
+        self.ll_fn = ll
+        sp: CpaSpace = ll.space
+        self.space = sp
+        dev = sp.device
+        self.C = ll.N
+        self.d = sp.d
+        self.theta = torch.as_tensor(theta0, dtype=torch.float64, device=dev).reshape(self.C, self.d).clone()
+        self.theta_prop = torch.empty_like(self.theta)
+        self.prop_std = torch.as_tensor(np.asarray(prop_std, dtype=np.float64), device=dev).contiguous()
+        self.scale = float(scale)
+        self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        self.rule = {"reference": 0, "standard": 1}[rule]
+        self.inv_npts = 1.0 / ll.nPts if use_ave_ll else 1.0
+        self.prior_prec = (torch.as_tensor(prior_precision, dtype=torch.float64, device=dev).contiguous()
+                           if prior_precision is not None else None)
+        self.wlp = float(wlp)
+        self.step = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.n_accepted = torch.zeros(self.C, dtype=torch.int64, device=dev)
+        self.ll_prop = torch.empty(self.C, dtype=torch.float64, device=dev)
+        D = sp.D
+        self.sA = torch.empty((self.C, D), dtype=torch.float64, device=dev)
+        self.Tr = torch.empty_like(self.sA)
+        # current likelihood and prior
+        self.ll = ll.batch(self.theta).clone()
+        self.lp = None
+        if self.prior_prec is not None:
+            th = self.theta
+            self.lp = -0.5 * torch.einsum("ci,ij,cj->c", th, self.prior_prec, th)
+        self._graph = None
+        self._graph_steps = 0
+
+    def _step_launches(self) -> None:
+        sp, c = self.space, self.space._ctx
+        s = _lib.stream_ptr()
+        c.check(c.lib.cpab_mcmc_propose(c.h, self.C, self.d, _lib.ptr(self.theta), _lib.ptr(self.prop_std), self.scale,
+                                        self.seed, _lib.ptr(self.step), _lib.ptr(self.theta_prop), s))
+        c.check(c.lib.cpab_theta_to_trels(c.h, _lib.ptr(sp.B), self.d, _lib.ptr(self.theta_prop), self.C,
+                                          self.ll_fn.dt, -1, None, _lib.ptr(self.sA), _lib.ptr(self.Tr), s))
+        self.ll_fn.batch_tables((self.sA, self.Tr), ll=self.ll_prop)
+        c.check(c.lib.cpab_mcmc_accept(c.h, self.C, self.d, _lib.ptr(self.theta), _lib.ptr(self.theta_prop),
+                                       _lib.ptr(self.ll), _lib.ptr(self.ll_prop), self.inv_npts,
+                                       _lib.ptr(self.prior_prec), self.wlp, _lib.ptr(self.lp), self.rule, self.seed,
+                                       _lib.ptr(self.step), _lib.ptr(self.n_accepted), s))
+
+    def run(self, n_steps: int, graph_steps: int = 0) -> None:
+        """Advance every chain by n_steps.  graph_steps > 0 captures that many
+        steps in a CUDA graph (once) and replays it; the remainder runs eagerly."""
+        if graph_steps <= 0:
+            for _ in range(n_steps):
+                self._step_launches()
+            return
+        if self._graph is None or self._graph_steps != graph_steps:
+            # make sure every kernel attribute is set before capture
+            torch.cuda.synchronize()
+            g = torch.cuda.CUDAGraph()
+            saved = (self.theta.clone(), self.ll.clone(), self.step.clone(), self.n_accepted.clone(),
+                     None if self.lp is None else self.lp.clone())
+            with torch.cuda.graph(g):
+                for _ in range(graph_steps):
+                    self._step_launches()
+            # capture does not execute; restore to be safe
+            self.theta.copy_(saved[0]); self.ll.copy_(saved[1]); self.step.copy_(saved[2])
+            self.n_accepted.copy_(saved[3])
+            if self.lp is not None:
+                self.lp.copy_(saved[4])
+            self._graph, self._graph_steps = g, graph_steps
+        for _ in range(n_steps // graph_steps):
+            self._graph.replay()
+        for _ in range(n_steps % graph_steps):
+            self._step_launches()
+
+    def accept_ratio(self) -> np.ndarray:
+        """Percentage of accepted proposals per chain (Metropolis.py:84-85)."""
+        steps = int(self.step.item())
+        return self.n_accepted.cpu().numpy() * 100.0 / max(steps, 1)

@@ -170,6 +170,90 @@ int cpab_calc_trajectory(cpab_ctx *ctx, const double *signedA, const double *Tre
                          const double *pts, double *traj, int64_t nPts,
                          double dt, int nTimeSteps, int nStepsODE, void *stream);
 
+/* ------------------------------------------------------------------ images */
+
+/* Scratch bytes of cpab_remap_ssd for N images of H x W. */
+size_t cpab_remap_workspace_bytes(int N, int H, int W);
+
+/* Bilinear remap of N float32 images src [N, H, W] through maps [N, H*W, 2]
+ * (x, y per pixel; float64 or float32 per map_precision), with cv2.remap
+ * semantics -- x is the column, y the row, integer coordinates at pixel
+ * centres, taps outside the image read 0 (the remap of
+ * cpab/cpa2d/TransformWrapper.py:261-317, remap_fwd / remap_inv).  A map point
+ * (x, y) is sampled at pixel coordinates (x*sx + ox, y*sy + oy): (W, -0.5, H,
+ * -0.5) for points of the unit square, (1, 0, 1, 0) for pixel units.
+ * warped [N, H, W] float32 may be NULL when dst is given.  With dst [N, H, W]
+ * the same pass computes the Gaussian log-likelihood
+ *   ll[n] = sum_i -0.5 (warped_i - dst_i)^2 / sigma^2
+ * (cpab/cpa2d/model/transformations/register/gpu/gaussian.py:15-34 and the
+ * reduction of _ScaleDependentLogLikelihoodGeneral.py:108-131) in a fixed
+ * order (identical alone or batched).  workspace: cpab_remap_workspace_bytes.
+ * ctx may be NULL (errors then go to the thread's error string). */
+int cpab_remap_ssd(cpab_ctx *ctx, const void *map, int map_precision, const float *src, const float *dst,
+                   int N, int H, int W, double sx, double ox, double sy, double oy, double sigma,
+                   float *warped, double *ll, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Scratch bytes of cpab_register_ll for N image pairs of H x W. */
+size_t cpab_register_workspace_bytes(const cpab_ctx *ctx, int N, int H, int W);
+
+/* The registration log-likelihood of N (theta, src, dst) triples in one
+ * launch (ScaleDependentLogLikelihoodGaussian.calc_ll,
+ * cpab/cpa2d/model/transformations/register/_ScaleDependentLogLikelihoodGaussian.py:34-109):
+ * every pixel centre ((c+0.5)/W, (r+0.5)/H) of the unit square is integrated
+ * with instance n's tables (pass sign -1 tables for calc_T_inv, as the
+ * reference does), src[n] is sampled there (bilinear, as cpab_remap_ssd) and
+ * compared with dst[n]; ll[n] as in cpab_remap_ssd.  The transformed points
+ * are never written.  2D spaces; REF scheme; precision sets the integration
+ * arithmetic (CPAB_F64 bit-exact).  warped may be NULL. */
+int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, int N, const float *src,
+                     const float *dst, int H, int W, double sigma, int precision, double dt, int nTimeSteps,
+                     int nStepsODE, double *ll, float *warped, void *workspace, size_t workspace_bytes,
+                     uint64_t *counters, void *stream);
+
+/* ------------------------------------------------------------------ inference */
+
+/* Random-walk proposals for C chains (Proposal.__call__,
+ * cpab/cpaNd/inference/Proposal.py:29-64, diagonal covariance :61-64):
+ *   theta_prop[c] = theta[c] + scale * prop_std .* z,  z ~ N(0, I)
+ * z from Philox4x32-10 keyed by seed with counter (chain, *step, 0, pair),
+ * Box-Muller in double.  step: device int64 read by the kernel. */
+int cpab_mcmc_propose(cpab_ctx *ctx, int C, int d, const double *theta, const double *prop_std, double scale,
+                      uint64_t seed, const int64_t *step, double *theta_prop, void *stream);
+
+/* Accept/reject for C chains and advance *step by one (Metropolis.step,
+ * cpab/cpaNd/inference/Metropolis.py:41-85): log_ratio = (ll_prop - ll) *
+ * inv_npts (+ wlp * (lp' - lp) with the prior precision prior_prec [d, d]);
+ * accept when log_ratio > 0, else with u ~ U(0,1) (Philox stream 1):
+ * rule 0 accepts when log(u) > log_ratio -- the reference's own test
+ * (Metropolis.py:77-82) -- and rule 1 when log(u) < log_ratio (textbook MH).
+ * On accept theta, ll (and lp) take the proposal's values and n_accepted
+ * (may be NULL) counts it. */
+int cpab_mcmc_accept(cpab_ctx *ctx, int C, int d, double *theta, const double *theta_prop, double *ll,
+                     const double *ll_prop, double inv_npts, const double *prior_prec, double wlp, double *lp,
+                     int rule, uint64_t seed, int64_t *step, int64_t *n_accepted, void *stream);
+
+/* ------------------------------------------------------------------ gradient */
+
+/* Scratch bytes of cpab_grad_theta: checkpoints every ck time steps. */
+size_t cpab_grad_workspace_bytes(const cpab_ctx *ctx, int N, int64_t n_per_inst, int nTimeSteps, int ck);
+
+/* Gradient of a scalar loss of T(x) through the midpoint scheme
+ * (calc_T_simple semantics: nTimeSteps * nStepsODE sub-steps, the scheme whose
+ * derivative the reference's unbound calc_grad_theta carries forward,
+ * cpab/gpu/calc_2Dto2D.cu:202-319,448-491, cpab/cpaNd/_CpaSpace.py:669-686).
+ * N instances of n_per_inst points (pts, grad_out = dLoss/dT(x): [N*n, dim]
+ * float64); signedA [N, nC, ne] = sign * A.  Runs the forward again (out, may
+ * be NULL, receives T(x)), then the discrete adjoint backwards:
+ *   gA [N, nC*ne]      dLoss/d(signedA) (written; no accumulation across calls)
+ *   dtheta [N, d]      sign * B^T gA (NULL to skip; needs B [nC*ne, d])
+ *   grad_pts [N*n, dim] dLoss/dx (NULL to skip).
+ * ck: checkpoint stride in time steps (1 = fastest, nTimeSteps = least
+ * memory); workspace: cpab_grad_workspace_bytes.  nStepsODE <= 256. */
+int cpab_grad_theta(cpab_ctx *ctx, const double *B, int d, const double *signedA, int N, const double *pts,
+                    int64_t n_per_inst, const double *grad_out, double dt, int nTimeSteps, int nStepsODE, int sign,
+                    int ck, double *out, double *grad_pts, double *gA, double *dtheta, void *workspace,
+                    size_t workspace_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -515,9 +515,10 @@ int64_t oracle_closed_form_1d(const double *As, const double *x_tess, const doub
 
 /* Bilinear sample with cv2.remap conventions (x = column, y = row, integer
  * coordinates at pixel centres, taps outside the image read 0), the
- * semantics documented at cpab/cpa2d/TransformWrapper.py:286-317.  The map
- * holds points of the unit square; pixel coordinates are x*W - 0.5,
- * y*H - 0.5 (pixel centres at (i+0.5)/W). */
+ * semantics documented at cpab/cpa2d/TransformWrapper.py:286-317.  Map points
+ * become pixel coordinates px = x*sx + ox, py = y*sy + oy: (W, -0.5, H, -0.5)
+ * for points of the unit square with pixel centres at (i+0.5)/W, (1, 0, 1, 0)
+ * for the reference's pixel-unit domain. */
 static inline double tap(const float *img, int H, int W, int r, int c)
 {
     return (r >= 0 && r < H && c >= 0 && c < W) ? (double)img[(int64_t)r * W + c] : 0.0;
@@ -525,20 +526,21 @@ static inline double tap(const float *img, int H, int W, int r, int c)
 static inline double bilinear(const float *img, int H, int W, double px, double py)
 {
     double fx0 = floor(px), fy0 = floor(py);
-    double fx = px - fx0, fy = py - fy0;
-    int c0 = (int)fx0, r0 = (int)fy0;
     if (!(fx0 > -2.0 && fx0 < (double)W + 1.0 && fy0 > -2.0 && fy0 < (double)H + 1.0))
         return 0.0;
+    double fx = px - fx0, fy = py - fy0;
+    int c0 = (int)fx0, r0 = (int)fy0;
     double top = (1 - fx) * tap(img, H, W, r0, c0) + fx * tap(img, H, W, r0, c0 + 1);
     double bot = (1 - fx) * tap(img, H, W, r0 + 1, c0) + fx * tap(img, H, W, r0 + 1, c0 + 1);
     return (1 - fy) * top + fy * bot;
 }
 
-void oracle_remap(const double *map, const float *src, double *out, int H, int W)
+void oracle_remap(const double *map, const float *src, double *out, int H, int W,
+                  double sx, double ox, double sy, double oy)
 {
     #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)H * W; ++i)
-        out[i] = bilinear(src, H, W, map[2 * i] * W - 0.5, map[2 * i + 1] * H - 0.5);
+        out[i] = bilinear(src, H, W, map[2 * i] * sx + ox, map[2 * i + 1] * sy + oy);
 }
 
 /* Gaussian log-likelihood of the warped source against dst:
@@ -546,13 +548,13 @@ void oracle_remap(const double *map, const float *src, double *out, int H, int W
  * cpab/cpa2d/model/transformations/register/gpu/gaussian.py:15-34 and the
  * sum of _ScaleDependentLogLikelihoodGeneral.py:108-131.  Summed with
  * Kahan compensation in a fixed order. */
-double oracle_remap_ssd(const double *map, const float *src, const float *dst,
-                        int H, int W, double sigma, double *warped)
+double oracle_remap_ssd(const double *map, const float *src, const float *dst, int H, int W,
+                        double sx, double ox, double sy, double oy, double sigma, double *warped)
 {
     double s = 0, comp = 0;
     double k = -0.5 / (sigma * sigma);
     for (int64_t i = 0; i < (int64_t)H * W; ++i) {
-        double w = bilinear(src, H, W, map[2 * i] * W - 0.5, map[2 * i + 1] * H - 0.5);
+        double w = bilinear(src, H, W, map[2 * i] * sx + ox, map[2 * i + 1] * sy + oy);
         if (warped) warped[i] = w;
         double e = w - (double)dst[i];
         double term = e * e * k;

@@ -247,6 +247,109 @@ def ref_expm_1d(M) -> np.ndarray:
     return T
 
 
+def remap(map_pts, src, sx, ox, sy, oy) -> np.ndarray:
+    """warped [H, W] float64 from a map [H*W, 2] and a float32 image [H, W]."""
+    src = np.ascontiguousarray(src, dtype=np.float32)
+    H, W = src.shape
+    mp = _c64(map_pts)
+    out = np.empty(H * W)
+    lib().oracle_remap(_d(mp), src.ctypes.data_as(_fp), _d(out), C.c_int(H), C.c_int(W), C.c_double(sx),
+                       C.c_double(ox), C.c_double(sy), C.c_double(oy))
+    return out.reshape(H, W)
+
+
+def remap_ssd(map_pts, src, dst, sigma, sx, ox, sy, oy):
+    """(ll, warped) with ll = sum -0.5 (warped - dst)^2 / sigma^2 (Kahan sum)."""
+    src = np.ascontiguousarray(src, dtype=np.float32)
+    dst = np.ascontiguousarray(dst, dtype=np.float32)
+    H, W = src.shape
+    mp = _c64(map_pts)
+    warped = np.empty(H * W)
+    ll = lib().oracle_remap_ssd(_d(mp), src.ctypes.data_as(_fp), dst.ctypes.data_as(_fp), C.c_int(H), C.c_int(W),
+                                C.c_double(sx), C.c_double(ox), C.c_double(sy), C.c_double(oy),
+                                C.c_double(sigma), _d(warped))
+    return float(ll), warped.reshape(H, W)
+
+
+def register_ll(t: OracleTess, Trels_inv, sA_inv, src, dst, sigma, dt, nT, nODE):
+    """The registration log-likelihood of one image pair: the pixel centres
+    are mapped by T^-1 (tables with sign -1), src is sampled there and scored
+    against dst (cpab/cpa2d/model/transformations/register/
+    _ScaleDependentLogLikelihoodGaussian.py:34-109)."""
+    H, W = np.shape(src)
+    ys, xs = np.meshgrid((np.arange(H) + 0.5) / H, (np.arange(W) + 0.5) / W, indexing="ij")
+    grid = np.stack([xs.ravel(), ys.ravel()], axis=1)
+    pts, _ = calc_T(t, Trels_inv, sA_inv, grid, dt, nT, nODE)
+    return remap_ssd(pts, src, dst, sigma, W, -0.5, H, -0.5)
+
+
+# ------------------------------------------------------------------ MCMC (batched Metropolis)
+
+
+def philox4x32_10(c, key):
+    """Philox4x32-10 (Salmon et al., SC 2011) on uint32 arrays c[..., 4]; key (k0, k1)."""
+    M0, M1, W0, W1 = np.uint64(0xD2511F53), np.uint64(0xCD9E8D57), np.uint64(0x9E3779B9), np.uint64(0xBB67AE85)
+    mask = np.uint64(0xFFFFFFFF)
+    c = [np.asarray(c[..., i], dtype=np.uint64) for i in range(4)]
+    k0, k1 = np.uint64(key[0]), np.uint64(key[1])
+    for _ in range(10):
+        p0 = M0 * c[0]
+        p1 = M1 * c[2]
+        hi0, lo0 = p0 >> np.uint64(32), p0 & mask
+        hi1, lo1 = p1 >> np.uint64(32), p1 & mask
+        c = [(hi1 ^ c[1] ^ k0) & mask, lo1, (hi0 ^ c[3] ^ k1) & mask, lo0]
+        k0 = (k0 + W0) & mask
+        k1 = (k1 + W1) & mask
+    return np.stack(c, axis=-1).astype(np.uint32)
+
+
+def _u53(hi, lo):
+    m = (hi.astype(np.uint64) >> np.uint64(5)) << np.uint64(26) | (lo.astype(np.uint64) >> np.uint64(6))
+    return (m.astype(np.float64) + 0.5) * (1.0 / 9007199254740992.0)
+
+
+def mcmc_normals(seed: int, step: int, C: int, d: int) -> np.ndarray:
+    """z [C, d] of the proposal at `step` (stream 0), as the GPU draws them."""
+    pairs = (d + 1) // 2
+    ch, j = np.meshgrid(np.arange(C), np.arange(pairs), indexing="ij")
+    c = np.stack([ch, np.full_like(ch, step & 0xFFFFFFFF), np.full_like(ch, ((step >> 32) << 8) | 0), j], -1)
+    r = philox4x32_10(c.astype(np.uint64), (seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF))
+    u1, u2 = _u53(r[..., 0], r[..., 1]), _u53(r[..., 2], r[..., 3])
+    rad = np.sqrt(-2.0 * np.log(u1))
+    z = np.empty((C, 2 * pairs))
+    z[:, 0::2] = rad * np.cos(2 * np.pi * u2)
+    z[:, 1::2] = rad * np.sin(2 * np.pi * u2)
+    return z[:, :d]
+
+
+def mcmc_log_uniform(seed: int, step: int, C: int) -> np.ndarray:
+    ch = np.arange(C)
+    c = np.stack([ch, np.full_like(ch, step & 0xFFFFFFFF), np.full_like(ch, ((step >> 32) << 8) | 1),
+                  np.zeros_like(ch)], -1)
+    r = philox4x32_10(c.astype(np.uint64), (seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF))
+    return np.log(_u53(r[..., 0], r[..., 1]))
+
+
+def mcmc_run(B, ll_of_theta, theta0, prop_std, scale, seed, n_steps, inv_npts, rule=0):
+    """Batched Metropolis on the CPU with the GPU's random stream.
+    ll_of_theta(theta [C, d]) -> [C].  Returns (theta, ll, accepted [n_steps, C])."""
+    theta = np.array(theta0, dtype=np.float64, copy=True)
+    C, d = theta.shape
+    ll = ll_of_theta(theta)
+    acc = np.zeros((n_steps, C), dtype=bool)
+    for step in range(n_steps):
+        prop = theta + scale * prop_std[None, :] * mcmc_normals(seed, step, C, d)
+        llp = ll_of_theta(prop)
+        lr = (llp - ll) * inv_npts
+        lu = mcmc_log_uniform(seed, step, C)
+        a = (lr > 0) | ((lu > lr) if rule == 0 else (lu < lr))
+        a &= ~np.isnan(lr)
+        theta[a] = prop[a]
+        ll[a] = llp[a]
+        acc[step] = a
+    return theta, ll, acc
+
+
 def nproc() -> int:
     try:
         return len(os.sched_getaffinity(0))
