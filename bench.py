@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the cpu baseline and the 2D plain-vs-batched leg")
     ap.add_argument("--theta", type=int, default=N_THETA)
+    ap.add_argument("--serve-seconds", type=float, default=0.5,
+                    help="seconds of Poisson arrivals (2000 req/s) for the serving leg; 0 skips it")
     return ap.parse_args()
 
 
@@ -451,6 +453,16 @@ def main():
                 line["plain_vs_batched_2d"] = plain_vs_batched_2d(torch, dev)
             except Exception as ex:  # reported, never fatal
                 line["plain_vs_batched_2d"] = {"error": repr(ex)}
+            if args.serve_seconds > 0:
+                try:
+                    from cpabdiffeo_b200.serving_load import make_requests, run_load
+                    reqs = make_requests(2000.0, args.serve_seconds, seed=4)
+                    line["serving"] = dict(run_load(reqs, device=dev), arrival_rate_hz=2000.0,
+                                           arrivals_s=args.serve_seconds,
+                                           mix="1D/2D/3D, nC in {16,64,256,1024}, 1e3-4e6 pts, 10% 200-step "
+                                               "registrations (side 64-1024)")
+                except Exception as ex:
+                    line["serving"] = {"error": repr(ex)}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

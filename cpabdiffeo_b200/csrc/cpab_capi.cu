@@ -75,7 +75,7 @@ int cpab_set_launch(cpab_ctx *ctx, int block, int ctas_per_sm, int tile_pts)
     if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
     if (block && (block < 32 || block > 256 || block % 32))
         return fail(ctx, CPAB_BAD_ARG, "block must be a multiple of 32 in [32, 256] (got %d)", block);
-    if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(ctx, CPAB_BAD_ARG, "ctas_per_sm out of range");
+    if (ctas_per_sm < 0 || ctas_per_sm > 64) return fail(ctx, CPAB_BAD_ARG, "ctas_per_sm out of range");
     if (tile_pts < 0) return fail(ctx, CPAB_BAD_ARG, "tile_pts < 0");
     if (block) ctx->cfg.block = block;
     if (ctas_per_sm) ctx->cfg.ctas_per_sm = ctas_per_sm;
@@ -184,8 +184,8 @@ static int run_integrate(cpab_ctx *ctx, IntegrateArgs &a, int precision, int sch
                          cudaStream_t s)
 {
     LaunchCfg cfg = ctx->cfg;
-    int persistent = num_sms() * cfg.ctas_per_sm;
-    if (uniform_tiles_total > 0 && uniform_tiles_total < persistent) cfg.grid = (int)uniform_tiles_total;
+    // small uniform launches: one CTA per tile (the persistent grid would leave CTAs idle)
+    if (uniform_tiles_total > 0 && uniform_tiles_total < (int64_t)num_sms() * 2) cfg.grid = (int)uniform_tiles_total;
     cudaError_t e = (scheme == CPAB_SCHEME_EXACT) ? launch_integrate_exact1d(a, precision, cfg, s)
                                                    : launch_integrate(a, precision, scheme, cfg, s);
     return cuda_status(ctx, e, "integrate launch");

@@ -74,11 +74,43 @@ __device__ __forceinline__ double cf_phi(const Exact1D &e, int c, double x, doub
     return ea * x + b * (ea - 1) / a;
 }
 
+// Every visit after the first starts at a nudged vertex (x_k + 1e-12 when
+// entering cell k from the left, x_{k+1} - 1e-12 from the right), so its
+// hitting time depends on (cell, direction) only.  Those are evaluated once
+// per instance with the same function (cf_crossing) into shared memory:
+//   enter[0][k], enter[1][k]  entry point from the left / right,
+//   tc[0][k], nx[0][k]        hitting time and next cell from the left entry,
+//   tc[1][k], nx[1][k]        ... from the right entry.
+// The walk then reads the table; the results are those of evaluating
+// cf_crossing at every visit.
+struct Transit {
+    double *enter0, *enter1, *tc0, *tc1;
+    int *nx0, *nx1, *cell0, *cell1;
+};
+
+__device__ void build_transit(const Exact1D &e, Transit tr)
+{
+    for (int k = threadIdx.x; k < e.nC; k += blockDim.x) {
+        double x0 = fmin(1.0, fmax(0.0, vert(e, k) + 1e-12));
+        double x1 = fmin(1.0, fmax(0.0, vert(e, k + 1) - 1e-12));
+        tr.enter0[k] = x0;
+        tr.enter1[k] = x1;
+        int c0 = cf_cell(e, x0), c1 = cf_cell(e, x1), n0, n1;
+        tr.cell0[k] = c0;
+        tr.cell1[k] = c1;
+        tr.tc0[k] = cf_crossing(e, x0, c0, n0);
+        tr.nx0[k] = n0;
+        tr.tc1[k] = cf_crossing(e, x1, c1, n1);
+        tr.nx1[k] = n1;
+    }
+}
+
 // calc_phi for one point; returns false when the crossing cap is hit
 // (the reference raises ValueError, ClosedFormInt.py:155-160).
-__device__ bool cf_point(const Exact1D &e, double x, double t, int cap, double &out, unsigned long long &visits)
+__device__ bool cf_point(const Exact1D &e, const Transit &tr, double x, double t, int cap, double &out,
+                         unsigned long long &visits)
 {
-    double x_old = x, x_new = x, t_rem = t;
+    double x_old = x, t_rem = t;
     if (0 < x_old && x_old < 1) {
         // on a vertex with non-positive velocity: start just left of it
         double u = x_old * (double)e.nC;
@@ -89,32 +121,52 @@ __device__ bool cf_point(const Exact1D &e, double x, double t, int cap, double &
             if (!(vk > 0)) x_old = x_old - 1e-16;
         }
     }
+    // first visit: general position
+    int c = cf_cell(e, x_old), cn;
+    double tc = cf_crossing(e, x_old, c, cn);
     for (int counter = 0;;) {
         ++visits;
-        const int c = cf_cell(e, x_old);
-        int cn;
-        double tc = cf_crossing(e, x_old, c, cn);
-        bool crossed = true;
-        if (tc >= t_rem) { tc = t_rem; crossed = false; }
-        if (crossed) x_new = (cn > c) ? vert(e, cn) + 1e-12 : vert(e, c) - 1e-12;
-        else x_new = cf_phi(e, c, x_old, tc);
-        x_new = fmin(1.0, fmax(0.0, x_new));
+        if (tc >= t_rem) {
+            out = fmin(1.0, fmax(0.0, cf_phi(e, c, x_old, t_rem)));
+            return true;
+        }
         t_rem -= tc;
-        if (!crossed) break;
-        if (++counter >= cap) { out = x_new; return false; }
-        x_old = x_new;
+        if (++counter >= cap) {
+            // the point would have been left at the crossing it just made
+            out = (cn > c) ? tr.enter0[cn] : tr.enter1[cn];
+            return false;
+        }
+        // enter cell cn at the nudged vertex and read its transit from the table
+        if (cn > c) {
+            x_old = tr.enter0[cn];
+            c = tr.cell0[cn];
+            tc = tr.tc0[cn];
+            cn = tr.nx0[cn];
+        } else {
+            x_old = tr.enter1[cn];
+            c = tr.cell1[cn];
+            tc = tr.tc1[cn];
+            cn = tr.nx1[cn];
+        }
     }
-    out = x_new;
-    return true;
 }
 
 template <typename Real>
 __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *sA = reinterpret_cast<double *>(smem_raw);
-    __shared__ TileInfo s_tile;
     const int nC = a.t.nC;
+    double *sA = reinterpret_cast<double *>(smem_raw);
+    Transit tr;
+    tr.enter0 = sA + 2 * nC;
+    tr.enter1 = tr.enter0 + nC;
+    tr.tc0 = tr.enter1 + nC;
+    tr.tc1 = tr.tc0 + nC;
+    tr.nx0 = reinterpret_cast<int *>(tr.tc1 + nC);
+    tr.nx1 = tr.nx0 + nC;
+    tr.cell0 = tr.nx1 + nC;
+    tr.cell1 = tr.cell0 + nC;
+    __shared__ TileInfo s_tile;
     const double T_total = a.dt * (double)a.nTimeSteps;
     const int64_t ntiles = total_tiles(a.batch);
     unsigned long long c_pts = 0, c_fail = 0, c_visits = 0;
@@ -132,6 +184,8 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
         if (ti.inst != loaded) {
             const double *gA = a.A + (size_t)ti.inst * nC * 2;
             for (int i = threadIdx.x; i < nC * 2; i += blockDim.x) sA[i] = gA[i];
+            __syncthreads();
+            build_transit(e, tr);
             loaded = ti.inst;
             __syncthreads();
         }
@@ -139,7 +193,7 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
             Real xin;
             load_pt<1, Real>(a.pts_in, i, &xin);
             double y;
-            bool ok = cf_point(e, (double)xin, T_total, cap, y, c_visits);
+            bool ok = cf_point(e, tr, (double)xin, T_total, cap, y, c_visits);
             if (a.clamp) y = clamp_ref(y, a.clamp_lo, a.clamp_hi);
             Real yo = (Real)y;
             store_pt<1, Real>(a.pts_out, i, &yo);
@@ -162,14 +216,15 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
 
 cudaError_t launch_integrate_exact1d(const IntegrateArgs &a, int prec, const LaunchCfg &cfg, cudaStream_t s)
 {
-    size_t smem = (size_t)a.t.nC * 2 * sizeof(double);
-    int grid = cfg.grid > 0 ? cfg.grid : num_sms() * cfg.ctas_per_sm;
+    // A (2 doubles), entry points and hitting times (4 doubles), next cells and entry cells (4 ints)
+    size_t smem = (size_t)a.t.nC * (6 * sizeof(double) + 4 * sizeof(int));
     if (prec == PREC_F64) {
         auto kern = k_exact1d<double>;
         if (smem > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
+        int grid = cfg.grid > 0 ? cfg.grid : persistent_grid(kern, cfg, smem);
         kern<<<grid, cfg.block, smem, s>>>(a);
     } else {
         auto kern = k_exact1d<float>;
@@ -177,6 +232,7 @@ cudaError_t launch_integrate_exact1d(const IntegrateArgs &a, int prec, const Lau
             cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
+        int grid = cfg.grid > 0 ? cfg.grid : persistent_grid(kern, cfg, smem);
         kern<<<grid, cfg.block, smem, s>>>(a);
     }
     return cudaGetLastError();

@@ -15,6 +15,8 @@
 // Layout in HBM: points row-major [nPts, DIM] (the reference's layout);
 // per-instance tables [N, nC, DIM*(DIM+1)] float64; the current instance's
 // tables are staged in shared memory (converted to float in FP32 mode).
+#include <mutex>
+
 #include "cpab_integrate.cuh"
 #include "cpab_launch.h"
 
@@ -367,6 +369,37 @@ int num_sms()
     return g_num_sms;
 }
 
+// Persistent grid: SMs x resident CTAs of this kernel at this block size and
+// shared memory (capped by cfg.ctas_per_sm when that is smaller).
+// Occupancy queries are cached per (kernel, block, shared memory) so that a
+// launch inside stream capture makes no query.
+int persistent_grid_impl(const void *kern, const LaunchCfg &cfg, size_t smem)
+{
+    struct Key {
+        const void *k;
+        int block;
+        size_t smem;
+        int per_sm;
+    };
+    static Key cache[64];
+    static int n_cached = 0;
+    static std::mutex mu;
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        for (int i = 0; i < n_cached; ++i)
+            if (cache[i].k == kern && cache[i].block == cfg.block && cache[i].smem == smem) per_sm = cache[i].per_sm;
+        if (per_sm == 0) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, cfg.block, smem) != cudaSuccess ||
+                per_sm < 1)
+                per_sm = 1;
+            if (n_cached < 64) cache[n_cached++] = Key{kern, cfg.block, smem, per_sm};
+        }
+    }
+    if (cfg.ctas_per_sm > 0 && cfg.ctas_per_sm < per_sm) per_sm = cfg.ctas_per_sm;
+    return num_sms() * per_sm;
+}
+
 static int grid_for(int64_t n, int block, int per_sm = 8)
 {
     int64_t g = (n + block - 1) / block;
@@ -386,7 +419,7 @@ static cudaError_t launch_integrate_t(const IntegrateArgs &a, const LaunchCfg &c
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    int grid = cfg.grid > 0 ? cfg.grid : num_sms() * cfg.ctas_per_sm;
+    int grid = cfg.grid > 0 ? cfg.grid : persistent_grid(kern, cfg, smem);
     kern<<<grid, cfg.block, smem, s>>>(a);
     return cudaGetLastError();
 }

@@ -11,12 +11,18 @@ namespace cpab {
 // Launch shape of the integration kernel (chosen by the autotuner).
 struct LaunchCfg {
     int block = 256;       // threads per CTA (multiple of 32, <= 256)
-    int ctas_per_sm = 4;   // persistent grid = SMs * ctas_per_sm
+    int ctas_per_sm = 32;  // cap on resident CTAs per SM of the persistent grid (occupancy decides below it)
     int grid = 0;          // explicit grid (0 = persistent default)
     int tile_pts = 2048;   // points per CTA tile
 };
 
 int num_sms();
+int persistent_grid_impl(const void *kern, const LaunchCfg &cfg, size_t smem);
+template <typename K>
+inline int persistent_grid(K kern, const LaunchCfg &cfg, size_t smem)
+{
+    return persistent_grid_impl(reinterpret_cast<const void *>(kern), cfg, smem);
+}
 
 cudaError_t launch_integrate(const IntegrateArgs &a, int prec, int scheme, const LaunchCfg &cfg, cudaStream_t s);
 cudaError_t launch_integrate_exact1d(const IntegrateArgs &a, int prec, const LaunchCfg &cfg, cudaStream_t s);

@@ -221,7 +221,7 @@ static cudaError_t launch_register_t(const RegisterArgs &a, const LaunchCfg &cfg
     }
     const int64_t npx = (int64_t)a.H * a.W;
     const int64_t ntiles = ((npx + a.tile_px - 1) / a.tile_px) * a.N;
-    int64_t grid = (int64_t)num_sms() * cfg.ctas_per_sm;
+    int64_t grid = persistent_grid(kern, cfg, smem);
     if (grid > ntiles) grid = ntiles;
     kern<<<(unsigned)grid, cfg.block, smem, s>>>(a);
     return cudaGetLastError();

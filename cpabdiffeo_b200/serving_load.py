@@ -1,0 +1,90 @@
+"""Seeded open-loop load for the continuous-batching server: Poisson arrivals
+of a mixed request stream, replayed in real time; reports latency
+percentiles and throughput.
+
+Mix (the serving configuration): each request is 1D, 2D or 3D with equal
+probability and nC drawn from {16, 64, 256, 1024}, mapped to grids
+  1D: nC cells;  2D tess I: 2x2, 4x4, 8x8, 16x16 boxes (4 triangles each);
+  3D tess II: (4,2,2), (4,4,4), (8,8,4) and (8,8,8) boxes -- type II because
+  5 tetrahedra per box cannot make these counts; the largest uses 512 cells
+  instead of 1024 to keep the dense null-space construction of its basis
+  under a minute.
+Payload log-uniform in [1e3, 4e6] points (FP32); 10% of the requests are
+registration jobs (a float32 image pair, side uniform in [64, 1024], 200
+Metropolis steps); theta from the Gaussian prior.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import torch
+from scipy.ndimage import gaussian_filter
+
+from .serving import CpabServer, RegistrationRequest, TransformRequest
+from .space import Prior, build_space
+
+GRIDS = {
+    1: [((16,), "II"), ((64,), "II"), ((256,), "II"), ((1024,), "II")],
+    2: [((2, 2), "I"), ((4, 4), "I"), ((8, 8), "I"), ((16, 16), "I")],
+    3: [((4, 2, 2), "II"), ((4, 4, 4), "II"), ((8, 8, 4), "II"), ((8, 8, 8), "II")],
+}
+
+
+def make_requests(rate_hz: float, duration_s: float, seed: int = 4, max_points: float = 4e6,
+                  reg_fraction: float = 0.1, reg_steps: int = 200, max_side: int = 1024):
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    priors = {}
+    while True:
+        t += rng.exponential(1.0 / rate_hz)
+        if t > duration_s:
+            break
+        if rng.uniform() < reg_fraction:
+            side = int(rng.integers(64, max_side + 1))
+            src = gaussian_filter(rng.uniform(0, 1, (side, side)).astype(np.float32), 8.0)
+            dst = np.roll(src, 2, axis=1) + rng.normal(0, 0.02, (side, side)).astype(np.float32)
+            out.append((t, RegistrationRequest(src, dst, n_steps=reg_steps, seed=int(rng.integers(1 << 31)))))
+            continue
+        dim = int(rng.integers(1, 4))
+        nCs, tess = GRIDS[dim][int(rng.integers(0, 4))]
+        key = (dim, nCs, tess)
+        if key not in priors:
+            priors[key] = Prior.create(build_space(dim, nCs, tess), 0.1, 1.0)
+        theta = priors[key].sample(1, rng)[0]
+        n = int(10 ** rng.uniform(3, np.log10(max_points)))
+        pts = rng.uniform(0, 1, (n, dim)).astype(np.float32)
+        out.append((t, TransformRequest(dim, nCs, theta, pts, tess=tess)))
+    return out
+
+
+def run_load(requests, device=None, time_limit_s: float = 120.0) -> dict:
+    srv = CpabServer(device=device)
+    # warm the spaces (setup, not timed)
+    for _, r in requests:
+        if isinstance(r, TransformRequest):
+            srv.space(r.dim, r.nCs, r.tess, torch.float32)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    i = 0
+    while i < len(requests) or not srv.idle():
+        now = time.perf_counter() - t0
+        while i < len(requests) and requests[i][0] <= now:
+            srv.submit(requests[i][1], t_submit=t0 + requests[i][0])
+            i += 1
+        srv.step()
+        if now > time_limit_s:
+            break
+    wall = time.perf_counter() - t0
+    lat = np.asarray([r.t_done - r.t_submit for r in srv.done.values()])
+    pts = sum(int(np.asarray(r.req.pts).shape[0]) for r in srv.done.values() if isinstance(r.req, TransformRequest))
+    n_reg = sum(1 for r in srv.done.values() if isinstance(r.req, RegistrationRequest))
+    lat_t = np.asarray([r.t_done - r.t_submit for r in srv.done.values() if isinstance(r.req, TransformRequest)])
+    return {
+        "requests_submitted": len(requests), "requests_done": len(srv.done), "registrations_done": n_reg,
+        "wall_s": wall, "req_per_s": len(srv.done) / wall, "points_per_s": pts / wall,
+        "p50_ms": float(np.percentile(lat, 50) * 1e3) if lat.size else None,
+        "p99_ms": float(np.percentile(lat, 99) * 1e3) if lat.size else None,
+        "transform_p50_ms": float(np.percentile(lat_t, 50) * 1e3) if lat_t.size else None,
+        "transform_p99_ms": float(np.percentile(lat_t, 99) * 1e3) if lat_t.size else None,
+    }
