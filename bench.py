@@ -274,6 +274,99 @@ def plain_vs_batched_2d(torch, dev):
             "ratio": batched / plain}
 
 
+def other_configs(torch, dev) -> dict:
+    """Bounded measurements of the other configurations (device-timed, CUDA events)."""
+    from scipy.ndimage import gaussian_filter
+
+    from cpabdiffeo_b200.autograd import transform
+    from cpabdiffeo_b200.cpa_space import CpaSpace
+    from cpabdiffeo_b200.mcmc import BatchedMetropolis
+    from cpabdiffeo_b200.registration import GaussianLogLikelihood, remap
+    from cpabdiffeo_b200.space import Prior, pixel_centers
+    out = {}
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    p = dict(dt=DT, nTimeSteps=NT, nStepsODEsolver=NODE)
+
+    # 2D nC=64, single theta, FP64: 512x512 pixel centres forward and inverse, remap of a 512^2 image
+    sp = CpaSpace([0, 0], [1, 1], (4, 4), tess="I", device=dev)
+    rng = np.random.default_rng(0)
+    th = Prior.create(sp.geo, 0.1, 1.0).sample(1, rng)[0]
+    sp.update_pat(sp.B @ torch.as_tensor(th, device=dev))
+    x = torch.as_tensor(pixel_centers(512, 512), device=dev)
+    y, z = torch.empty_like(x), torch.empty_like(x)
+    img = torch.as_tensor(gaussian_filter(rng.uniform(0, 1, (512, 512)).astype(np.float32), 8.0), device=dev)
+    warped = torch.empty_like(img)
+    for _ in range(3):
+        sp.calc_T_fwd(pts=x, out=y, **p)
+        sp.calc_T_inv(pts=x, out=z, **p)
+        remap(z, img, out=warped, pixel_map=(512, -0.5, 512, -0.5))
+    a, b, c, d = ev(), ev(), ev(), ev()
+    a.record()
+    for _ in range(5):
+        sp.calc_T_fwd(pts=x, out=y, **p)
+    b.record()
+    for _ in range(5):
+        sp.calc_T_inv(pts=x, out=z, **p)
+    c.record()
+    for _ in range(5):
+        remap(z, img, out=warped, pixel_map=(512, -0.5, 512, -0.5))
+    d.record()
+    d.synchronize()
+    out["c0_2d_single_theta_f64"] = {"points": 262144, "fwd_ms": a.elapsed_time(b) / 5, "inv_ms": b.elapsed_time(c) / 5,
+                                     "remap_512sq_ms": c.elapsed_time(d) / 5,
+                                     "fwd_points_per_s": 262144 / (a.elapsed_time(b) / 5e3)}
+
+    # 3D nC=320 (4x4x4 tess I): forward + adjoint dL/dtheta, L = 0.5||T(x) - y||^2, 8 theta x 64^3 points (FP64)
+    sp3 = CpaSpace([0, 0, 0], [1, 1, 1], (4, 4, 4), tess="I", device=dev)
+    pr3 = Prior.create(sp3.geo, 0.15, 0.5)
+    th3 = torch.as_tensor(pr3.sample(8, rng), device=dev)
+    g = (np.arange(64) + 0.5) / 64
+    grid = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    x3 = torch.as_tensor(np.tile(grid, (8, 1)), device=dev)
+    with torch.no_grad():
+        y3 = transform(torch.as_tensor(pr3.sample(8, rng), device=dev), x3, sp3, **p)
+    t = th3.clone().requires_grad_(True)
+    for _ in range(2):
+        t.grad = None
+        (0.5 * ((transform(t, x3, sp3, **p) - y3) ** 2).sum()).backward()
+    a, b = ev(), ev()
+    a.record()
+    t.grad = None
+    (0.5 * ((transform(t, x3, sp3, **p) - y3) ** 2).sum()).backward()
+    b.record()
+    b.synchronize()
+    n3 = x3.shape[0]
+    out["c2_3d_fwd_adjoint_f64"] = {"theta": 8, "points_per_theta": 64 ** 3, "d": sp3.d,
+                                    "ms_fwd_plus_adjoint": a.elapsed_time(b),
+                                    "points_per_s": n3 / (a.elapsed_time(b) * 1e-3),
+                                    "scheme": "midpoint (calc_T_simple) forward, discrete adjoint"}
+
+    # batched MCMC registration: 256 chains x 256^2, FP32, steps captured in a CUDA graph
+    sp2 = CpaSpace([0, 0], [1, 1], (4, 4), tess="I", device=dev, precision=torch.float32)
+    pr2 = Prior.create(sp2.geo, 0.1, 1.0)
+    C, H = 256, 256
+    src = np.stack([gaussian_filter(rng.uniform(0, 1, (H, H)).astype(np.float32), 8.0) for _ in range(C)])
+    srcg = torch.as_tensor(src, device=dev)
+    warped = torch.empty_like(srcg)
+    GaussianLogLikelihood(sp2, srcg, srcg, 0.05, p).batch(torch.as_tensor(pr2.sample(C, rng), device=dev),
+                                                          warped=warped)
+    dst = warped + 0.02 * torch.randn_like(warped)
+    ll = GaussianLogLikelihood(sp2, srcg, dst, 0.05, p)
+    mh = BatchedMetropolis(ll, torch.zeros((C, sp2.d), device=dev), np.sqrt(np.diag(pr2.cov_cpa)), scale=0.05, seed=3)
+    mh.run(10, graph_steps=10)
+    torch.cuda.synchronize()
+    a, b = ev(), ev()
+    a.record()
+    mh.run(20, graph_steps=10)
+    b.record()
+    b.synchronize()
+    ms = a.elapsed_time(b) / 20
+    out["c3_mcmc_256chains_256sq_f32"] = {"ms_per_mh_step": ms, "mh_steps_per_s_all_chains": C / (ms * 1e-3),
+                                          "pixels_per_s": C * H * H / (ms * 1e-3),
+                                          "accept_pct_mean": float(mh.accept_ratio().mean())}
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -348,13 +441,9 @@ def main():
     off_pin = torch.from_numpy(offsets_h).pin_memory()
 
     def e2e_step():
-        th_d = th_pin.to(dev, non_blocking=True)
-        off_d = off_pin.to(dev, non_blocking=True)
-        x_d = pts_pin.to(dev, non_blocking=True)
-        o_d = torch.empty_like(x_d)
-        tables = sp.tables_from_theta(th_d, DT, 1)
-        sp.calc_T_batched(tables, x_d, o_d, offsets=off_d, workspace=ws, scheme=_lib.SCHEME_EXACT, **p)
-        out_pin.copy_(o_d, non_blocking=True)
+        # the public host-buffer entry point: chunked copy-in / integrate / copy-out on three streams
+        sp.calc_T_batched_host(th_pin, pts_pin, out_pin, offsets_h, mysign=1, scheme=_lib.SCHEME_EXACT, chunks=8,
+                               **p)
 
     for _ in range(2):
         e2e_step()
@@ -453,6 +542,10 @@ def main():
                 line["plain_vs_batched_2d"] = plain_vs_batched_2d(torch, dev)
             except Exception as ex:  # reported, never fatal
                 line["plain_vs_batched_2d"] = {"error": repr(ex)}
+            try:
+                line["other_configs"] = other_configs(torch, dev)
+            except Exception as ex:
+                line["other_configs"] = {"error": repr(ex)}
             if args.serve_seconds > 0:
                 try:
                     from cpabdiffeo_b200.serving_load import make_requests, run_load

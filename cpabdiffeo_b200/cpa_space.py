@@ -323,6 +323,82 @@ class CpaSpace:
                                           scheme, dt, nT, nODE, _lib.ptr(counters), _lib.stream_ptr()))
         return out
 
+    def calc_T_batched_host(self, theta, pts_host: torch.Tensor, out_host: torch.Tensor, offsets_host,
+                            mysign: int = 1, scheme: int = _lib.SCHEME_REF, chunks: int = 8,
+                            **params_flow_int) -> torch.cuda.Event:
+        """calc_T_batched for inputs and outputs in (pinned) HOST memory.
+
+        The batch is cut into `chunks` contiguous groups of instances with about
+        equal point counts; group k+1 is copied in while group k is integrated
+        and group k-1 is copied out (three streams, two device buffers).
+        theta: [N, d] (host or device); offsets_host: int64 [N+1] (host).
+        Returns an event recorded on the current stream once out_host is
+        complete; the current stream waits for it."""
+        dt, nT, nODE = self._flow(params_flow_int)
+        offs = np.asarray(offsets_host, dtype=np.int64)
+        N = offs.size - 1
+        dev = self.device
+        cur = torch.cuda.current_stream(dev)
+        if not hasattr(self, "_pipe_streams"):
+            self._pipe_streams = [torch.cuda.Stream(device=dev) for _ in range(3)]
+        s_in, s_cmp, s_out = self._pipe_streams
+        th = torch.as_tensor(theta, dtype=torch.float64)
+        th = th.pin_memory().to(dev, non_blocking=True) if th.device.type == "cpu" else th.to(dev)
+        tables = self.tables_from_theta(th, dt, mysign)
+        ev_tables = torch.cuda.Event()
+        ev_tables.record(cur)
+        total = int(offs[-1])
+        chunks = max(1, min(int(chunks), N))
+        # instance boundaries with about total/chunks points each
+        cuts = np.searchsorted(offs, np.linspace(0, total, chunks + 1)[1:-1])
+        bounds = np.unique(np.concatenate([[0], cuts, [N]]))
+        groups = [(int(a), int(b)) for a, b in zip(bounds[:-1], bounds[1:]) if b > a]
+        maxpts = max(int(offs[b] - offs[a]) for a, b in groups)
+        dim = self.dim
+        dt_ = pts_host.dtype
+        bufs = []
+        for _ in range(2):
+            bufs.append(dict(x=torch.empty((maxpts, dim), dtype=dt_, device=dev),
+                             o=torch.empty((maxpts, dim), dtype=dt_, device=dev),
+                             off=torch.empty(len(offs), dtype=torch.int64, device=dev),
+                             ws=torch.empty(int(self._ctx.lib.cpab_batched_workspace_bytes(N)) + 256,
+                                            dtype=torch.uint8, device=dev),
+                             ev_free=None))
+        off_pin = torch.empty((len(groups), len(offs)), dtype=torch.int64).pin_memory()
+        ev_last = None
+        for k, (a, b) in enumerate(groups):
+            buf = bufs[k % 2]
+            o0, o1 = int(offs[a]), int(offs[b])
+            n = o1 - o0
+            off_pin[k, :b - a + 1] = torch.from_numpy(offs[a:b + 1] - o0)
+            if buf["ev_free"] is not None:
+                s_in.wait_event(buf["ev_free"])
+            with torch.cuda.stream(s_in):
+                buf["x"][:n].copy_(pts_host[o0:o1], non_blocking=True)
+                buf["off"][:b - a + 1].copy_(off_pin[k, :b - a + 1], non_blocking=True)
+                ev_in = torch.cuda.Event()
+                ev_in.record(s_in)
+            s_cmp.wait_event(ev_in)
+            s_cmp.wait_event(ev_tables)
+            with torch.cuda.stream(s_cmp):
+                self.calc_T_batched((tables[0][a:b], tables[1][a:b]), buf["x"][:n], buf["o"][:n],
+                                    offsets=buf["off"][:b - a + 1], scheme=scheme, workspace=buf["ws"], **params_flow_int)
+                ev_c = torch.cuda.Event()
+                ev_c.record(s_cmp)
+            s_out.wait_event(ev_c)
+            with torch.cuda.stream(s_out):
+                out_host[o0:o1].copy_(buf["o"][:n], non_blocking=True)
+                ev_o = torch.cuda.Event()
+                ev_o.record(s_out)
+            buf["ev_free"] = ev_o
+            ev_last = ev_o
+        cur.wait_event(ev_last)
+        # keep the device buffers alive until the copies are done
+        self._pipe_keep = (bufs, tables, th, off_pin)
+        done = torch.cuda.Event()
+        done.record(cur)
+        return done
+
     def set_launch(self, block: int = 0, ctas_per_sm: int = 0, tile_pts: int = 0) -> None:
         c = self._ctx
         c.check(c.lib.cpab_set_launch(c.h, block, ctas_per_sm, tile_pts))

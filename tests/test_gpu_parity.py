@@ -269,3 +269,24 @@ def test_full_size_c0_properties():
     z = torch.empty_like(xg)
     sp.calc_T_inv(pts=y, out=z, **p)
     assert (z - xg).abs().max().item() < 1e-3
+
+
+@pytest.mark.parametrize("scheme", [_lib.SCHEME_EXACT, _lib.SCHEME_REF])
+def test_batched_host_pipeline_equals_device(scheme):
+    """calc_T_batched_host (pinned host buffers, chunked over three streams) ==
+    calc_T_batched on device buffers, bit for bit."""
+    sp, theta, rng = _prior_space(1, (100,), "II", 17, torch.float32)
+    theta = Prior.create(sp.geo, 0.1, 1.0).sample(37, rng)
+    sizes = rng.integers(0, 3000, size=37)
+    offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    x = rng.uniform(0, 1, size=(int(offs[-1]), 1)).astype(np.float32)
+    p = dict(dt=0.02, nTimeSteps=50, nStepsODEsolver=100)
+    xh = torch.from_numpy(x).pin_memory()
+    oh = torch.empty_like(xh).pin_memory()
+    sp.calc_T_batched_host(theta, xh, oh, offs, scheme=scheme, chunks=5, **p)
+    torch.cuda.synchronize()
+    tables = sp.tables_from_theta(torch.as_tensor(theta, device=DEV), 0.02, 1)
+    xd = cuda(x, torch.float32)
+    od = torch.empty_like(xd)
+    sp.calc_T_batched(tables, xd, od, offsets=torch.as_tensor(offs, device=DEV), scheme=scheme, **p)
+    np.testing.assert_array_equal(oh.numpy(), od.cpu().numpy())
