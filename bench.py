@@ -230,6 +230,7 @@ def plain_vs_batched_2d(torch, dev):
     """North-star comparison on the 2D nC=64 workload: FP32 batched (one launch
     for all theta) vs the plain path (one theta per call: host A = B theta,
     expm launch, calc_T launch, stream sync), 4096 points per theta."""
+    from cpabdiffeo_b200 import _lib
     from cpabdiffeo_b200.cpa_space import CpaSpace
     from cpabdiffeo_b200.space import Prior
     sp64 = CpaSpace([0, 0], [1, 1], (4, 4), tess="I", device=dev, precision=torch.float64)
@@ -255,6 +256,9 @@ def plain_vs_batched_2d(torch, dev):
     xb = torch.as_tensor(x, device=dev, dtype=torch.float32)
     ob = torch.empty_like(xb)
     th = torch.as_tensor(theta, device=dev)
+
+    from cpabdiffeo_b200 import autotune
+    autotune.tune(sp32, sp32.tables_from_theta(th, DT, 1), xb, None, _lib.SCHEME_REF, sample_points=1 << 20, **p)
 
     def step():
         tables = sp32.tables_from_theta(th, DT, 1)
@@ -413,6 +417,8 @@ def main():
         if world > 1:
             dist.barrier()
 
+    from cpabdiffeo_b200 import autotune
+    tuned = autotune.tune(sp, sp.tables_from_theta(theta, DT, 1), pts, offsets, _lib.SCHEME_EXACT, **p)
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
@@ -428,10 +434,8 @@ def main():
     barrier()
     ms = s.elapsed_time(e)
     kern_ms = float(np.mean([a.elapsed_time(b) for a, b in k_ev]))
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    from cpabdiffeo_b200.distributed import max_over_ranks
+    ms = max_over_ranks(ms, dev)
     value = n_total * world * args.steps / (ms * 1e-3)
 
     # end to end through the public API, host buffers (pinned), copies inside the timed region
@@ -457,10 +461,7 @@ def main():
     torch.cuda.synchronize()
     barrier()
     ms_e2e = s2.elapsed_time(e2)
-    if world > 1:
-        t = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = max_over_ranks(ms_e2e, dev)
     h2d = pts_h.nbytes + theta_h.nbytes + offsets_h.nbytes
     d2h = pts_h.nbytes
 
@@ -473,15 +474,18 @@ def main():
     flops = flops_exact(cnt_h)
     out_h = out.cpu().numpy()
 
-    # the same workload through the reference's REF scheme (FP32 on the GPU)
-    for _ in range(2):
-        step(scheme=_lib.SCHEME_REF)
+    # the same workload through the reference's REF scheme (FP32 on the GPU), its own tuned launch shape
+    sp_ref = CpaSpace([0.0], [1.0], (NC,), device=dev, precision=torch.float32)
+    tab_ref = sp_ref.tables_from_theta(theta, DT, 1)
+    tuned_ref = autotune.tune(sp_ref, tab_ref, pts, offsets, _lib.SCHEME_REF, sample_points=2_000_000, **p)
+    sp_ref.calc_T_batched(tab_ref, pts, out, offsets=offsets, workspace=ws, scheme=_lib.SCHEME_REF, **p)
     torch.cuda.synchronize()
     s3, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     n_ref_steps = 2
     s3.record(stream)
     for _ in range(n_ref_steps):
-        step(scheme=_lib.SCHEME_REF)
+        tab_ref = sp_ref.tables_from_theta(theta, DT, 1)
+        sp_ref.calc_T_batched(tab_ref, pts, out, offsets=offsets, workspace=ws, scheme=_lib.SCHEME_REF, **p)
     e3.record(stream)
     torch.cuda.synchronize()
     ms_ref = s3.elapsed_time(e3) / n_ref_steps
@@ -504,7 +508,8 @@ def main():
             "clocks": clk.summary(),
             "work": {"cell_visits": int(cnt_h[0]), "points": int(cnt_h[3]), "failed": int(cnt_h[4])},
             "ref_scheme_gpu": {"points_per_s": n_total * world / (ms_ref * 1e-3), "ms_per_step": ms_ref,
-                               "precision": "f32"}}
+                               "precision": "f32", "launch": tuned_ref},
+            "launch": tuned}
     if rank == 0:
         peaks = measured_peaks(torch)
         achieved = flops / (kern_ms * 1e-3) / 1e12

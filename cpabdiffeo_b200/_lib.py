@@ -42,6 +42,7 @@ SIGNATURES = {
     "cpab_ctx_cell_len": (_i, [_vp]),
     "cpab_set_clamp": (_i, [_vp, _i, _d, _d]),
     "cpab_set_launch": (_i, [_vp, _i, _i, _i]),
+    "cpab_set_cell_sort": (_i, [_vp, _i]),
     "cpab_expm": (_i, [_vp, _vp, _i, _d, _i, _vp, _vp, _vp]),
     "cpab_theta_to_trels": (_i, [_vp, _vp, _i, _vp, _i, _d, _i, _vp, _vp, _vp, _vp]),
     "cpab_calc_cell_idx": (_i, [_vp, _vp, _vp, _i64, _vp]),

@@ -399,9 +399,11 @@ class CpaSpace:
         done.record(cur)
         return done
 
-    def set_launch(self, block: int = 0, ctas_per_sm: int = 0, tile_pts: int = 0) -> None:
+    def set_launch(self, block: int = 0, ctas_per_sm: int = 0, tile_pts: int = 0, cell_sort: bool | None = None) -> None:
         c = self._ctx
         c.check(c.lib.cpab_set_launch(c.h, block, ctas_per_sm, tile_pts))
+        if cell_sort is not None:
+            c.check(c.lib.cpab_set_cell_sort(c.h, int(bool(cell_sort))))
 
     def __repr__(self) -> str:
         return self.geo.subspace_string

@@ -83,6 +83,13 @@ int cpab_set_launch(cpab_ctx *ctx, int block, int ctas_per_sm, int tile_pts)
     return CPAB_OK;
 }
 
+int cpab_set_cell_sort(cpab_ctx *ctx, int enable)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    ctx->cfg.sort = enable ? 1 : 0;
+    return CPAB_OK;
+}
+
 int cpab_expm(cpab_ctx *ctx, const double *A, int N, double dt, int sign, double *signedA, double *Trels,
               void *stream)
 {
@@ -154,8 +161,10 @@ static int check_integrate(cpab_ctx *ctx, const double *signedA, const double *T
     size_t bytes = (size_t)nPts * ctx->t.dim * (precision == CPAB_F64 ? 8 : 4);
     if (nPts > 0 && overlaps(pts, bytes, out, bytes))
         return fail(ctx, CPAB_ALIAS, "pts and out cannot point to the same memory (_CpaCalcs.py:388)");
-    if (tables_smem(ctx, precision) > (size_t)max_smem_optin())
-        return fail(ctx, CPAB_UNSUPPORTED, "cell tables (%zu bytes) exceed shared memory", tables_smem(ctx, precision));
+    size_t need = tables_smem(ctx, precision);
+    if (ctx->cfg.sort) need += ((size_t)ctx->t.nC + 2 * (size_t)ctx->cfg.tile_pts) * sizeof(int);
+    if (need > (size_t)max_smem_optin())
+        return fail(ctx, CPAB_UNSUPPORTED, "cell tables and tile scratch (%zu bytes) exceed shared memory", need);
     return CPAB_OK;
 }
 
@@ -177,6 +186,7 @@ static IntegrateArgs make_args(cpab_ctx *ctx, const double *signedA, const doubl
     a.clamp_hi = ctx->clamp_hi;
     a.counters = reinterpret_cast<unsigned long long *>(counters);
     a.max_crossings = 4 * ctx->t.nC + 8;
+    a.sort = ctx->cfg.sort;
     return a;
 }
 

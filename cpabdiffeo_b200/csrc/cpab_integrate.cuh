@@ -125,18 +125,22 @@ __device__ __forceinline__ int cell_of(const Tess &t, const PState<DIM, float> &
 
 // Closed-form step with the table of cell c; kept (returns true) if the end
 // point is still in cell c.
+// cq receives the cell of the end point (equal to c when kept).
 template <int DIM, int TESS>
-__device__ __forceinline__ bool try_fast(const Tess &t, PState<DIM, double> &s, const double *T, int tab, int c)
+__device__ __forceinline__ bool try_fast(const Tess &t, PState<DIM, double> &s, const double *T, int tab, int c,
+                                         int &cq)
 {
     double q[DIM];
     exact_affine<DIM>(q, T + c * DIM * (DIM + 1), s.p);
-    if (exact_cell<DIM, TESS>(t, q) != c) return false;
+    cq = exact_cell<DIM, TESS>(t, q);
+    if (cq != c) return false;
 #pragma unroll
     for (int i = 0; i < DIM; ++i) s.p[i] = q[i];
     return true;
 }
 template <int DIM, int TESS>
-__device__ __forceinline__ bool try_fast(const Tess &t, PState<DIM, float> &s, const float *T, int tab, int c)
+__device__ __forceinline__ bool try_fast(const Tess &t, PState<DIM, float> &s, const float *T, int tab, int c,
+                                         int &cq)
 {
     constexpr int NH = DIM + 1;
     const float *Th = T + c * DIM * NH, *Tl = Th + tab;
@@ -155,7 +159,8 @@ __device__ __forceinline__ bool try_fast(const Tess &t, PState<DIM, float> &s, c
         q.lo[r] = s.lo[r];
         acc_add(q.hi[r], q.lo[r], d);
     }
-    if (fast_cell<DIM, TESS>(t, q.hi) != c) return false;
+    cq = fast_cell<DIM, TESS>(t, q.hi);
+    if (cq != c) return false;
     s = q;
     return true;
 }
@@ -189,21 +194,28 @@ __device__ __forceinline__ void substep(PState<DIM, float> &s, const float *A, f
 // exactly the reference's sequence of operations.
 //   Src::load(idx, st)     sets the start state of point idx
 //   Snk::put(idx, st)      receives the end state (PState; get() converts)
+//   perm (optional, shared memory): the k-th point of the range is
+//   ws_base + perm[k - ws_base] (a cell-sorted order inside the tile).
+// The reference recomputes the start cell of every time step; after a kept
+// closed-form step that cell was just computed for the same point, so it is
+// reused (identical value, one lookup per step saved).
 template <int DIM, int TESS, typename Real, int SCHEME, class Src, class Snk>
 __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE, const Real *sA, const Real *sT,
                                                 int64_t ws, int64_t we, Real h, const Src &src, Snk &snk,
                                                 unsigned long long &c_fast, unsigned long long &c_fb,
-                                                unsigned long long &c_sub, unsigned long long &c_pts)
+                                                unsigned long long &c_sub, unsigned long long &c_pts,
+                                                const int *perm = nullptr, int64_t perm_base = 0)
 {
     constexpr int NE = DIM * (DIM + 1);
     const int tab = t.nC * NE;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     int64_t next = ws + 32;
-    int64_t idx = ws + lane;
-    bool active = idx < we;
+    int64_t k = ws + lane;
+    bool active = k < we;
+    int64_t idx = (active && perm) ? perm_base + perm[k - perm_base] : k;
     PState<DIM, Real> st;
-    int steps_left = 0, sub_left = 0;
+    int steps_left = 0, sub_left = 0, known_cell = -1;
     if (active) {
         src.load(idx, st);
         steps_left = nT;
@@ -212,16 +224,20 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
     while (__any_sync(FULL, active)) {
         bool fin = false;
         if (active) {
-            int c = cell_of<DIM, TESS>(t, st);
             if (SCHEME == SCHEME_REF && sub_left == 0) {
-                if (try_fast<DIM, TESS>(t, st, sT, tab, c)) {
+                const int c = known_cell >= 0 ? known_cell : cell_of<DIM, TESS>(t, st);
+                int cq;
+                if (try_fast<DIM, TESS>(t, st, sT, tab, c, cq)) {
                     --steps_left;
                     ++c_fast;
+                    known_cell = cq;
                 } else {
                     sub_left = nODE;
                     ++c_fb;
+                    known_cell = -1;
                 }
             } else {
+                const int c = cell_of<DIM, TESS>(t, st);
                 substep<DIM>(st, sA + c * NE, h);
                 --sub_left;
                 ++c_sub;
@@ -236,12 +252,14 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
         unsigned done = __ballot_sync(FULL, fin);
         if (done) {
             if (fin) {
-                idx = next + __popc(done & lt);
-                active = idx < we;
+                k = next + __popc(done & lt);
+                active = k < we;
                 if (active) {
+                    idx = perm ? perm_base + perm[k - perm_base] : k;
                     src.load(idx, st);
                     steps_left = nT;
                     sub_left = (SCHEME == SCHEME_SIMPLE) ? nT * nODE : 0;
+                    known_cell = -1;
                 }
             }
             next += __popc(done);

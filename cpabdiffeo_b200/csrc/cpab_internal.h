@@ -45,6 +45,7 @@ struct IntegrateArgs {
     double clamp_lo, clamp_hi;
     unsigned long long *counters;  // [4] or nullptr: fast steps, fallback steps, sub-steps, points
     int max_crossings;    // EXACT: give up after this many boundary crossings
+    int sort;             // REF/SIMPLE: process each tile's points in order of their start cell
 };
 
 // Counters slots.

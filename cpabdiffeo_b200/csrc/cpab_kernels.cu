@@ -90,6 +90,10 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real *sA = reinterpret_cast<Real *>(smem_raw);
     Real *sT = sA + a.t.nC * NE;
+    // cell-sort scratch after the tables: histogram [nC], start cells and permutation [tile_pts]
+    int *s_hist = reinterpret_cast<int *>(sA + (1 + TableLayout<Real>::kTParts) * a.t.nC * NE);
+    int *s_cell = s_hist + a.t.nC;
+    int *s_perm = s_cell + a.batch.tile_pts;
     __shared__ TileInfo s_tile;
 
     const int nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5;
@@ -112,12 +116,35 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
             __syncthreads();
         }
         const int64_t n = ti.end - ti.start;
+        const int *perm = nullptr;
+        if (a.sort) {
+            // counting sort of the tile's points by start cell (order inside a cell is irrelevant:
+            // every point is integrated on its own)
+            for (int i = threadIdx.x; i < a.t.nC; i += blockDim.x) s_hist[i] = 0;
+            __syncthreads();
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                PState<DIM, Real> st;
+                src.load(ti.start + i, st);
+                const int c = cell_of<DIM, TESS>(a.t, st);
+                s_cell[i] = c;
+                atomicAdd(s_hist + c, 1);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int acc = 0;
+                for (int c = 0; c < a.t.nC; ++c) { int v = s_hist[c]; s_hist[c] = acc; acc += v; }
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < n; i += blockDim.x) s_perm[atomicAdd(s_hist + s_cell[i], 1)] = i;
+            __syncthreads();
+            perm = s_perm;
+        }
         const int64_t per = (n + nwarps - 1) / nwarps;
         int64_t ws = ti.start + warp * per, we = ws + per;
         if (we > ti.end) we = ti.end;
         if (ws < we)
             integrate_range<DIM, TESS, Real, SCHEME>(a.t, a.nTimeSteps, a.nStepsODE, sA, sT, ws, we, h, src, snk,
-                                                     c_fast, c_fb, c_sub, c_pts);
+                                                     c_fast, c_fb, c_sub, c_pts, perm, ti.start);
         __syncthreads();
     }
     if (a.counters) {
@@ -414,6 +441,7 @@ static cudaError_t launch_integrate_t(const IntegrateArgs &a, const LaunchCfg &c
 {
     constexpr int NE = DIM * (DIM + 1);
     size_t smem = (size_t)(1 + TableLayout<Real>::kTParts) * a.t.nC * NE * sizeof(Real);
+    if (a.sort) smem += ((size_t)a.t.nC + 2 * (size_t)a.batch.tile_pts) * sizeof(int);
     auto kern = k_integrate<DIM, TESS, Real, SCHEME>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -14,6 +14,7 @@ struct LaunchCfg {
     int ctas_per_sm = 32;  // cap on resident CTAs per SM of the persistent grid (occupancy decides below it)
     int grid = 0;          // explicit grid (0 = persistent default)
     int tile_pts = 2048;   // points per CTA tile
+    int sort = 0;          // cell-sort the points of each tile (REF / SIMPLE schemes)
 };
 
 int num_sms();

@@ -10,8 +10,10 @@ Requests of mixed dimension, tessellation and size arrive at any time
      tessellation, precision, sign, integration parameters) as ONE ragged
      batch (one prologue launch for all thetas, one persistent integration
      launch), on a stream of a small pool, with pinned-memory copies;
-  4. advances every running registration job by a slice of MCMC steps on its
-     own stream, so registration slices and transform batches overlap.
+  4. advances every running registration job by a slice of MCMC steps on a
+     low-priority stream, one slice in flight per job, so registration slices
+     and transform batches overlap and transform batches (high-priority
+     streams) are not queued behind long registrations.
 State kept resident on the GPU: the basis of each space, every job's theta,
 log-likelihood and chain state.  Results do not depend on what else was in
 the batch: the transform kernels are per point, the likelihood reduction has
@@ -81,8 +83,12 @@ class CpabServer:
             memory_budget_bytes = int(free * 0.5)
         self.budget = int(memory_budget_bytes)
         self.in_use = 0
-        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(n_streams)]
+        # transforms: high-priority streams; registration slices: low priority
+        self.streams = [torch.cuda.Stream(device=self.device, priority=-1) for _ in range(n_streams)]
+        self.job_streams = [torch.cuda.Stream(device=self.device, priority=0) for _ in range(n_streams)]
         self._rr = itertools.cycle(range(n_streams))
+        self._rr_jobs = itertools.cycle(range(n_streams))
+        self._pinned: dict = {}
         self.mcmc_slice = int(mcmc_slice)
         self.max_batch_points = int(max_batch_points)
         self._ids = itertools.count()
@@ -108,6 +114,18 @@ class CpabServer:
         if key not in self._priors:
             self._priors[key] = Prior.create(sp.geo, 0.1, 1.0)
         return self._priors[key]
+
+    def _pinned_buf(self, numel: int, dtype) -> torch.Tensor:
+        """A pinned host buffer of at least numel elements from a reusable pool."""
+        free = self._pinned.setdefault(dtype, [])
+        for i, b in enumerate(free):
+            if b.numel() >= numel:
+                return free.pop(i)
+        return torch.empty(max(numel, 1 << 16), dtype=dtype).pin_memory()
+
+    def _release_pinned(self, *bufs) -> None:
+        for b in bufs:
+            self._pinned.setdefault(b.dtype, []).append(b)
 
     @staticmethod
     def _estimate_bytes(req) -> int:
@@ -204,35 +222,43 @@ class CpabServer:
         np_dt = np.float64 if prec == torch.float64 else np.float32
         sizes = [int(np.asarray(r.req.pts).shape[0]) for r in recs]
         offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
-        pts_h = torch.from_numpy(np.ascontiguousarray(np.concatenate([np.asarray(r.req.pts, dtype=np_dt).reshape(-1, dim)
-                                                                      for r in recs]))).pin_memory()
-        th_h = torch.from_numpy(np.stack([np.asarray(r.req.theta, dtype=np.float64) for r in recs])).pin_memory()
-        off_h = torch.from_numpy(offs).pin_memory()
-        out_h = torch.empty_like(pts_h).pin_memory()
+        total = int(offs[-1])
+        tdt = torch.float64 if np_dt == np.float64 else torch.float32
+        pin_x = self._pinned_buf(total * dim, tdt)
+        pin_o = self._pinned_buf(total * dim, tdt)
+        pin_th = self._pinned_buf(len(recs) * sp.d, torch.float64)
+        pin_off = self._pinned_buf(len(offs), torch.int64)
+        xv = pin_x[:total * dim].numpy().reshape(total, dim)
+        for r, a, b in zip(recs, offs[:-1], offs[1:]):
+            xv[a:b] = np.asarray(r.req.pts, dtype=np_dt).reshape(-1, dim)
+        pin_th[:len(recs) * sp.d].numpy().reshape(len(recs), sp.d)[:] = np.stack(
+            [np.asarray(r.req.theta, dtype=np.float64) for r in recs])
+        pin_off[:len(offs)].numpy()[:] = offs
         stream = self.streams[next(self._rr)]
         sch = {"exact": _lib.SCHEME_EXACT, "ref": _lib.SCHEME_REF, "simple": _lib.SCHEME_SIMPLE}[scheme]
         with torch.cuda.stream(stream):
-            x = pts_h.to(self.device, non_blocking=True)
-            th = th_h.to(self.device, non_blocking=True)
-            off = off_h.to(self.device, non_blocking=True)
+            x = pin_x[:total * dim].view(total, dim).to(self.device, non_blocking=True)
+            th = pin_th[:len(recs) * sp.d].view(len(recs), sp.d).to(self.device, non_blocking=True)
+            off = pin_off[:len(offs)].to(self.device, non_blocking=True)
             out = torch.empty_like(x)
             tables = sp.tables_from_theta(th, float(params["dt"]), sign)
             sp.calc_T_batched(tables, x, out, offsets=off, scheme=sch, **params)
-            out_h.copy_(out, non_blocking=True)
+            pin_o[:total * dim].view(total, dim).copy_(out, non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(stream)
         keep = (x, th, off, out, tables)            # device buffers live until retired
 
-        def finalize(recs=recs, out_h=out_h, offs=offs, keep=keep):
-            res = out_h.numpy()
+        def finalize(recs=recs, offs=offs, keep=keep, bufs=(pin_x, pin_o, pin_th, pin_off), total=total):
+            res = bufs[1][:total * dim].numpy().reshape(total, dim)
             for r, a, b in zip(recs, offs[:-1], offs[1:]):
                 r.result = res[a:b].copy()
+            self._release_pinned(*bufs)
         self.inflight.append((ev, recs, finalize))
 
     def _start_job(self, r: _Record) -> None:
         q: RegistrationRequest = r.req
         sp = self.space(2, q.nCs, q.tess, torch.float32)
-        stream = self.streams[next(self._rr)]
+        stream = self.job_streams[next(self._rr_jobs)]
         with torch.cuda.stream(stream):
             src = torch.as_tensor(np.asarray(q.src, dtype=np.float32), device=self.device)
             dst = torch.as_tensor(np.asarray(q.dst, dtype=np.float32), device=self.device)
@@ -240,11 +266,14 @@ class CpabServer:
             prop_std = np.sqrt(np.diag(self.prior(sp).cov_cpa))
             mh = BatchedMetropolis(ll, torch.zeros((1, sp.d), dtype=torch.float64, device=self.device), prop_std,
                                    scale=q.scale, seed=q.seed, rule=q.rule)
-        self.jobs.append(dict(rec=r, mh=mh, stream=stream, left=int(q.n_steps), keep=(src, dst)))
+        self.jobs.append(dict(rec=r, mh=mh, stream=stream, left=int(q.n_steps), keep=(src, dst), ev=None))
 
     def _advance_jobs(self) -> None:
         running = []
         for job in self.jobs:
+            if job["ev"] is not None and not job["ev"].query():
+                running.append(job)            # one slice in flight per job
+                continue
             k = min(self.mcmc_slice, job["left"])
             with torch.cuda.stream(job["stream"]):
                 job["mh"].run(k)
@@ -265,5 +294,7 @@ class CpabServer:
                                           accepted=int(acc_h[0]))
                     self.inflight.append((ev, [job["rec"]], finalize))
                 else:
+                    job["ev"] = torch.cuda.Event()
+                    job["ev"].record(job["stream"])
                     running.append(job)
         self.jobs = running

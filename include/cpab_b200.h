@@ -91,6 +91,14 @@ int cpab_set_clamp(cpab_ctx *ctx, int enable, double lo, double hi);
  * CTA tile.  0 keeps the current value.  Used by the autotuner. */
 int cpab_set_launch(cpab_ctx *ctx, int block, int ctas_per_sm, int tile_pts);
 
+/* Cell-sort the points of each CTA tile by start cell before integrating
+ * (REF / SIMPLE schemes): lanes of a warp then share cells (shared-memory
+ * broadcasts, coherent branches).  Results are unchanged (every point is
+ * integrated on its own).  Off by default; the autotuner decides.  No
+ * reference counterpart (the reference launches one thread per point in input
+ * order, cpab/gpu/Calcs.py:515). */
+int cpab_set_cell_sort(cpab_ctx *ctx, int enable);
+
 /* ------------------------------------------------------------------ prologue */
 
 /* Per-cell signed matrices and their exponentials for N transforms:

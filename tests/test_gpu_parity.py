@@ -290,3 +290,38 @@ def test_batched_host_pipeline_equals_device(scheme):
     od = torch.empty_like(xd)
     sp.calc_T_batched(tables, xd, od, offsets=torch.as_tensor(offs, device=DEV), scheme=scheme, **p)
     np.testing.assert_array_equal(oh.numpy(), od.cpu().numpy())
+
+
+@pytest.mark.parametrize("dim,nCs,tess,precision", [(2, (4, 4), "I", torch.float64), (2, (4, 4), "I", torch.float32),
+                                                    (3, (4, 4, 4), "I", torch.float32), (1, (100,), "II", torch.float64)])
+def test_launch_shape_and_cell_sort_do_not_change_results(dim, nCs, tess, precision):
+    sp, theta, rng = _prior_space(dim, nCs, tess, 23, precision)
+    tables = sp.tables_from_theta(torch.as_tensor(theta, device=DEV), 0.02, 1)
+    sizes = [5000, 0, 777, 12000]
+    offs = torch.as_tensor(np.concatenate([[0], np.cumsum(sizes)]), device=DEV)
+    x = cuda(rng.uniform(0, 1, size=(int(sum(sizes)), dim)), precision)
+    p = dict(dt=0.02, nTimeSteps=50, nStepsODEsolver=100)
+    outs = []
+    for block, tile, srt in [(256, 2048, False), (128, 1024, True), (256, 4096, True), (64, 512, False)]:
+        sp.set_launch(block=block, tile_pts=tile, cell_sort=srt)
+        o = torch.empty_like(x)
+        sp.calc_T_batched(tables, x, o, offsets=offs, **p)
+        outs.append(o)
+    for o in outs[1:]:
+        assert torch.equal(o, outs[0])
+
+
+def test_autotune_picks_a_config_and_keeps_results():
+    from cpabdiffeo_b200 import autotune
+    sp, theta, rng = _prior_space(2, (4, 4), "I", 29, torch.float32)
+    tables = sp.tables_from_theta(torch.as_tensor(theta, device=DEV), 0.02, 1)
+    offs = torch.as_tensor(np.array([0, 20000, 45000, 60000, 80000]), device=DEV)
+    x = cuda(rng.uniform(0, 1, size=(80000, 2)), torch.float32)
+    p = dict(dt=0.02, nTimeSteps=50, nStepsODEsolver=100)
+    ref = torch.empty_like(x)
+    sp.calc_T_batched(tables, x, ref, offsets=offs, **p)
+    cfg = autotune.tune(sp, tables, x, offs, _lib.SCHEME_REF, sample_points=50000, use_cache=False, **p)
+    assert cfg["block"] in (128, 256) and cfg["ms_sample"] > 0
+    out = torch.empty_like(x)
+    sp.calc_T_batched(tables, x, out, offsets=offs, **p)
+    assert torch.equal(out, ref)
