@@ -19,7 +19,7 @@ STATUS_NAMES = {
 }
 CPAB_F64, CPAB_F32 = 0, 1
 SCHEME_REF, SCHEME_SIMPLE, SCHEME_EXACT = 0, 1, 2
-CNT_FAST, CNT_FALLBACK, CNT_SUBSTEPS, CNT_POINTS, CNT_FAILED, CNT_N = 0, 1, 2, 3, 4, 5
+CNT_FAST, CNT_FALLBACK, CNT_SUBSTEPS, CNT_POINTS, CNT_FAILED, CNT_NAN, CNT_CANCELLED, CNT_N = 0, 1, 2, 3, 4, 5, 6, 7
 
 
 class CpabLibraryError(RuntimeError):
@@ -41,6 +41,9 @@ SIGNATURES = {
     "cpab_ctx_num_cells": (_i, [_vp]),
     "cpab_ctx_cell_len": (_i, [_vp]),
     "cpab_set_clamp": (_i, [_vp, _i, _d, _d]),
+    "cpab_cancel": (_i, [_vp]),
+    "cpab_clear_cancel": (_i, [_vp]),
+    "cpab_cancel_requested": (_i, [_vp]),
     "cpab_set_launch": (_i, [_vp, _i, _i, _i]),
     "cpab_set_cell_sort": (_i, [_vp, _i]),
     "cpab_expm": (_i, [_vp, _vp, _i, _d, _i, _vp, _vp, _vp]),

@@ -89,8 +89,6 @@ def tune(space: CpaSpace, tables, pts: torch.Tensor, offsets: torch.Tensor | Non
     out = torch.empty_like(x)
     cand = [dict(block=b, tile_pts=t, cell_sort=s) for b, t, s in
             itertools.product(CANDIDATES["block"], CANDIDATES["tile_pts"], CANDIDATES["cell_sort"])]
-    if scheme == _lib.SCHEME_EXACT:
-        cand = [c for c in cand if not c["cell_sort"]]
     best, best_ms = None, float("inf")
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for c in cand:

@@ -330,7 +330,8 @@ class CpaSpace:
 
         The batch is cut into `chunks` contiguous groups of instances with about
         equal point counts; group k+1 is copied in while group k is integrated
-        and group k-1 is copied out (three streams, two device buffers).
+        and group k-1 is copied out (three streams, three device buffers, so
+        no stage waits for a buffer while the other two are busy).
         theta: [N, d] (host or device); offsets_host: int64 [N+1] (host).
         Returns an event recorded on the current stream once out_host is
         complete; the current stream waits for it."""
@@ -357,7 +358,8 @@ class CpaSpace:
         dim = self.dim
         dt_ = pts_host.dtype
         bufs = []
-        for _ in range(2):
+        nbuf = min(3, len(groups))
+        for _ in range(nbuf):
             bufs.append(dict(x=torch.empty((maxpts, dim), dtype=dt_, device=dev),
                              o=torch.empty((maxpts, dim), dtype=dt_, device=dev),
                              off=torch.empty(len(offs), dtype=torch.int64, device=dev),
@@ -367,7 +369,7 @@ class CpaSpace:
         off_pin = torch.empty((len(groups), len(offs)), dtype=torch.int64).pin_memory()
         ev_last = None
         for k, (a, b) in enumerate(groups):
-            buf = bufs[k % 2]
+            buf = bufs[k % nbuf]
             o0, o1 = int(offs[a]), int(offs[b])
             n = o1 - o0
             off_pin[k, :b - a + 1] = torch.from_numpy(offs[a:b + 1] - o0)
@@ -398,6 +400,15 @@ class CpaSpace:
         done = torch.cuda.Event()
         done.record(cur)
         return done
+
+    def cancel(self) -> None:
+        """Stop running and future launches of this space between tiles (see cpab_cancel)."""
+        c = self._ctx
+        c.check(c.lib.cpab_cancel(c.h))
+
+    def clear_cancel(self) -> None:
+        c = self._ctx
+        c.check(c.lib.cpab_clear_cancel(c.h))
 
     def set_launch(self, block: int = 0, ctas_per_sm: int = 0, tile_pts: int = 0, cell_sort: bool | None = None) -> None:
         c = self._ctx

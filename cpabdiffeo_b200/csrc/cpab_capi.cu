@@ -45,14 +45,52 @@ int cpab_ctx_create(cpab_ctx **out, int dim, int tess, const int *nCs, const dou
         return fail(nullptr, CPAB_BAD_ARG, "invalid nCs/incs (need nCs >= 1, finite incs > 0, at most 2^20 cells)");
     }
     for (int k = 0; k < 3; ++k) c->nCs[k] = k < dim ? nCs[k] : 1;
+    // cancel flag in mapped host memory (only where a device is present)
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0) {
+        void *h = nullptr;
+        if (cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped) == cudaSuccess) {
+            void *d = nullptr;
+            if (cudaHostGetDevicePointer(&d, h, 0) == cudaSuccess) {
+                c->cancel_host = static_cast<int *>(h);
+                c->cancel_dev = static_cast<int *>(d);
+                *c->cancel_host = 0;
+            } else {
+                cudaFreeHost(h);
+            }
+        }
+    }
+    cudaGetLastError();  // a missing device is not an error here
     *out = c;
     return CPAB_OK;
 }
 
 int cpab_ctx_destroy(cpab_ctx *ctx)
 {
+    if (ctx && ctx->cancel_host) cudaFreeHost(ctx->cancel_host);
     delete ctx;
     return CPAB_OK;
+}
+
+int cpab_cancel(cpab_ctx *ctx)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (!ctx->cancel_host) return fail(ctx, CPAB_UNSUPPORTED, "this context has no cancel flag");
+    __atomic_store_n(ctx->cancel_host, 1, __ATOMIC_SEQ_CST);
+    return CPAB_OK;
+}
+
+int cpab_clear_cancel(cpab_ctx *ctx)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (!ctx->cancel_host) return fail(ctx, CPAB_UNSUPPORTED, "this context has no cancel flag");
+    __atomic_store_n(ctx->cancel_host, 0, __ATOMIC_SEQ_CST);
+    return CPAB_OK;
+}
+
+int cpab_cancel_requested(const cpab_ctx *ctx)
+{
+    return (ctx && ctx->cancel_host) ? __atomic_load_n(ctx->cancel_host, __ATOMIC_SEQ_CST) : 0;
 }
 
 const char *cpab_last_error_string(const cpab_ctx *ctx) { return ctx ? ctx->err : g_thread_err; }
@@ -161,8 +199,14 @@ static int check_integrate(cpab_ctx *ctx, const double *signedA, const double *T
     size_t bytes = (size_t)nPts * ctx->t.dim * (precision == CPAB_F64 ? 8 : 4);
     if (nPts > 0 && overlaps(pts, bytes, out, bytes))
         return fail(ctx, CPAB_ALIAS, "pts and out cannot point to the same memory (_CpaCalcs.py:388)");
-    size_t need = tables_smem(ctx, precision);
-    if (ctx->cfg.sort) need += ((size_t)ctx->t.nC + 2 * (size_t)ctx->cfg.tile_pts) * sizeof(int);
+    size_t need;
+    if (scheme == CPAB_SCHEME_EXACT) {
+        need = exact1d_smem_bytes(ctx->t.nC, ctx->cfg.tile_pts, ctx->cfg.sort,
+                                  precision == CPAB_F64 ? PREC_F64 : PREC_F32);
+    } else {
+        need = tables_smem(ctx, precision);
+        if (ctx->cfg.sort) need += ((size_t)ctx->t.nC + 2 * (size_t)ctx->cfg.tile_pts) * sizeof(int);
+    }
     if (need > (size_t)max_smem_optin())
         return fail(ctx, CPAB_UNSUPPORTED, "cell tables and tile scratch (%zu bytes) exceed shared memory", need);
     return CPAB_OK;
@@ -187,6 +231,7 @@ static IntegrateArgs make_args(cpab_ctx *ctx, const double *signedA, const doubl
     a.counters = reinterpret_cast<unsigned long long *>(counters);
     a.max_crossings = 4 * ctx->t.nC + 8;
     a.sort = ctx->cfg.sort;
+    a.cancel = ctx->cancel_dev;
     return a;
 }
 

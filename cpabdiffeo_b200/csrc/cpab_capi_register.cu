@@ -115,9 +115,11 @@ int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
     if (!(sigma > 0)) return fail(ctx, CPAB_BAD_ARG, "sigma must be positive");
     if (nTimeSteps < 1 || nStepsODE < 1) return fail(ctx, CPAB_BAD_ARG, "nTimeSteps and nStepsODE must be >= 1");
     if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
-    if ((size_t)ctx->t.nC * 6 * (precision == CPAB_F64 ? 2 * 8 : 3 * 4) > (size_t)max_smem_optin())
-        return fail(ctx, CPAB_UNSUPPORTED, "cell tables exceed shared memory");
     const int tile_px = ctx->cfg.tile_pts;
+    // cell tables plus one double per pixel of a tile
+    if ((size_t)ctx->t.nC * 6 * (precision == CPAB_F64 ? 2 * 8 : 3 * 4) + (size_t)tile_px * 8 >
+        (size_t)max_smem_optin())
+        return fail(ctx, CPAB_UNSUPPORTED, "cell tables and tile scratch exceed shared memory");
     const WsLayout L = ws_layout(N, tiles_of(H, W, tile_px));
     if (!workspace || workspace_bytes < L.total)
         return fail(ctx, CPAB_NO_MEMORY, "workspace of %zu bytes needed", L.total);
@@ -142,6 +144,7 @@ int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
     a.dt = dt;
     a.nTimeSteps = nTimeSteps;
     a.nStepsODE = nStepsODE;
+    a.cancel = ctx->cancel_dev;
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(a.tickets, 0, (size_t)N * sizeof(unsigned), s);
     if (e != cudaSuccess) return cuda_status(ctx, e, "ticket reset");

@@ -258,9 +258,15 @@ CPAB_HD void exact_midpoint(double *p, const double *A, double h)
 
 CPAB_HD int fast_box_coord(float p, int n, float inv)
 {
+#ifdef __CUDA_ARCH__
+    // one float->int conversion rounding down; NaN converts to 0, +-inf saturate
+    int k = __float2int_rd(p * inv);
+    return min(max(k, 0), n - 1);
+#else
     float k = floorf(p * inv);
     k = fminf(fmaxf(k, 0.0f), (float)(n - 1));  // NaN -> 0
     return (int)k;
+#endif
 }
 
 CPAB_HD int fast_cell_2d_tri(const Tess &t, const float *p)

@@ -16,6 +16,8 @@ struct cpab_ctx {
     int clamp = 0;
     double clamp_lo = 0, clamp_hi = 0;
     cpab::LaunchCfg cfg;
+    int *cancel_host = nullptr;  // mapped pinned host flag
+    int *cancel_dev = nullptr;   // its device-side address
     char err[512] = {0};
 };
 

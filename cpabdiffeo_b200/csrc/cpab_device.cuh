@@ -80,4 +80,44 @@ __device__ __forceinline__ TileInfo decode_tile(const Batch &b, int64_t tile)
     return ti;
 }
 
+// True (in every thread of the CTA) once the context's cancel flag is set;
+// call at a point all threads reach.  The persistent kernels poll it every
+// 8th tile (a read of mapped host memory costs about a microsecond).
+__device__ __forceinline__ bool cta_cancelled(const volatile int *flag, unsigned long long *counters)
+{
+    __shared__ int s_stop;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_stop = (flag && *flag) ? 1 : 0;
+        if (s_stop && counters) atomicAdd(counters + CNT_CANCELLED, 1ull);
+    }
+    __syncthreads();
+    return s_stop != 0;
+}
+
+// Exclusive prefix sum of hist[0, n) in place, by the CTA's first warp
+// (each lane scans a contiguous chunk, the chunk totals are combined with
+// shuffles).  The caller synchronises before and after.
+__device__ __forceinline__ void warp0_exclusive_scan(int *hist, int n)
+{
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    const int per = (n + 31) / 32;
+    const int lo = min(lane * per, n), hi = min(lo + per, n);
+    int sum = 0;
+    for (int c = lo; c < hi; ++c) sum += hist[c];
+    int inc = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(FULL, inc, o);
+        if (lane >= o) inc += v;
+    }
+    int run = inc - sum;
+    for (int c = lo; c < hi; ++c) {
+        const int v = hist[c];
+        hist[c] = run;
+        run += v;
+    }
+}
+
 }  // namespace cpab

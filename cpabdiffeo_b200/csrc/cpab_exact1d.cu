@@ -23,6 +23,8 @@ namespace cpab {
 
 struct Exact1D {
     const double *A;  // [nC, 2] signed (a, b) of the current instance, shared memory
+    const double *ba; // [nC] b / a
+    const double *ia; // [nC] 1.0 / a
     int nC;
     double step;      // 1/nC: vertices x_k = k*step, x_nC = 1 (np.linspace(0,1,nC+1))
 };
@@ -60,7 +62,7 @@ __device__ double cf_crossing(const Exact1D &e, double x, int c, int &next)
     double t;
     if (xn == 0 || xn == 1) t = CUDART_INF;
     else if (near0(a)) t = (xn - x) / b;
-    else t = 1.0 / a * log((xn + b / a) / (x + b / a));
+    else t = e.ia[c] * log((xn + e.ba[c]) / (x + e.ba[c]));   // 1.0/a * log((xn + b/a) / (x + b/a))
     next = cn;
     return t;
 }
@@ -124,17 +126,18 @@ __device__ bool cf_point(const Exact1D &e, const Transit &tr, double x, double t
     // first visit: general position
     int c = cf_cell(e, x_old), cn;
     double tc = cf_crossing(e, x_old, c, cn);
+    bool ok = true;
+    // walk the transit table (cheap, divergent); the final exponential runs
+    // after the loop so that all lanes of a warp evaluate it together
     for (int counter = 0;;) {
         ++visits;
-        if (tc >= t_rem) {
-            out = fmin(1.0, fmax(0.0, cf_phi(e, c, x_old, t_rem)));
-            return true;
-        }
+        if (tc >= t_rem) break;
         t_rem -= tc;
         if (++counter >= cap) {
             // the point would have been left at the crossing it just made
-            out = (cn > c) ? tr.enter0[cn] : tr.enter1[cn];
-            return false;
+            x_old = (cn > c) ? tr.enter0[cn] : tr.enter1[cn];
+            ok = false;
+            break;
         }
         // enter cell cn at the nudged vertex and read its transit from the table
         if (cn > c) {
@@ -149,6 +152,22 @@ __device__ bool cf_point(const Exact1D &e, const Transit &tr, double x, double t
             cn = tr.nx1[cn];
         }
     }
+    out = ok ? fmin(1.0, fmax(0.0, cf_phi(e, c, x_old, t_rem))) : x_old;
+    return ok;
+}
+
+// Shared memory of k_exact1d: per cell A (2 doubles), b/a and 1/a (2),
+// entry points and hitting times (4 doubles), next and entry cells (4 ints)
+// -- 80 bytes, so what follows is 16-byte aligned -- and, when cell-sorting,
+// sorted start points and results in input order [tile_pts] (Real), start
+// cells and permutation [tile_pts] and the histogram [nC] (int).
+size_t exact1d_smem_bytes(int nC, int tile_pts, int sort, int prec)
+{
+    size_t b = (size_t)nC * (8 * sizeof(double) + 4 * sizeof(int));
+    if (sort)
+        b += 2 * (size_t)tile_pts * (prec == PREC_F64 ? sizeof(double) : sizeof(float)) +
+             ((size_t)nC + 2 * (size_t)tile_pts) * sizeof(int);
+    return b;
 }
 
 template <typename Real>
@@ -157,8 +176,9 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nC = a.t.nC;
     double *sA = reinterpret_cast<double *>(smem_raw);
+    double *s_ba = sA + 2 * nC, *s_ia = s_ba + nC;
     Transit tr;
-    tr.enter0 = sA + 2 * nC;
+    tr.enter0 = s_ia + nC;
     tr.enter1 = tr.enter0 + nC;
     tr.tc0 = tr.enter1 + nC;
     tr.tc1 = tr.tc0 + nC;
@@ -166,47 +186,109 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
     tr.nx1 = tr.nx0 + nC;
     tr.cell0 = tr.nx1 + nC;
     tr.cell1 = tr.cell0 + nC;
+    // cell-sort scratch (see exact1d_smem_bytes)
+    const int tp = a.batch.tile_pts;
+    Real *s_xs = reinterpret_cast<Real *>(tr.cell1 + nC);
+    Real *s_y = s_xs + tp;
+    int *s_cell = reinterpret_cast<int *>(s_y + tp);
+    int *s_perm = s_cell + tp;
+    int *s_hist = s_perm + tp;
     __shared__ TileInfo s_tile;
+    __shared__ int s_claim;
     const double T_total = a.dt * (double)a.nTimeSteps;
     const int64_t ntiles = total_tiles(a.batch);
-    unsigned long long c_pts = 0, c_fail = 0, c_visits = 0;
+    const int lane = threadIdx.x & 31;
+    unsigned long long c_pts = 0, c_fail = 0, c_visits = 0, c_nan = 0;
     int loaded = -1;
     Exact1D e;
     e.A = sA;
+    e.ba = s_ba;
+    e.ia = s_ia;
     e.nC = nC;
     e.step = 1.0 / (double)nC;
     // the reference gives up after nC crossings
     const int cap = nC;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        if (threadIdx.x == 0) s_tile = decode_tile(a.batch, tile);
+        if ((((tile - blockIdx.x) / gridDim.x) & 7) == 0 && cta_cancelled(a.cancel, a.counters)) break;
+        if (threadIdx.x == 0) {
+            s_tile = decode_tile(a.batch, tile);
+            s_claim = 0;
+        }
         __syncthreads();
         const TileInfo ti = s_tile;
         if (ti.inst != loaded) {
             const double *gA = a.A + (size_t)ti.inst * nC * 2;
             for (int i = threadIdx.x; i < nC * 2; i += blockDim.x) sA[i] = gA[i];
+            for (int c = threadIdx.x; c < nC; c += blockDim.x) {
+                const double ac = gA[2 * c], bc = gA[2 * c + 1];
+                s_ba[c] = bc / ac;
+                s_ia[c] = 1.0 / ac;
+            }
             __syncthreads();
             build_transit(e, tr);
             loaded = ti.inst;
             __syncthreads();
         }
-        for (int64_t i = ti.start + threadIdx.x; i < ti.end; i += blockDim.x) {
-            Real xin;
-            load_pt<1, Real>(a.pts_in, i, &xin);
-            double y;
-            bool ok = cf_point(e, tr, (double)xin, T_total, cap, y, c_visits);
-            if (a.clamp) y = clamp_ref(y, a.clamp_lo, a.clamp_hi);
-            Real yo = (Real)y;
-            store_pt<1, Real>(a.pts_out, i, &yo);
-            ++c_pts;
-            c_fail += ok ? 0 : 1;
+        const int n = (int)(ti.end - ti.start);
+        if (a.sort) {
+            // counting sort by start cell: a warp then takes neighbouring points,
+            // which cross the same cells (same walk length).  Points are staged
+            // in shared memory so that global loads and stores stay coalesced.
+            for (int c = threadIdx.x; c < nC; c += blockDim.x) s_hist[c] = 0;
+            __syncthreads();
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                Real xin;
+                load_pt<1, Real>(a.pts_in, ti.start + j, &xin);
+                const int c = cf_cell(e, (double)xin);
+                s_y[j] = xin;
+                s_cell[j] = c;
+                atomicAdd(s_hist + c, 1);
+            }
+            __syncthreads();
+            warp0_exclusive_scan(s_hist, nC);
+            __syncthreads();
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                const int pos = atomicAdd(s_hist + s_cell[j], 1);
+                s_perm[pos] = j;
+                s_xs[pos] = s_y[j];
+            }
+            __syncthreads();
+        }
+        // warps claim 32 consecutive (sorted) points at a time until the tile is done
+        for (;;) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&s_claim, 32);
+            base = __shfl_sync(FULL, base, 0);
+            if (base >= n) break;
+            const int k = base + lane;
+            if (k < n) {
+                Real xin;
+                if (a.sort) xin = s_xs[k];
+                else load_pt<1, Real>(a.pts_in, ti.start + k, &xin);
+                double y;
+                bool ok = cf_point(e, tr, (double)xin, T_total, cap, y, c_visits);
+                if (a.clamp) y = clamp_ref(y, a.clamp_lo, a.clamp_hi);
+                Real yo = (Real)y;
+                if (a.sort) s_y[s_perm[k]] = yo;
+                else store_pt<1, Real>(a.pts_out, ti.start + k, &yo);
+                ++c_pts;
+                c_fail += ok ? 0 : 1;
+                c_nan += (y != y) ? 1 : 0;
+            }
         }
         __syncthreads();
+        if (a.sort) {
+            for (int j = threadIdx.x; j < n; j += blockDim.x) store_pt<1, Real>(a.pts_out, ti.start + j, s_y + j);
+            // the next tile rewrites s_y only after its first barrier
+        }
     }
     if (a.counters) {
         c_pts = warp_sum_u64(c_pts);
         c_fail = warp_sum_u64(c_fail);
         c_visits = warp_sum_u64(c_visits);
+        c_nan = warp_sum_u64(c_nan);
         if ((threadIdx.x & 31) == 0) {
+            if (c_nan) atomicAdd(a.counters + CNT_NAN, c_nan);
             atomicAdd(a.counters + CNT_FAST, c_visits);  // cell visits (closed-form segments)
             atomicAdd(a.counters + CNT_POINTS, c_pts);
             atomicAdd(a.counters + CNT_FAILED, c_fail);
@@ -216,8 +298,7 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
 
 cudaError_t launch_integrate_exact1d(const IntegrateArgs &a, int prec, const LaunchCfg &cfg, cudaStream_t s)
 {
-    // A (2 doubles), entry points and hitting times (4 doubles), next cells and entry cells (4 ints)
-    size_t smem = (size_t)a.t.nC * (6 * sizeof(double) + 4 * sizeof(int));
+    const size_t smem = exact1d_smem_bytes(a.t.nC, a.batch.tile_pts, a.sort, prec);
     if (prec == PREC_F64) {
         auto kern = k_exact1d<double>;
         if (smem > 48 * 1024) {

@@ -196,6 +196,10 @@ __device__ __forceinline__ void substep(PState<DIM, float> &s, const float *A, f
 //   Snk::put(idx, st)      receives the end state (PState; get() converts)
 //   perm (optional, shared memory): the k-th point of the range is
 //   ws_base + perm[k - ws_base] (a cell-sorted order inside the tile).
+//   claim (optional, shared memory, zero on entry): all warps of the CTA
+//   share one queue over [ws, we) -- a warp whose lanes finish claims the next
+//   points of the whole tile, so no warp idles at the end-of-tile barrier
+//   while another still works through a fixed slice.
 // The reference recomputes the start cell of every time step; after a kept
 // closed-form step that cell was just computed for the same point, so it is
 // reused (identical value, one lookup per step saved).
@@ -204,14 +208,22 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
                                                 int64_t ws, int64_t we, Real h, const Src &src, Snk &snk,
                                                 unsigned long long &c_fast, unsigned long long &c_fb,
                                                 unsigned long long &c_sub, unsigned long long &c_pts,
-                                                const int *perm = nullptr, int64_t perm_base = 0)
+                                                const int *perm = nullptr, int64_t perm_base = 0,
+                                                unsigned long long *claim = nullptr)
 {
     constexpr int NE = DIM * (DIM + 1);
     const int tab = t.nC * NE;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     int64_t next = ws + 32;
-    int64_t k = ws + lane;
+    int64_t k;
+    if (claim) {
+        unsigned long long b = 0;
+        if (lane == 0) b = atomicAdd(claim, 32ull);
+        k = ws + (int64_t)__shfl_sync(FULL, b, 0) + lane;
+    } else {
+        k = ws + lane;
+    }
     bool active = k < we;
     int64_t idx = (active && perm) ? perm_base + perm[k - perm_base] : k;
     PState<DIM, Real> st;
@@ -251,8 +263,16 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
         }
         unsigned done = __ballot_sync(FULL, fin);
         if (done) {
+            int64_t base;
+            if (claim) {
+                unsigned long long b = 0;
+                if (lane == 0) b = atomicAdd(claim, (unsigned long long)__popc(done));
+                base = ws + (int64_t)__shfl_sync(FULL, b, 0);
+            } else {
+                base = next;
+            }
             if (fin) {
-                k = next + __popc(done & lt);
+                k = base + __popc(done & lt);
                 active = k < we;
                 if (active) {
                     idx = perm ? perm_base + perm[k - perm_base] : k;

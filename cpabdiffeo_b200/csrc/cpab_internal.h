@@ -46,9 +46,13 @@ struct IntegrateArgs {
     unsigned long long *counters;  // [4] or nullptr: fast steps, fallback steps, sub-steps, points
     int max_crossings;    // EXACT: give up after this many boundary crossings
     int sort;             // REF/SIMPLE: process each tile's points in order of their start cell
+    const volatile int *cancel;  // host-mapped flag polled between tiles, or nullptr
 };
 
 // Counters slots.
-enum { CNT_FAST = 0, CNT_FALLBACK = 1, CNT_SUBSTEPS = 2, CNT_POINTS = 3, CNT_FAILED = 4, CNT_N = 5 };
+// CNT_NAN: points whose result has a NaN coordinate; CNT_CANCELLED: CTAs that
+// stopped early because the context's cancel flag was set.
+enum { CNT_FAST = 0, CNT_FALLBACK = 1, CNT_SUBSTEPS = 2, CNT_POINTS = 3, CNT_FAILED = 4, CNT_NAN = 5,
+       CNT_CANCELLED = 6, CNT_N = 7 };
 
 }  // namespace cpab

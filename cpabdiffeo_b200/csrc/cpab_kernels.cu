@@ -70,15 +70,19 @@ struct ArraySnk {
     void *base;
     int clamp;
     double lo, hi;
+    unsigned long long nan;
     template <typename Real>
     __device__ __forceinline__ void put(int64_t i, const PState<DIM, Real> &st)
     {
         Real p[DIM];
         st.get(p);
-        if (clamp) {
+        bool bad = false;
 #pragma unroll
-            for (int k = 0; k < DIM; ++k) p[k] = clamp_ref(p[k], lo, hi);
+        for (int k = 0; k < DIM; ++k) {
+            if (clamp) p[k] = clamp_ref(p[k], lo, hi);
+            bad |= (p[k] != p[k]);
         }
+        nan += bad ? 1 : 0;
         store_pt<DIM, Real>(base, i, p);
     }
 };
@@ -95,18 +99,22 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
     int *s_cell = s_hist + a.t.nC;
     int *s_perm = s_cell + a.batch.tile_pts;
     __shared__ TileInfo s_tile;
+    __shared__ unsigned long long s_claim;
 
-    const int nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5;
     const int tab = a.t.nC * NE;
     const Real h = (Real)(a.dt / (double)a.nStepsODE);
     const int64_t ntiles = total_tiles(a.batch);
     unsigned long long c_fast = 0, c_fb = 0, c_sub = 0, c_pts = 0;
     int loaded = -1;
     const ArraySrc<DIM> src{a.pts_in};
-    ArraySnk<DIM> snk{a.pts_out, a.clamp, a.clamp_lo, a.clamp_hi};
+    ArraySnk<DIM> snk{a.pts_out, a.clamp, a.clamp_lo, a.clamp_hi, 0ull};
 
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        if (threadIdx.x == 0) s_tile = decode_tile(a.batch, tile);
+        if ((((tile - blockIdx.x) / gridDim.x) & 7) == 0 && cta_cancelled(a.cancel, a.counters)) break;
+        if (threadIdx.x == 0) {
+            s_tile = decode_tile(a.batch, tile);
+            s_claim = 0ull;
+        }
         __syncthreads();
         const TileInfo ti = s_tile;
         if (ti.inst != loaded) {
@@ -130,21 +138,15 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
                 atomicAdd(s_hist + c, 1);
             }
             __syncthreads();
-            if (threadIdx.x == 0) {
-                int acc = 0;
-                for (int c = 0; c < a.t.nC; ++c) { int v = s_hist[c]; s_hist[c] = acc; acc += v; }
-            }
+            warp0_exclusive_scan(s_hist, a.t.nC);
             __syncthreads();
             for (int i = threadIdx.x; i < n; i += blockDim.x) s_perm[atomicAdd(s_hist + s_cell[i], 1)] = i;
             __syncthreads();
             perm = s_perm;
         }
-        const int64_t per = (n + nwarps - 1) / nwarps;
-        int64_t ws = ti.start + warp * per, we = ws + per;
-        if (we > ti.end) we = ti.end;
-        if (ws < we)
-            integrate_range<DIM, TESS, Real, SCHEME>(a.t, a.nTimeSteps, a.nStepsODE, sA, sT, ws, we, h, src, snk,
-                                                     c_fast, c_fb, c_sub, c_pts, perm, ti.start);
+        // every warp works on the whole tile through the shared claim counter
+        integrate_range<DIM, TESS, Real, SCHEME>(a.t, a.nTimeSteps, a.nStepsODE, sA, sT, ti.start, ti.end, h, src,
+                                                 snk, c_fast, c_fb, c_sub, c_pts, perm, ti.start, &s_claim);
         __syncthreads();
     }
     if (a.counters) {
@@ -152,11 +154,13 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
         c_fb = warp_sum_u64(c_fb);
         c_sub = warp_sum_u64(c_sub);
         c_pts = warp_sum_u64(c_pts);
+        unsigned long long c_nan = warp_sum_u64(snk.nan);
         if ((threadIdx.x & 31) == 0) {
             atomicAdd(a.counters + CNT_FAST, c_fast);
             atomicAdd(a.counters + CNT_FALLBACK, c_fb);
             atomicAdd(a.counters + CNT_SUBSTEPS, c_sub);
             atomicAdd(a.counters + CNT_POINTS, c_pts);
+            if (c_nan) atomicAdd(a.counters + CNT_NAN, c_nan);
         }
     }
 }

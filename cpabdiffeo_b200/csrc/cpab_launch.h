@@ -14,7 +14,7 @@ struct LaunchCfg {
     int ctas_per_sm = 32;  // cap on resident CTAs per SM of the persistent grid (occupancy decides below it)
     int grid = 0;          // explicit grid (0 = persistent default)
     int tile_pts = 2048;   // points per CTA tile
-    int sort = 0;          // cell-sort the points of each tile (REF / SIMPLE schemes)
+    int sort = 0;          // cell-sort the points of each tile
 };
 
 int num_sms();
@@ -27,6 +27,7 @@ inline int persistent_grid(K kern, const LaunchCfg &cfg, size_t smem)
 
 cudaError_t launch_integrate(const IntegrateArgs &a, int prec, int scheme, const LaunchCfg &cfg, cudaStream_t s);
 cudaError_t launch_integrate_exact1d(const IntegrateArgs &a, int prec, const LaunchCfg &cfg, cudaStream_t s);
+size_t exact1d_smem_bytes(int nC, int tile_pts, int sort, int prec);
 cudaError_t launch_tile_prefix(const int64_t *offsets, int64_t *prefix, int N, int tile_pts, cudaStream_t s);
 cudaError_t launch_trajectory(const IntegrateArgs &a, int64_t nPts, cudaStream_t s);
 cudaError_t launch_cell_idx(const Tess &t, const double *pts, int32_t *out, int64_t n, cudaStream_t s);

@@ -136,14 +136,16 @@ struct PixelSrc {
 };
 
 // End points: sampled from src and scored against dst; nothing stored
-// unless `warped` is given.
+// unless `warped` is given.  Each pixel's term goes to its slot of the
+// tile's shared-memory array, so the tile sum can be taken in a fixed order
+// whichever warp finished the pixel.
 struct SsdSnk {
     const float *src, *dst;
     float *warped;
     int H, W;
-    int64_t base;
+    int64_t base, tile_start;
     double k;
-    double acc;
+    double *term;
     template <typename Real>
     __device__ __forceinline__ void put(int64_t i, const PState<2, Real> &st)
     {
@@ -153,7 +155,7 @@ struct SsdSnk {
         double w = bilinear(src, H, W, p[0] * W - 0.5, p[1] * H - 0.5);
         if (warped) warped[j] = (float)w;
         double e = w - (double)__ldg(dst + j);
-        acc += e * e * k;
+        term[i - tile_start] = e * e * k;
     }
 };
 
@@ -164,7 +166,9 @@ __global__ void __launch_bounds__(256) k_register_ll(RegisterArgs a)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real *sA = reinterpret_cast<Real *>(smem_raw);
     Real *sT = sA + a.t.nC * NE;
-    const int nwarps = blockDim.x >> 5, warp = threadIdx.x >> 5;
+    // per-pixel terms of the current tile, after the tables (their size is a multiple of 8 bytes)
+    double *s_term = reinterpret_cast<double *>(sA + (1 + TableLayout<Real>::kTParts) * a.t.nC * NE);
+    __shared__ unsigned long long s_claim;
     const int tab = a.t.nC * NE;
     const Real h = (Real)(a.dt / (double)a.nStepsODE);
     const int64_t npx = (int64_t)a.H * a.W;
@@ -173,6 +177,7 @@ __global__ void __launch_bounds__(256) k_register_ll(RegisterArgs a)
     unsigned long long c_fast = 0, c_fb = 0, c_sub = 0, c_pts = 0;
     int loaded = -1;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        if ((((tile - blockIdx.x) / gridDim.x) & 7) == 0 && cta_cancelled(a.cancel, a.counters)) break;
         const int inst = (int)(tile / tpi);
         const int64_t k = tile - (int64_t)inst * tpi;
         const int64_t base = (int64_t)inst * npx;
@@ -185,16 +190,18 @@ __global__ void __launch_bounds__(256) k_register_ll(RegisterArgs a)
             __syncthreads();
         }
         PixelSrc src{a.H, a.W, base};
-        SsdSnk snk{a.src + base, a.dst + base, a.warped ? a.warped + base : nullptr, a.H, a.W, base,
-                   -0.5 / (a.sigma * a.sigma), 0.0};
-        const int64_t n = end - start;
-        const int64_t per = (n + nwarps - 1) / nwarps;
-        int64_t ws = start + warp * per, we = ws + per;
-        if (we > end) we = end;
-        if (ws < we)
-            integrate_range<DIM, TESS, Real, SCHEME_REF>(a.t, a.nTimeSteps, a.nStepsODE, sA, sT, ws, we, h, src,
-                                                         snk, c_fast, c_fb, c_sub, c_pts);
-        finish_tile(snk.acc, tile, inst, (int)tpi, (int64_t)inst * tpi, a.partials, a.tickets, a.ll);
+        SsdSnk snk{a.src + base, a.dst + base, a.warped ? a.warped + base : nullptr, a.H, a.W, base, start,
+                   -0.5 / (a.sigma * a.sigma), s_term};
+        if (threadIdx.x == 0) s_claim = 0ull;
+        __syncthreads();
+        // all warps share the tile through the claim counter
+        integrate_range<DIM, TESS, Real, SCHEME_REF>(a.t, a.nTimeSteps, a.nStepsODE, sA, sT, start, end, h, src,
+                                                     snk, c_fast, c_fb, c_sub, c_pts, nullptr, 0, &s_claim);
+        __syncthreads();
+        // fixed-order sum of the tile's terms: thread t takes slots t, t + blockDim, ...
+        double acc = 0.0;
+        for (int j = threadIdx.x; j < (int)(end - start); j += blockDim.x) acc += s_term[j];
+        finish_tile(acc, tile, inst, (int)tpi, (int64_t)inst * tpi, a.partials, a.tickets, a.ll);
     }
     if (a.counters) {
         c_fast = warp_sum_u64(c_fast);
@@ -213,7 +220,8 @@ __global__ void __launch_bounds__(256) k_register_ll(RegisterArgs a)
 template <int TESS, typename Real>
 static cudaError_t launch_register_t(const RegisterArgs &a, const LaunchCfg &cfg, cudaStream_t s)
 {
-    size_t smem = (size_t)(1 + TableLayout<Real>::kTParts) * a.t.nC * 6 * sizeof(Real);
+    size_t smem = (size_t)(1 + TableLayout<Real>::kTParts) * a.t.nC * 6 * sizeof(Real) +
+                  (size_t)a.tile_px * sizeof(double);
     auto kern = k_register_ll<TESS, Real>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

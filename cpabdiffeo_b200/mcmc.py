@@ -70,6 +70,19 @@ class BatchedMetropolis:
                                        _lib.ptr(self.prior_prec), self.wlp, _lib.ptr(self.lp), self.rule, self.seed,
                                        _lib.ptr(self.step), _lib.ptr(self.n_accepted), s))
 
+    def capture(self, graph_steps: int) -> None:
+        """Capture `graph_steps` steps into a CUDA graph on the current stream
+        without a device-wide synchronisation (for servers that keep other
+        streams busy).  Needs one eager step beforehand; allocates nothing."""
+        g = torch.cuda.CUDAGraph()
+        g.capture_begin(capture_error_mode="thread_local")
+        try:
+            for _ in range(graph_steps):
+                self._step_launches()
+        finally:
+            g.capture_end()
+        self._graph, self._graph_steps = g, graph_steps
+
     def run(self, n_steps: int, graph_steps: int = 0) -> None:
         """Advance every chain by n_steps.  graph_steps > 0 captures that many
         steps in a CUDA graph (once) and replays it; the remainder runs eagerly."""

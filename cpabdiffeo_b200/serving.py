@@ -276,7 +276,15 @@ class CpabServer:
                 continue
             k = min(self.mcmc_slice, job["left"])
             with torch.cuda.stream(job["stream"]):
-                job["mh"].run(k)
+                mh = job["mh"]
+                if k == self.mcmc_slice and job.get("warm"):
+                    # full slices replay a CUDA graph captured on this stream (one host call per slice)
+                    if mh._graph is None:
+                        mh.capture(self.mcmc_slice)
+                    mh._graph.replay()
+                else:
+                    mh.run(k)
+                    job["warm"] = True
                 job["left"] -= k
                 if job["left"] == 0:
                     mh = job["mh"]

@@ -62,9 +62,12 @@ enum { CPAB_F64 = 0, CPAB_F32 = 1 };
  *                     (1D; cpab/cpa1d/calcs/ClosedFormInt.py:64-256). */
 enum { CPAB_SCHEME_REF = 0, CPAB_SCHEME_SIMPLE = 1, CPAB_SCHEME_EXACT = 2 };
 
-/* Counter slots written by calls that take `counters` (uint64[5], added to). */
+/* Counter slots written by calls that take `counters` (uint64[CPAB_CNT_N],
+ * added to): closed-form steps kept (cell visits for the exact scheme),
+ * fallback steps, midpoint sub-steps, points finished, points that hit the
+ * crossing cap, points with a NaN result, CTAs stopped by cpab_cancel. */
 enum { CPAB_CNT_FAST = 0, CPAB_CNT_FALLBACK = 1, CPAB_CNT_SUBSTEPS = 2, CPAB_CNT_POINTS = 3,
-       CPAB_CNT_FAILED = 4, CPAB_CNT_N = 5 };
+       CPAB_CNT_FAILED = 4, CPAB_CNT_NAN = 5, CPAB_CNT_CANCELLED = 6, CPAB_CNT_N = 7 };
 
 /* ------------------------------------------------------------------ context */
 
@@ -81,6 +84,18 @@ const char *cpab_last_error_string(const cpab_ctx *ctx);
 /* Number of cells and length of one cell's matrix (dim*(dim+1)). */
 int cpab_ctx_num_cells(const cpab_ctx *ctx);
 int cpab_ctx_cell_len(const cpab_ctx *ctx);
+
+/* Cancellation.  Each context owns a flag in mapped host memory that the
+ * persistent integration, exact and registration kernels read before every
+ * tile; once it is set they finish the tile in hand, skip the rest and count
+ * themselves in CPAB_CNT_CANCELLED (no device fault, no trap).  cpab_cancel
+ * may be called from any host thread while a launch runs; the flag stays set
+ * until cpab_clear_cancel.  CPAB_UNSUPPORTED if the context has no flag (it is
+ * allocated at cpab_ctx_create when a device is present).  No counterpart in
+ * the reference (its launches cannot be stopped). */
+int cpab_cancel(cpab_ctx *ctx);
+int cpab_clear_cancel(cpab_ctx *ctx);
+int cpab_cancel_requested(const cpab_ctx *ctx);
 
 /* 1D zero-velocity boundary epilogue: clamp outputs of calc_T to [lo, hi]
  * (threshold_krnl, cpab/cpaNd/_CpaSpace.py:35-43 and :655-664). */
