@@ -58,10 +58,11 @@ def parse():
     ap.add_argument("--theta", type=int, default=N_THETA)
     ap.add_argument("--serve-seconds", type=float, default=0.5,
                     help="seconds of Poisson arrivals (2000 req/s) for the serving leg; 0 skips it")
-    ap.add_argument("--workload", default="batched_1d", choices=["batched_1d", "batched_2d_nc64"],
+    ap.add_argument("--workload", default="batched_1d", choices=["batched_1d", "batched_2d_nc64", "remap_ssd"],
                     help="batched_1d: the headline (1D nC=100, 4096 theta, ragged); batched_2d_nc64: the reference "
                          "scheme in FP32 on 2D tess I 4x4 (nC=64), 4096 theta x 8192 points, for the "
-                         "integration kernel's FP32 roofline")
+                         "integration kernel's FP32 roofline; remap_ssd: remap + SSD of 256 pairs of 256x256 "
+                         "images through FP32 maps, for its HBM roofline")
     return ap.parse_args()
 
 
@@ -426,36 +427,7 @@ def other_configs(torch, dev) -> dict:
                                           "pixels_per_s": C * H * H / (ms * 1e-3),
                                           "accept_pct_mean": float(mh.accept_ratio().mean())}
 
-    # standalone remap + SSD at the MCMC scale: 256 FP32 maps [256^2, 2] precomputed (the chains' current
-    # transforms), src and dst [256, 256, 256] float32; 16 algorithmic bytes per pixel; L2 flushed before each call
-    from cpabdiffeo_b200.registration import remap_ssd
-    sp2d = CpaSpace([0, 0], [1, 1], (4, 4), tess="I", device=dev, precision=torch.float32)
-    xs = torch.as_tensor(pixel_centers(H, H), dtype=torch.float32, device=dev)
-    tab = sp2d.tables_from_theta(mh.theta, DT, -1)
-    maps = torch.empty((C * H * H, 2), dtype=torch.float32, device=dev)
-    offs = torch.arange(C + 1, dtype=torch.int64, device=dev) * (H * H)
-    sp2d.calc_T_batched(tab, xs.repeat(C, 1), maps, offsets=offs, **p)
-    maps = maps.view(C, H * H, 2)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    pm = (H, -0.5, H, -0.5)
-    for _ in range(3):
-        remap_ssd(maps, srcg, dst, 0.05, pixel_map=pm)
-    times = []
-    for _ in range(10):
-        flush.zero_()
-        a, b = ev(), ev()
-        a.record()
-        remap_ssd(maps, srcg, dst, 0.05, pixel_map=pm)
-        b.record()
-        b.synchronize()
-        times.append(a.elapsed_time(b))
-    ms_r = float(np.median(times))
-    nbytes = 16 * C * H * H
-    pk = measured_peaks(torch).get("hbm_gbs")
-    out["remap_ssd_256x256sq_f32_map"] = {"ms": ms_r, "algorithmic_bytes": nbytes,
-                                          "achieved_gbs": nbytes / (ms_r * 1e-3) / 1e9, "hbm_peak_gbs": pk,
-                                          "frac": (nbytes / (ms_r * 1e-3) / 1e9 / pk) if pk else None,
-                                          "l2": "256 MB buffer written before each timed call"}
+    out["remap_ssd_256x256sq_f32_map"] = remap_ssd_c3(torch, dev, mh.theta, srcg, dst)
     return out
 
 
@@ -550,6 +522,73 @@ def bench_2d(args, torch, dev) -> dict:
             "error_vs_fp64_oracle": {"max_abs": err, "points_checked": 4 * npt, "tolerance": 1e-5}}
 
 
+def remap_ssd_c3(torch, dev, theta, src, dst, reps: int = 10) -> dict:
+    """Standalone remap + SSD at the MCMC scale: C FP32 maps [256^2, 2]
+    (the inverse transforms of theta [C, d] applied to the pixel centres),
+    src and dst [C, 256, 256] float32; 16 algorithmic bytes per pixel (map 8,
+    src 4, dst 4); a 256 MB buffer is written before each timed call."""
+    from cpabdiffeo_b200.cpa_space import CpaSpace
+    from cpabdiffeo_b200.registration import remap_ssd
+    from cpabdiffeo_b200.space import pixel_centers
+    C, H, W = src.shape
+    p = dict(dt=DT, nTimeSteps=NT, nStepsODEsolver=NODE)
+    sp2d = CpaSpace([0, 0], [1, 1], (4, 4), tess="I", device=dev, precision=torch.float32)
+    xs = torch.as_tensor(pixel_centers(H, W), dtype=torch.float32, device=dev)
+    tab = sp2d.tables_from_theta(theta, DT, -1)
+    maps = torch.empty((C * H * W, 2), dtype=torch.float32, device=dev)
+    offs = torch.arange(C + 1, dtype=torch.int64, device=dev) * (H * W)
+    sp2d.calc_T_batched(tab, xs.repeat(C, 1), maps, offsets=offs, **p)
+    maps = maps.view(C, H * W, 2)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    pm = (W, -0.5, H, -0.5)
+    for _ in range(3):
+        remap_ssd(maps, src, dst, 0.05, pixel_map=pm)
+    times = []
+    torch.cuda.nvtx.range_push("timed_remap")
+    for _ in range(reps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        remap_ssd(maps, src, dst, 0.05, pixel_map=pm)
+        b.record()
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    torch.cuda.nvtx.range_pop()
+    ms_r = float(np.median(times))
+    nbytes = 16 * C * H * W
+    pk = measured_peaks(torch).get("hbm_gbs")
+    ach = nbytes / (ms_r * 1e-3) / 1e9
+    return {"ms": ms_r, "images": C, "side": H, "algorithmic_bytes": nbytes, "achieved_gbs": ach,
+            "hbm_peak_gbs": pk, "frac": ach / pk if pk else None,
+            "l2": "256 MB buffer written before each timed call"}
+
+
+def bench_remap(args, torch, dev) -> dict:
+    """remap + SSD of 256 image pairs 256x256 through precomputed FP32 maps."""
+    from scipy.ndimage import gaussian_filter
+
+    from cpabdiffeo_b200.space import Prior, build_space
+    rng = np.random.default_rng(3)
+    C, H = 256, 256
+    geo = build_space(2, (4, 4), "I")
+    theta = torch.as_tensor(Prior.create(geo, 0.1, 1.0).sample(C, rng), device=dev)
+    src = torch.as_tensor(np.stack([gaussian_filter(rng.uniform(0, 1, (H, H)).astype(np.float32), 8.0)
+                                    for _ in range(C)]), device=dev)
+    dst = src + 0.02 * torch.randn_like(src)
+    with ClockSampler(dev.index or 0) as clk:
+        r = remap_ssd_c3(torch, dev, theta, src, dst, reps=max(args.steps, 3))
+    px = C * H * H
+    return {"metric": METRIC, "value": px / (r["ms"] * 1e-3), "unit": "pixels/s", "n_gpus": 1,
+            "steps": max(args.steps, 3), "warmup": 3, "ms_per_step": r["ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (smoothed noise images)",
+            "config": {"workload": "remap_ssd_256images_256x256_f32_maps", "l2": r["l2"]},
+            "gpu_launches": max(args.steps, 3), "clocks": clk.summary(),
+            "roofline": {"bound": "hbm", "kernel": "k_remap_ssd<float>", "achieved": r["achieved_gbs"],
+                         "peak": r["hbm_peak_gbs"], "unit": "GB/s", "frac": r["frac"],
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                         "bytes_per_pixel": 16, "traffic": None}}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -566,8 +605,8 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if args.workload == "batched_2d_nc64":
-        line = bench_2d(args, torch, dev)
+    if args.workload != "batched_1d":
+        line = bench_2d(args, torch, dev) if args.workload == "batched_2d_nc64" else bench_remap(args, torch, dev)
         if rank == 0:
             print(json.dumps(line), flush=True)
         return

@@ -33,7 +33,7 @@ def nvcc() -> str:
 def _compile(src: Path, verbose: bool) -> Path:
     obj = BUILD / (src.stem + ".o")
     if obj.exists() and obj.stat().st_mtime >= max(
-            [src.stat().st_mtime] + [h.stat().st_mtime for h in CSRC.glob("*.h*")] +
+            [src.stat().st_mtime] + [h.stat().st_mtime for h in (*CSRC.glob("*.h"), *CSRC.glob("*.cuh"))] +
             [p.stat().st_mtime for p in (PKG.parent / "include").glob("*.h")]):
         return obj
     cmd = [nvcc(), *NVCC_FLAGS, "-I", str(CSRC), "-I", str(PKG.parent / "include"), "-c", str(src), "-o", str(obj)]

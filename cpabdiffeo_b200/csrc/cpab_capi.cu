@@ -135,6 +135,7 @@ int cpab_expm(cpab_ctx *ctx, const double *A, int N, double dt, int sign, double
     if (N < 0) return fail(ctx, CPAB_BAD_SHAPE, "N < 0");
     if (N == 0) return CPAB_OK;
     if (!A || !Trels) return fail(ctx, CPAB_BAD_ARG, "A/Trels is NULL");
+    CPAB_CHECK_ALIGN(ctx, {A, 8, "A"}, {signedA, 8, "signedA"}, {Trels, 8, "Trels"});
     if (sign != 1 && sign != -1) return fail(ctx, CPAB_BAD_ARG, "sign must be +1 or -1");
     if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
     return cuda_status(ctx, launch_expm(ctx->t.dim, A, signedA, Trels, (int64_t)N * ctx->t.nC, dt, (double)sign,
@@ -149,6 +150,8 @@ int cpab_theta_to_trels(cpab_ctx *ctx, const double *B, int d, const double *the
     if (N < 0 || d < 1) return fail(ctx, CPAB_BAD_SHAPE, "need N >= 0 and d >= 1");
     if (N == 0) return CPAB_OK;
     if (!B || !theta || !Trels) return fail(ctx, CPAB_BAD_ARG, "B/theta/Trels is NULL");
+    CPAB_CHECK_ALIGN(ctx, {B, 8, "B"}, {theta, 8, "theta"}, {A, 8, "A"}, {signedA, 8, "signedA"},
+                     {Trels, 8, "Trels"});
     if (sign != 1 && sign != -1) return fail(ctx, CPAB_BAD_ARG, "sign must be +1 or -1");
     if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
     return cuda_status(ctx, launch_theta_to_trels(ctx->t.dim, B, theta, d, ctx->t.nC, N, dt, (double)sign, A,
@@ -162,6 +165,7 @@ int cpab_calc_cell_idx(cpab_ctx *ctx, const double *pts, int32_t *cell_idx, int6
     if (nPts < 0) return fail(ctx, CPAB_BAD_SHAPE, "nPts < 0");
     if (nPts == 0) return CPAB_OK;
     if (!pts || !cell_idx) return fail(ctx, CPAB_BAD_ARG, "pts/cell_idx is NULL");
+    CPAB_CHECK_ALIGN(ctx, {pts, 8, "pts"}, {cell_idx, 4, "cell_idx"});
     return cuda_status(ctx, launch_cell_idx(ctx->t, pts, cell_idx, nPts, (cudaStream_t)stream), "cell_idx launch");
 }
 
@@ -171,6 +175,7 @@ int cpab_calc_v(cpab_ctx *ctx, const double *A, const double *pts, double *vel, 
     if (nPts < 0) return fail(ctx, CPAB_BAD_SHAPE, "nPts < 0");
     if (nPts == 0) return CPAB_OK;
     if (!A || !pts || !vel) return fail(ctx, CPAB_BAD_ARG, "A/pts/vel is NULL");
+    CPAB_CHECK_ALIGN(ctx, {A, 8, "A"}, {pts, 8, "pts"}, {vel, 8, "vel"});
     size_t bytes = (size_t)nPts * ctx->t.dim * 8;
     if (overlaps(pts, bytes, vel, bytes)) return fail(ctx, CPAB_ALIAS, "pts and vel overlap");
     if ((size_t)ctx->t.nC * cell_len(ctx) * 8 > (size_t)max_smem_optin())
@@ -196,6 +201,8 @@ static int check_integrate(cpab_ctx *ctx, const double *signedA, const double *T
     if (!signedA) return fail(ctx, CPAB_BAD_ARG, "signedA is NULL");
     if (scheme == CPAB_SCHEME_REF && !Trels) return fail(ctx, CPAB_BAD_ARG, "Trels is NULL");
     if (nPts > 0 && (!pts || !out)) return fail(ctx, CPAB_BAD_ARG, "pts/out is NULL");
+    const size_t el = precision == CPAB_F64 ? 8 : 4;
+    CPAB_CHECK_ALIGN(ctx, {signedA, 8, "signedA"}, {Trels, 8, "Trels"}, {pts, el, "pts"}, {out, el, "out"});
     size_t bytes = (size_t)nPts * ctx->t.dim * (precision == CPAB_F64 ? 8 : 4);
     if (nPts > 0 && overlaps(pts, bytes, out, bytes))
         return fail(ctx, CPAB_ALIAS, "pts and out cannot point to the same memory (_CpaCalcs.py:388)");
@@ -253,6 +260,7 @@ int cpab_calc_T(cpab_ctx *ctx, const double *signedA, const double *Trels, const
     if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
     int st = check_integrate(ctx, signedA, Trels, pts, out, nPts, precision, scheme, dt, nTimeSteps, nStepsODE);
     if (st != CPAB_OK) return st;
+    CPAB_CHECK_ALIGN(ctx, {counters, 8, "counters"});
     if (nPts == 0) return CPAB_OK;
     IntegrateArgs a = make_args(ctx, signedA, Trels, pts, out, dt, nTimeSteps, nStepsODE, counters);
     a.batch.N = 1;
@@ -286,6 +294,7 @@ int cpab_calc_T_batched(cpab_ctx *ctx, const double *signedA, const double *Trel
     if (st != CPAB_OK) return st;
     if (offsets && (!pts || !out)) return fail(ctx, CPAB_BAD_ARG, "pts/out is NULL");
     if (offsets && pts == out) return fail(ctx, CPAB_ALIAS, "pts and out are the same buffer");
+    CPAB_CHECK_ALIGN(ctx, {offsets, 8, "offsets"}, {workspace, 8, "workspace"}, {counters, 8, "counters"});
     cudaStream_t s = (cudaStream_t)stream;
     IntegrateArgs a = make_args(ctx, signedA, Trels, pts, out, dt, nTimeSteps, nStepsODE, counters);
     a.batch.N = N;
@@ -318,6 +327,7 @@ int cpab_calc_trajectory(cpab_ctx *ctx, const double *signedA, const double *Tre
     if (nPts < 0) return fail(ctx, CPAB_BAD_SHAPE, "nPts < 0");
     if (nPts == 0) return CPAB_OK;
     if (!pts || !traj) return fail(ctx, CPAB_BAD_ARG, "pts/traj is NULL");
+    CPAB_CHECK_ALIGN(ctx, {pts, 8, "pts"}, {traj, 8, "traj"});
     size_t in_bytes = (size_t)nPts * ctx->t.dim * 8, out_bytes = in_bytes * (size_t)(nTimeSteps + 1);
     if (overlaps(pts, in_bytes, traj, out_bytes)) return fail(ctx, CPAB_ALIAS, "pts and traj overlap");
     IntegrateArgs a = make_args(ctx, signedA, Trels, pts, traj, dt, nTimeSteps, nStepsODE, nullptr);

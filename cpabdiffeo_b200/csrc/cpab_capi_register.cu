@@ -61,6 +61,8 @@ int cpab_remap_ssd(cpab_ctx *ctx, const void *map, int map_precision, const floa
     if (dst && !(sigma > 0) ) return fail(ctx, CPAB_BAD_ARG, "sigma must be positive");
     if (!std::isfinite(sx) || !std::isfinite(ox) || !std::isfinite(sy) || !std::isfinite(oy))
         return fail(ctx, CPAB_BAD_ARG, "pixel mapping is not finite");
+    CPAB_CHECK_ALIGN(ctx, {map, map_precision == CPAB_F64 ? 8u : 4u, "map"}, {src, 4, "src"}, {dst, 4, "dst"},
+                     {warped, 4, "warped"}, {ll, 8, "ll"}, {workspace, 8, "workspace"});
     const int64_t tpi = tiles_of(H, W, kRemapTilePx);
     const WsLayout L = ws_layout(N, tpi);
     RemapArgs a;
@@ -112,6 +114,8 @@ int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
     if (precision != CPAB_F64 && precision != CPAB_F32)
         return fail(ctx, CPAB_BAD_DTYPE, "precision must be CPAB_F64 or CPAB_F32");
     if (!signedA || !Trels || !src || !dst || !ll) return fail(ctx, CPAB_BAD_ARG, "NULL argument");
+    CPAB_CHECK_ALIGN(ctx, {signedA, 8, "signedA"}, {Trels, 8, "Trels"}, {src, 4, "src"}, {dst, 4, "dst"},
+                     {ll, 8, "ll"}, {warped, 4, "warped"}, {workspace, 8, "workspace"}, {counters, 8, "counters"});
     if (!(sigma > 0)) return fail(ctx, CPAB_BAD_ARG, "sigma must be positive");
     if (nTimeSteps < 1 || nStepsODE < 1) return fail(ctx, CPAB_BAD_ARG, "nTimeSteps and nStepsODE must be >= 1");
     if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
@@ -178,6 +182,8 @@ int cpab_mcmc_propose(cpab_ctx *ctx, int C, int d, const double *theta, const do
     if (st != CPAB_OK) return st;
     if (C == 0) return CPAB_OK;
     if (!prop_std) return fail(ctx, CPAB_BAD_ARG, "prop_std is NULL");
+    CPAB_CHECK_ALIGN(ctx, {theta, 8, "theta"}, {prop_std, 8, "prop_std"}, {step, 8, "step"},
+                     {theta_prop, 8, "theta_prop"});
     if (!std::isfinite(scale)) return fail(ctx, CPAB_BAD_ARG, "scale is not finite");
     McmcArgs a;
     memset(&a, 0, sizeof(a));
@@ -202,6 +208,9 @@ int cpab_mcmc_accept(cpab_ctx *ctx, int C, int d, double *theta, const double *t
     if (prior_prec && !lp) return fail(ctx, CPAB_BAD_ARG, "lp is NULL (needed with prior_prec)");
     if (C > 0) {
         if (!ll || !ll_prop) return fail(ctx, CPAB_BAD_ARG, "ll/ll_prop is NULL");
+        CPAB_CHECK_ALIGN(ctx, {theta, 8, "theta"}, {theta_prop, 8, "theta_prop"}, {ll, 8, "ll"},
+                         {ll_prop, 8, "ll_prop"}, {prior_prec, 8, "prior_prec"}, {lp, 8, "lp"}, {step, 8, "step"},
+                         {n_accepted, 8, "n_accepted"});
         McmcArgs a;
         memset(&a, 0, sizeof(a));
         a.C = C;
@@ -259,6 +268,9 @@ int cpab_grad_theta(cpab_ctx *ctx, const double *B, int d, const double *signedA
     if (ck < 1) return fail(ctx, CPAB_BAD_ARG, "checkpoint stride must be >= 1");
     if (sign != 1 && sign != -1) return fail(ctx, CPAB_BAD_ARG, "sign must be +1 or -1");
     if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
+    CPAB_CHECK_ALIGN(ctx, {B, 8, "B"}, {signedA, 8, "signedA"}, {pts, 8, "pts"}, {grad_out, 8, "grad_out"},
+                     {out, 8, "out"}, {grad_pts, 8, "grad_pts"}, {gA, 8, "gA"}, {dtheta, 8, "dtheta"},
+                     {workspace, 8, "workspace"});
     if ((size_t)2 * ctx->t.nC * cell_len(ctx) * 8 > (size_t)max_smem_optin())
         return fail(ctx, CPAB_UNSUPPORTED, "cell tables exceed shared memory");
     const size_t need = cpab_grad_workspace_bytes(ctx, N, n_per_inst, nTimeSteps, ck);

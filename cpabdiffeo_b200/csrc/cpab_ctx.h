@@ -5,6 +5,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cstdint>
+#include <initializer_list>
 
 #include "../../include/cpab_b200.h"
 #include "cpab_internal.h"
@@ -48,6 +50,26 @@ inline bool overlaps(const void *a, size_t na, const void *b, size_t nb)
     const char *pa = (const char *)a, *pb = (const char *)b;
     return pa < pb + nb && pb < pa + na;
 }
+
+// Device arrays must be aligned to their element size (a misaligned access
+// faults the kernel).  Returns the name of the first offender, or nullptr.
+struct AlignReq {
+    const void *p;
+    size_t bytes;
+    const char *name;
+};
+inline const char *misaligned(std::initializer_list<AlignReq> reqs)
+{
+    for (const AlignReq &r : reqs)
+        if (r.p && (reinterpret_cast<uintptr_t>(r.p) % r.bytes) != 0) return r.name;
+    return nullptr;
+}
+
+#define CPAB_CHECK_ALIGN(ctx, ...)                                                                          \
+    do {                                                                                                    \
+        if (const char *m_ = ::cpab::misaligned({__VA_ARGS__}))                                             \
+            return fail(ctx, CPAB_BAD_ARG, "%s is not aligned to its element size", m_);                   \
+    } while (0)
 
 int max_smem_optin();
 

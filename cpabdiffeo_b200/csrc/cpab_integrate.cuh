@@ -123,75 +123,72 @@ __device__ __forceinline__ int cell_of(const Tess &t, const PState<DIM, float> &
     return fast_cell<DIM, TESS>(t, s.hi);
 }
 
-// Closed-form step with the table of cell c; kept (returns true) if the end
-// point is still in cell c.
-// cq receives the cell of the end point (equal to c when kept).
-template <int DIM, int TESS>
-__device__ __forceinline__ bool try_fast(const Tess &t, PState<DIM, double> &s, const double *T, int tab, int c,
-                                         int &cq)
+// One unit of work on a point in cell c: the candidate end point q of a
+// closed-form step (fast: q = T_c [p; 1]) or of one explicit-midpoint
+// sub-step with A_c.  The caller looks up the cell of q; a closed-form step
+// is kept when that is still c (calc_2Dto2D.cu:380-400), a sub-step always
+// is, and its end cell is the cell of the next sub-step's start point.
+//   double: the reference's arithmetic (exact_affine / exact_midpoint).
+//   float:  both kinds share the first matrix-vector product (T - I)_hi [p; 1]
+//           resp. A [p; 1] and the compensated update, so a warp whose lanes
+//           mix closed-form steps and sub-steps diverges only in between.
+template <int DIM>
+__device__ __forceinline__ void advance(bool fast, const PState<DIM, double> &s, const double *A, const double *T,
+                                        const double *, double h, PState<DIM, double> &q)
 {
-    double q[DIM];
-    exact_affine<DIM>(q, T + c * DIM * (DIM + 1), s.p);
-    cq = exact_cell<DIM, TESS>(t, q);
-    if (cq != c) return false;
-#pragma unroll
-    for (int i = 0; i < DIM; ++i) s.p[i] = q[i];
-    return true;
+    if (fast) {
+        exact_affine<DIM>(q.p, T, s.p);
+    } else {
+        q = s;
+        exact_midpoint<DIM>(q.p, A, h);
+    }
 }
-template <int DIM, int TESS>
-__device__ __forceinline__ bool try_fast(const Tess &t, PState<DIM, float> &s, const float *T, int tab, int c,
-                                         int &cq)
+template <int DIM>
+__device__ __forceinline__ void advance(bool fast, const PState<DIM, float> &s, const float *A, const float *Th,
+                                        const float *Tl, float h, PState<DIM, float> &q)
 {
     constexpr int NH = DIM + 1;
-    const float *Th = T + c * DIM * NH, *Tl = Th + tab;
-    PState<DIM, float> q;
+    float y[DIM], d[DIM];
+    fast_affine<DIM>(y, fast ? Th : A, s.hi);
+    if (fast) {
+        // d = (T - I)[p; 1] with the lo table and the lo part of p: small terms first
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) {
+            float e = Tl[r * NH + DIM];
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) {
+                e = fmaf(Tl[r * NH + k], s.hi[k], e);
+                e = fmaf(Th[r * NH + k], s.lo[k], e);
+            }
+            d[r] = y[r] + e;
+        }
+    } else {
+        float pm[DIM];
+        const float hh = 0.5f * h;
+#pragma unroll
+        for (int i = 0; i < DIM; ++i) pm[i] = fmaf(hh, y[i], s.hi[i]);
+        fast_affine<DIM>(y, A, pm);
+#pragma unroll
+        for (int i = 0; i < DIM; ++i) d[i] = h * y[i];
+    }
 #pragma unroll
     for (int r = 0; r < DIM; ++r) {
-        // d = (T - I)[r] . [p; 1], hi and lo parts of the table, hi + lo of p
-        float d = Th[r * NH + DIM] + Tl[r * NH + DIM];
-#pragma unroll
-        for (int k = 0; k < DIM; ++k) {
-            d = fmaf(Th[r * NH + k], s.hi[k], d);
-            d = fmaf(Tl[r * NH + k], s.hi[k], d);
-            d = fmaf(Th[r * NH + k], s.lo[k], d);
-        }
         q.hi[r] = s.hi[r];
         q.lo[r] = s.lo[r];
-        acc_add(q.hi[r], q.lo[r], d);
+        acc_add(q.hi[r], q.lo[r], d[r]);
     }
-    cq = fast_cell<DIM, TESS>(t, q.hi);
-    if (cq != c) return false;
-    s = q;
-    return true;
-}
-
-template <int DIM>
-__device__ __forceinline__ void substep(PState<DIM, double> &s, const double *A, double h)
-{
-    exact_midpoint<DIM>(s.p, A, h);
-}
-template <int DIM>
-__device__ __forceinline__ void substep(PState<DIM, float> &s, const float *A, float h)
-{
-    float v[DIM], pm[DIM];
-    fast_affine<DIM>(v, A, s.hi);
-    const float hh = 0.5f * h;
-#pragma unroll
-    for (int i = 0; i < DIM; ++i) pm[i] = fmaf(hh, v[i], s.hi[i]);
-    fast_affine<DIM>(v, A, pm);
-#pragma unroll
-    for (int i = 0; i < DIM; ++i) acc_add(s.hi[i], s.lo[i], h * v[i]);
 }
 
 // ------------------------------------------------------------ integration
 
 // One warp integrates the points [ws, we).  Every lane owns one point and
 // advances it by one unit per iteration -- a closed-form Trel step or one
-// midpoint sub-step, which cost about the same -- and claims the next
-// unprocessed point of the range as soon as its own is finished.  A point
-// that falls back to nStepsODE sub-steps therefore keeps one lane busy, not
-// the whole warp.  Results do not depend on the schedule: each point follows
-// exactly the reference's sequence of operations.
+// midpoint sub-step, which cost about the same and share most of their
+// instructions (advance) -- and claims the next unprocessed point of the
+// range as soon as its own is finished.  A point that falls back to
+// nStepsODE sub-steps therefore keeps one lane busy, not the whole warp.
+// Results do not depend on the schedule: each point follows exactly the
+// reference's sequence of operations.
 //   Src::load(idx, st)     sets the start state of point idx
 //   Snk::put(idx, st)      receives the end state (PState; get() converts)
 //   perm (optional, shared memory): the k-th point of the range is
@@ -200,9 +197,11 @@ __device__ __forceinline__ void substep(PState<DIM, float> &s, const float *A, f
 //   share one queue over [ws, we) -- a warp whose lanes finish claims the next
 //   points of the whole tile, so no warp idles at the end-of-tile barrier
 //   while another still works through a fixed slice.
-// The reference recomputes the start cell of every time step; after a kept
-// closed-form step that cell was just computed for the same point, so it is
-// reused (identical value, one lookup per step saved).
+// Every iteration ends with one cell lookup, of the candidate end point: for
+// a closed-form step it is the reference's keep test, for a sub-step it is
+// the cell the next sub-step (or the next time step) starts in, which the
+// reference would look up from the same point.  So each lane always knows
+// the cell of its current point.
 template <int DIM, int TESS, typename Real, int SCHEME, class Src, class Snk>
 __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE, const Real *sA, const Real *sT,
                                                 int64_t ws, int64_t we, Real h, const Src &src, Snk &snk,
@@ -212,6 +211,7 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
                                                 unsigned long long *claim = nullptr)
 {
     constexpr int NE = DIM * (DIM + 1);
+    constexpr bool kTwoPart = TableLayout<Real>::kTParts == 2;
     const int tab = t.nC * NE;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -227,33 +227,35 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
     bool active = k < we;
     int64_t idx = (active && perm) ? perm_base + perm[k - perm_base] : k;
     PState<DIM, Real> st;
-    int steps_left = 0, sub_left = 0, known_cell = -1;
+    int steps_left = 0, sub_left = 0, c = 0;
     if (active) {
         src.load(idx, st);
+        c = cell_of<DIM, TESS>(t, st);
         steps_left = nT;
         sub_left = (SCHEME == SCHEME_SIMPLE) ? nT * nODE : 0;
     }
     while (__any_sync(FULL, active)) {
         bool fin = false;
         if (active) {
-            if (SCHEME == SCHEME_REF && sub_left == 0) {
-                const int c = known_cell >= 0 ? known_cell : cell_of<DIM, TESS>(t, st);
-                int cq;
-                if (try_fast<DIM, TESS>(t, st, sT, tab, c, cq)) {
+            const bool fast = (SCHEME == SCHEME_REF) && sub_left == 0;
+            PState<DIM, Real> q;
+            advance<DIM>(fast, st, sA + c * NE, sT + c * NE, kTwoPart ? sT + tab + c * NE : nullptr, h, q);
+            const int cq = cell_of<DIM, TESS>(t, q);
+            if (fast && cq != c) {
+                // the end point left the cell: redo the step with nStepsODE sub-steps from p
+                sub_left = nODE;
+                ++c_fb;
+            } else {
+                st = q;
+                c = cq;
+                if (fast) {
                     --steps_left;
                     ++c_fast;
-                    known_cell = cq;
                 } else {
-                    sub_left = nODE;
-                    ++c_fb;
-                    known_cell = -1;
+                    --sub_left;
+                    ++c_sub;
+                    if (SCHEME == SCHEME_REF && sub_left == 0) --steps_left;
                 }
-            } else {
-                const int c = cell_of<DIM, TESS>(t, st);
-                substep<DIM>(st, sA + c * NE, h);
-                --sub_left;
-                ++c_sub;
-                if (sub_left == 0) --steps_left;
             }
             fin = (SCHEME == SCHEME_SIMPLE) ? (sub_left == 0) : (steps_left == 0);
             if (fin) {
@@ -277,9 +279,9 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
                 if (active) {
                     idx = perm ? perm_base + perm[k - perm_base] : k;
                     src.load(idx, st);
+                    c = cell_of<DIM, TESS>(t, st);
                     steps_left = nT;
                     sub_left = (SCHEME == SCHEME_SIMPLE) ? nT * nODE : 0;
-                    known_cell = -1;
                 }
             }
             next += __popc(done);

@@ -79,26 +79,110 @@ __device__ void finish_tile(double acc, int64_t tile, int inst, int tiles_of_ins
 
 // ------------------------------------------------------------ standalone remap (+ SSD)
 
+__device__ __forceinline__ void load_pair(const float *p, float &x, float &y)
+{
+    const float2 v = __ldg(reinterpret_cast<const float2 *>(p));
+    x = v.x;
+    y = v.y;
+}
+
+__device__ __forceinline__ void load_pair(const double *p, double &x, double &y)
+{
+    const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+    x = v.x;
+    y = v.y;
+}
+
+// Bilinear sampling split in two halves so that a thread can issue the tap
+// loads of several pixels before it needs any of them: same arithmetic as
+// bilinear().
+struct TapSet {
+    float v[4];      // (r0, c0), (r0, c0 + 1), (r0 + 1, c0), (r0 + 1, c0 + 1)
+    double fx, fy;
+    bool inside;
+};
+
+__device__ __forceinline__ void taps_issue(const float *img, int H, int W, double px, double py, TapSet &t)
+{
+    const double fx0 = floor(px), fy0 = floor(py);
+    t.inside = fx0 > -2.0 && fx0 < (double)W + 1.0 && fy0 > -2.0 && fy0 < (double)H + 1.0;
+    t.fx = px - fx0;
+    t.fy = py - fy0;
+    const int c0 = t.inside ? (int)fx0 : -2, r0 = t.inside ? (int)fy0 : -2;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int r = r0 + (k >> 1), c = c0 + (k & 1);
+        t.v[k] = (r >= 0 && r < H && c >= 0 && c < W) ? __ldg(img + (int64_t)r * W + c) : 0.0f;
+    }
+}
+
+__device__ __forceinline__ double taps_combine(const TapSet &t)
+{
+    if (!t.inside) return 0.0;
+    const double top = (1 - t.fx) * (double)t.v[0] + t.fx * (double)t.v[1];
+    const double bot = (1 - t.fx) * (double)t.v[2] + t.fx * (double)t.v[3];
+    return (1 - t.fy) * top + t.fy * bot;
+}
+
+// Each thread handles kRemapBatch pixels per round (stride blockDim.x, so a
+// warp's accesses stay coalesced): all map and dst loads of the round are
+// issued first, then all tap loads, then the arithmetic -- enough loads in
+// flight per SM to stream HBM.  Per-thread sums keep pixel order.
+constexpr int kRemapBatch = 4;
+
 template <typename MapT>
-__global__ void __launch_bounds__(256) k_remap_ssd(RemapArgs a)
+__global__ void __launch_bounds__(256, 3) k_remap_ssd(RemapArgs a)
 {
     const int inst = blockIdx.y;
     const int64_t npx = (int64_t)a.H * a.W;
     const int64_t tile = blockIdx.x;
-    const int64_t start = tile * a.tile_px, end = min(start + (int64_t)a.tile_px, npx);
-    const MapT *map = static_cast<const MapT *>(a.map) + (int64_t)inst * npx * 2;
+    const int64_t start = tile * a.tile_px;
+    const int n = (int)(min(start + (int64_t)a.tile_px, npx) - start);   // pixels of this tile
+    // tile-relative pointers: the per-pixel indices below are 32-bit
+    const int64_t off = (int64_t)inst * npx + start;
+    const MapT *map = static_cast<const MapT *>(a.map) + 2 * off;
     const float *src = a.src + (int64_t)inst * npx;
-    const float *dst = a.dst ? a.dst + (int64_t)inst * npx : nullptr;
-    float *warped = a.warped ? a.warped + (int64_t)inst * npx : nullptr;
+    const float *dst = a.dst ? a.dst + off : nullptr;
+    float *warped = a.warped ? a.warped + off : nullptr;
     const double k = -0.5 / (a.sigma * a.sigma);
     double acc = 0.0;
-    for (int64_t i = start + threadIdx.x; i < end; i += blockDim.x) {
-        double mx = (double)map[2 * i], my = (double)map[2 * i + 1];
-        double w = bilinear(src, a.H, a.W, mx * a.sx + a.ox, my * a.sy + a.oy);
-        if (warped) warped[i] = (float)w;
-        if (dst) {
-            double e = w - (double)__ldg(dst + i);
-            acc += e * e * k;
+    // one vector load per (x, y) pair when the map is aligned for it (uniform over the launch)
+    const bool vec = (reinterpret_cast<uintptr_t>(a.map) & (2 * sizeof(MapT) - 1)) == 0;
+    for (int j0 = threadIdx.x; j0 < n; j0 += kRemapBatch * blockDim.x) {
+        MapT mx[kRemapBatch], my[kRemapBatch];
+        float dv[kRemapBatch];
+#pragma unroll
+        for (int u = 0; u < kRemapBatch; ++u) {
+            const int j = j0 + u * blockDim.x;
+            mx[u] = my[u] = 0;
+            dv[u] = 0.0f;
+            if (j < n) {
+                if (vec) {
+                    load_pair(map + 2 * j, mx[u], my[u]);
+                } else {
+                    mx[u] = map[2 * j];
+                    my[u] = map[2 * j + 1];
+                }
+                if (dst) dv[u] = __ldg(dst + j);
+            }
+        }
+        TapSet ts[kRemapBatch];
+#pragma unroll
+        for (int u = 0; u < kRemapBatch; ++u) {
+            if (j0 + u * (int)blockDim.x < n)
+                taps_issue(src, a.H, a.W, (double)mx[u] * a.sx + a.ox, (double)my[u] * a.sy + a.oy, ts[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < kRemapBatch; ++u) {
+            const int j = j0 + u * blockDim.x;
+            if (j < n) {
+                const double w = taps_combine(ts[u]);
+                if (warped) warped[j] = (float)w;
+                if (dst) {
+                    const double e = w - (double)dv[u];
+                    acc += e * e * k;
+                }
+            }
         }
     }
     if (dst) {

@@ -58,3 +58,29 @@ def test_ctx_create_validation():
     assert lib.cpab_calc_T(h, 8, 8, 16, 16, 10, 0, 2, 0.02, 50, 100, None, None) == 10  # exact needs 1D
     assert lib.cpab_set_launch(h, 48, 0, 0) == 1
     assert lib.cpab_ctx_destroy(h) == 0
+
+
+def test_misaligned_pointers_are_rejected_before_launch():
+    """A device pointer that is not aligned to its element size returns
+    CPAB_BAD_ARG naming the argument (a misaligned access would fault the GPU)."""
+    lib = _lib.load()
+    h = C.c_void_p()
+    nCs = (C.c_int * 3)(4, 4, 1)
+    incs = (C.c_double * 3)(0.25, 0.25, 1.0)
+    assert lib.cpab_ctx_create(C.byref(h), 2, 1, nCs, incs) == 0
+    base = 1 << 20
+    # FP64 points at a 4-byte offset
+    assert lib.cpab_calc_T(h, base, base, base + 4096 + 4, base + 8192, 10, 0, 0, 0.02, 50, 100, None, None) == 1
+    assert b"pts is not aligned" in lib.cpab_last_error_string(h)
+    # FP32 points at a 4-byte offset are fine up to the table check; the tables must be 8-aligned
+    assert lib.cpab_calc_T(h, base + 4, base, base + 4096, base + 8192, 10, 1, 0, 0.02, 50, 100, None, None) == 1
+    assert b"signedA is not aligned" in lib.cpab_last_error_string(h)
+    # cell index output at an odd address
+    assert lib.cpab_calc_cell_idx(h, base, base + 4096 + 2, 10, None) == 1
+    assert b"cell_idx is not aligned" in lib.cpab_last_error_string(h)
+    # remap with a float64 map on a 4-byte boundary
+    assert lib.cpab_remap_ssd(h, base + 4, 0, base + 4096, None, 1, 8, 8, 1.0, 0.0, 1.0, 0.0, 1.0,
+                              base + 8192, None, None, 0, None) == 1
+    assert b"map is not aligned" in lib.cpab_last_error_string(h)
+    assert lib.cpab_ctx_destroy(h) == 0
+
