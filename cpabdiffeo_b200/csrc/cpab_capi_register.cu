@@ -3,6 +3,7 @@
 #include <cmath>
 
 #include "cpab_ctx.h"
+#include "cpab_landmarks.h"
 #include "cpab_register.h"
 
 using namespace cpab;
@@ -154,6 +155,73 @@ int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
     if (e != cudaSuccess) return cuda_status(ctx, e, "ticket reset");
     return cuda_status(ctx, launch_register_ll(a, precision == CPAB_F64 ? PREC_F64 : PREC_F32, ctx->cfg, s),
                        "register_ll launch");
+}
+
+size_t cpab_landmark_workspace_bytes(const cpab_ctx *ctx, int N, int n_lm)
+{
+    if (!ctx || N < 0 || n_lm < 1) return 0;
+    return ws_layout(N, ((int64_t)n_lm + ctx->cfg.tile_pts - 1) / ctx->cfg.tile_pts).total;
+}
+
+int cpab_landmark_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, int N, const double *src,
+                     int64_t src_stride, const double *dst, int64_t dst_stride, int n_lm, double sigma, int precision,
+                     double dt, int nTimeSteps, int nStepsODE, double *ll, double *transformed, void *workspace,
+                     size_t workspace_bytes, uint64_t *counters, void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (N < 0 || n_lm < 1) return fail(ctx, CPAB_BAD_SHAPE, "need N >= 0 and n_lm >= 1");
+    if (src_stride < 0 || dst_stride < 0) return fail(ctx, CPAB_BAD_SHAPE, "strides must be >= 0");
+    if (N == 0) return CPAB_OK;
+    if (precision != CPAB_F64 && precision != CPAB_F32)
+        return fail(ctx, CPAB_BAD_DTYPE, "precision must be CPAB_F64 or CPAB_F32");
+    if (!signedA || !Trels || !src || !dst || !ll) return fail(ctx, CPAB_BAD_ARG, "NULL argument");
+    if (!(sigma > 0)) return fail(ctx, CPAB_BAD_ARG, "sigma must be positive");
+    if (nTimeSteps < 1 || nStepsODE < 1) return fail(ctx, CPAB_BAD_ARG, "nTimeSteps and nStepsODE must be >= 1");
+    if ((long long)nTimeSteps * nStepsODE > 0x7fffffffLL)
+        return fail(ctx, CPAB_BAD_ARG, "nTimeSteps * nStepsODE overflows");
+    if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
+    CPAB_CHECK_ALIGN(ctx, {signedA, 8, "signedA"}, {Trels, 8, "Trels"}, {src, 8, "src"}, {dst, 8, "dst"},
+                     {ll, 8, "ll"}, {transformed, 8, "transformed"}, {workspace, 8, "workspace"},
+                     {counters, 8, "counters"});
+    const int prec = precision == CPAB_F64 ? PREC_F64 : PREC_F32;
+    if (landmark_smem_bytes(ctx->t, ctx->cfg.tile_pts, prec) > (size_t)max_smem_optin())
+        return fail(ctx, CPAB_UNSUPPORTED, "cell tables and tile scratch exceed shared memory");
+    const size_t need = cpab_landmark_workspace_bytes(ctx, N, n_lm);
+    if (!workspace || workspace_bytes < need) return fail(ctx, CPAB_NO_MEMORY, "workspace of %zu bytes needed", need);
+    if (transformed) {
+        const size_t tb = (size_t)N * n_lm * ctx->t.dim * 8;
+        if (overlaps(transformed, tb, src, (size_t)((N - 1) * src_stride + n_lm) * ctx->t.dim * 8) ||
+            overlaps(transformed, tb, dst, (size_t)((N - 1) * dst_stride + n_lm) * ctx->t.dim * 8))
+            return fail(ctx, CPAB_ALIAS, "transformed overlaps src or dst");
+    }
+    const WsLayout L = ws_layout(N, ((int64_t)n_lm + ctx->cfg.tile_pts - 1) / ctx->cfg.tile_pts);
+    LandmarkArgs a;
+    memset(&a, 0, sizeof(a));
+    a.t = ctx->t;
+    a.A = signedA;
+    a.T = Trels;
+    a.src = src;
+    a.dst = dst;
+    a.src_stride = src_stride;
+    a.dst_stride = dst_stride;
+    a.transformed = transformed;
+    a.ll = ll;
+    char *w = static_cast<char *>(workspace);
+    a.partials = reinterpret_cast<double *>(w + L.partials_off);
+    a.tickets = reinterpret_cast<unsigned *>(w + L.tickets_off);
+    a.counters = reinterpret_cast<unsigned long long *>(counters);
+    a.N = N;
+    a.n_lm = n_lm;
+    a.tile_pts = ctx->cfg.tile_pts;
+    a.sigma = sigma;
+    a.dt = dt;
+    a.nTimeSteps = nTimeSteps;
+    a.nStepsODE = nStepsODE;
+    a.cancel = ctx->cancel_dev;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(a.tickets, 0, (size_t)N * sizeof(unsigned), s);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "ticket reset");
+    return cuda_status(ctx, launch_landmark_ll(a, prec, ctx->cfg, s), "landmark_ll launch");
 }
 
 }  // extern "C"

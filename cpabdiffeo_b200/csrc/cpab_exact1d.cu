@@ -159,14 +159,14 @@ __device__ bool cf_point(const Exact1D &e, const Transit &tr, double x, double t
 // Shared memory of k_exact1d: per cell A (2 doubles), b/a and 1/a (2),
 // entry points and hitting times (4 doubles), next and entry cells (4 ints)
 // -- 80 bytes, so what follows is 16-byte aligned -- and, when cell-sorting,
-// sorted start points and results in input order [tile_pts] (Real), start
-// cells and permutation [tile_pts] and the histogram [nC] (int).
+// sorted start points and results in input order [tile_pts] (Real), the
+// permutation [tile_pts] and the histogram [nC] (int).
 size_t exact1d_smem_bytes(int nC, int tile_pts, int sort, int prec)
 {
     size_t b = (size_t)nC * (8 * sizeof(double) + 4 * sizeof(int));
     if (sort)
         b += 2 * (size_t)tile_pts * (prec == PREC_F64 ? sizeof(double) : sizeof(float)) +
-             ((size_t)nC + 2 * (size_t)tile_pts) * sizeof(int);
+             ((size_t)nC + (size_t)tile_pts) * sizeof(int);
     return b;
 }
 
@@ -190,8 +190,7 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
     const int tp = a.batch.tile_pts;
     Real *s_xs = reinterpret_cast<Real *>(tr.cell1 + nC);
     Real *s_y = s_xs + tp;
-    int *s_cell = reinterpret_cast<int *>(s_y + tp);
-    int *s_perm = s_cell + tp;
+    int *s_perm = reinterpret_cast<int *>(s_y + tp);
     int *s_hist = s_perm + tp;
     __shared__ TileInfo s_tile;
     __shared__ int s_claim;
@@ -239,18 +238,17 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
             for (int j = threadIdx.x; j < n; j += blockDim.x) {
                 Real xin;
                 load_pt<1, Real>(a.pts_in, ti.start + j, &xin);
-                const int c = cf_cell(e, (double)xin);
                 s_y[j] = xin;
-                s_cell[j] = c;
-                atomicAdd(s_hist + c, 1);
+                atomicAdd(s_hist + cf_cell(e, (double)xin), 1);
             }
             __syncthreads();
             warp0_exclusive_scan(s_hist, nC);
             __syncthreads();
             for (int j = threadIdx.x; j < n; j += blockDim.x) {
-                const int pos = atomicAdd(s_hist + s_cell[j], 1);
+                const Real xin = s_y[j];
+                const int pos = atomicAdd(s_hist + cf_cell(e, (double)xin), 1);
                 s_perm[pos] = j;
-                s_xs[pos] = s_y[j];
+                s_xs[pos] = xin;
             }
             __syncthreads();
         }
@@ -301,7 +299,7 @@ cudaError_t launch_integrate_exact1d(const IntegrateArgs &a, int prec, const Lau
     const size_t smem = exact1d_smem_bytes(a.t.nC, a.batch.tile_pts, a.sort, prec);
     if (prec == PREC_F64) {
         auto kern = k_exact1d<double>;
-        if (smem > 48 * 1024) {
+        if (smem > kSmemOptInAbove) {
             cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
@@ -309,7 +307,7 @@ cudaError_t launch_integrate_exact1d(const IntegrateArgs &a, int prec, const Lau
         kern<<<grid, cfg.block, smem, s>>>(a);
     } else {
         auto kern = k_exact1d<float>;
-        if (smem > 48 * 1024) {
+        if (smem > kSmemOptInAbove) {
             cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }

@@ -178,7 +178,7 @@ static cudaError_t launch_grad_t(const GradArgs &a, cudaStream_t s)
     constexpr int NE = DIM * (DIM + 1);
     size_t smem = (size_t)2 * a.t.nC * NE * sizeof(double);
     auto kern = k_grad_simple<DIM, TESS>;
-    if (smem > 48 * 1024) {
+    if (smem > kSmemOptInAbove) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }

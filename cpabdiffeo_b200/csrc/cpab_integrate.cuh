@@ -12,13 +12,20 @@ namespace cpab {
 // Two per-point states:
 //  * double (bit-exact family): one double per coordinate, the reference's
 //    arithmetic (cpab_cell.cuh).
-//  * float (FP32 mode): a compensated pair hi + lo per coordinate (TwoSum,
-//    Knuth), so the many small increments of the integration are not lost to
-//    float rounding; velocities and cell lookups use hi.  The closed-form
-//    step table holds T - I split into a float pair (hi, lo), so rounding T to
-//    float does not bias every step; the velocity table A is plain float.
-// Shared-memory tables per cell:
-//  double: A[ne], T[ne];   float: A[ne], (T-I)_hi[ne], (T-I)_lo[ne].
+//  * float (FP32 mode): an unnormalised compensated pair hi + lo per
+//    coordinate plus x = fl(hi + lo), the float nearest the point, which the
+//    velocity, the closed-form step and the cell lookup read.  Each update
+//    adds its increment d to hi and the rounding error of that addition
+//    (Fast2Sum; |d| is a small step, and where |hi| < |d| the error term is
+//    below ulp(d)) to lo, so the many small increments of the integration are
+//    not lost to float rounding.  The closed-form step table holds T - I
+//    split into a float pair (hi, lo), so rounding T to float does not bias
+//    every step; the velocity table A is plain float.
+// Shared-memory tables per cell (ne = DIM * (DIM + 1)):
+//  double: A[ne], T[ne], row-major as in global memory;
+//  float:  A[ne], then per cell (T-I)_hi[ne] followed by (T-I)_lo[ne], each
+//          column-major (the DIM columns of the linear part, then the
+//          offset) so that a cell's matrix is read with 8- or 16-byte loads.
 
 template <int DIM, typename Real>
 struct PState;
@@ -41,47 +48,41 @@ struct PState<DIM, double> {
 
 template <int DIM>
 struct PState<DIM, float> {
-    float hi[DIM], lo[DIM];
-    __device__ __forceinline__ void set(const float *x)
+    float hi[DIM], lo[DIM], x[DIM];
+    __device__ __forceinline__ void set(const float *v)
     {
 #pragma unroll
-        for (int i = 0; i < DIM; ++i) { hi[i] = x[i]; lo[i] = 0.0f; }
+        for (int i = 0; i < DIM; ++i) { hi[i] = v[i]; lo[i] = 0.0f; x[i] = v[i]; }
     }
-    __device__ __forceinline__ void set(const double *x)
+    __device__ __forceinline__ void set(const double *v)
     {
 #pragma unroll
-        for (int i = 0; i < DIM; ++i) { hi[i] = (float)x[i]; lo[i] = (float)(x[i] - (double)hi[i]); }
+        for (int i = 0; i < DIM; ++i) {
+            hi[i] = (float)v[i];
+            lo[i] = (float)(v[i] - (double)hi[i]);
+            x[i] = hi[i] + lo[i];
+        }
     }
-    __device__ __forceinline__ void get(float *x) const
+    __device__ __forceinline__ void get(float *v) const
     {
 #pragma unroll
-        for (int i = 0; i < DIM; ++i) x[i] = hi[i] + lo[i];
+        for (int i = 0; i < DIM; ++i) v[i] = x[i];
     }
-    __device__ __forceinline__ void get(double *x) const
+    __device__ __forceinline__ void get(double *v) const
     {
 #pragma unroll
-        for (int i = 0; i < DIM; ++i) x[i] = (double)hi[i] + (double)lo[i];
+        for (int i = 0; i < DIM; ++i) v[i] = (double)hi[i] + (double)lo[i];
     }
-    __device__ __forceinline__ const float *lookup() const { return hi; }
+    __device__ __forceinline__ const float *lookup() const { return x; }
+    // hi + lo += d
+    __device__ __forceinline__ void add(int i, float d)
+    {
+        const float s = hi[i] + d;
+        lo[i] += d - (s - hi[i]);
+        hi[i] = s;
+        x[i] = s + lo[i];
+    }
 };
-
-// s + e == a + b exactly (Knuth's TwoSum).
-__device__ __forceinline__ void two_sum(float a, float b, float &s, float &e)
-{
-    s = a + b;
-    float bb = s - a;
-    e = (a - (s - bb)) + (b - bb);
-}
-
-// (hi, lo) += d, renormalised.
-__device__ __forceinline__ void acc_add(float &hi, float &lo, float d)
-{
-    float s, e;
-    two_sum(hi, d, s, e);
-    e += lo;
-    hi = s + e;
-    lo = e - (hi - s);
-}
 
 template <typename Real>
 struct TableLayout {
@@ -89,7 +90,7 @@ struct TableLayout {
     static constexpr int kTParts = sizeof(Real) == 8 ? 1 : 2;
 };
 
-// Stage one instance's tables in shared memory.
+// Stage one instance's tables in shared memory (layout above).
 template <int DIM, typename Real>
 __device__ __forceinline__ void stage_tables(const double *gA, const double *gT, int nC, bool with_T, Real *sA,
                                              Real *sT)
@@ -97,18 +98,58 @@ __device__ __forceinline__ void stage_tables(const double *gA, const double *gT,
     constexpr int NE = DIM * (DIM + 1);
     const int tab = nC * NE;
     for (int i = threadIdx.x; i < tab; i += blockDim.x) {
-        sA[i] = (Real)gA[i];
-        if (with_T) {
-            if (sizeof(Real) == 8) {
-                sT[i] = (Real)gT[i];
-            } else {
-                const int e = i % NE, r = e / (DIM + 1), c = e % (DIM + 1);
-                const double d = gT[i] - (r == c ? 1.0 : 0.0);
+        if (sizeof(Real) == 8) {
+            sA[i] = (Real)gA[i];
+            if (with_T) sT[i] = (Real)gT[i];
+        } else {
+            const int c = i / NE, e = i - c * NE, r = e / (DIM + 1), col = e - r * (DIM + 1);
+            const int cm = col * DIM + r;
+            sA[c * NE + cm] = (Real)gA[i];
+            if (with_T) {
+                const double d = gT[i] - (r == col ? 1.0 : 0.0);
                 const float hi = (float)d;
-                sT[i] = hi;
-                sT[tab + i] = (float)(d - (double)hi);
+                sT[c * 2 * NE + cm] = hi;
+                sT[c * 2 * NE + NE + cm] = (float)(d - (double)hi);
             }
         }
+    }
+}
+
+// A cell's column-major float matrix into registers (8-byte loads in 1D/2D,
+// 16-byte loads in 3D; the tables' offsets keep those aligned).
+template <int DIM>
+__device__ __forceinline__ void load_cell(const float *p, float *m)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    if (DIM == 3) {
+#pragma unroll
+        for (int i = 0; i < NE / 4; ++i) {
+            const float4 v = reinterpret_cast<const float4 *>(p)[i];
+            m[4 * i] = v.x;
+            m[4 * i + 1] = v.y;
+            m[4 * i + 2] = v.z;
+            m[4 * i + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < NE / 2; ++i) {
+            const float2 v = reinterpret_cast<const float2 *>(p)[i];
+            m[2 * i] = v.x;
+            m[2 * i + 1] = v.y;
+        }
+    }
+}
+
+// y = M [x; 1] for a column-major cell matrix held in registers
+template <int DIM>
+__device__ __forceinline__ void cm_affine(float *y, const float *m, const float *x)
+{
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) {
+        float acc = m[DIM * DIM + r];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) acc = fmaf(m[k * DIM + r], x[k], acc);
+        y[r] = acc;
     }
 }
 
@@ -120,7 +161,7 @@ __device__ __forceinline__ int cell_of(const Tess &t, const PState<DIM, double> 
 template <int DIM, int TESS>
 __device__ __forceinline__ int cell_of(const Tess &t, const PState<DIM, float> &s)
 {
-    return fast_cell<DIM, TESS>(t, s.hi);
+    return fast_cell<DIM, TESS>(t, s.x);
 }
 
 // One unit of work on a point in cell c: the candidate end point q of a
@@ -144,39 +185,33 @@ __device__ __forceinline__ void advance(bool fast, const PState<DIM, double> &s,
     }
 }
 template <int DIM>
-__device__ __forceinline__ void advance(bool fast, const PState<DIM, float> &s, const float *A, const float *Th,
-                                        const float *Tl, float h, PState<DIM, float> &q)
+__device__ __forceinline__ void advance(bool fast, const PState<DIM, float> &s, const float *A, const float *T,
+                                        const float *, float h, PState<DIM, float> &q)
 {
-    constexpr int NH = DIM + 1;
-    float y[DIM], d[DIM];
-    fast_affine<DIM>(y, fast ? Th : A, s.hi);
+    constexpr int NE = DIM * (DIM + 1);
+    float m[NE], y[DIM], d[DIM];
+    // (T - I)_hi for a closed-form step, A for a sub-step
+    load_cell<DIM>(fast ? T : A, m);
+    cm_affine<DIM>(y, m, s.x);
     if (fast) {
-        // d = (T - I)[p; 1] with the lo table and the lo part of p: small terms first
+        // d = (T - I)[x; 1], the lo part of the table added first
+        float l[NE], e[DIM];
+        load_cell<DIM>(T + NE, l);
+        cm_affine<DIM>(e, l, s.x);
 #pragma unroll
-        for (int r = 0; r < DIM; ++r) {
-            float e = Tl[r * NH + DIM];
-#pragma unroll
-            for (int k = 0; k < DIM; ++k) {
-                e = fmaf(Tl[r * NH + k], s.hi[k], e);
-                e = fmaf(Th[r * NH + k], s.lo[k], e);
-            }
-            d[r] = y[r] + e;
-        }
+        for (int r = 0; r < DIM; ++r) d[r] = y[r] + e[r];
     } else {
         float pm[DIM];
         const float hh = 0.5f * h;
 #pragma unroll
-        for (int i = 0; i < DIM; ++i) pm[i] = fmaf(hh, y[i], s.hi[i]);
-        fast_affine<DIM>(y, A, pm);
+        for (int i = 0; i < DIM; ++i) pm[i] = fmaf(hh, y[i], s.x[i]);
+        cm_affine<DIM>(y, m, pm);
 #pragma unroll
         for (int i = 0; i < DIM; ++i) d[i] = h * y[i];
     }
+    q = s;
 #pragma unroll
-    for (int r = 0; r < DIM; ++r) {
-        q.hi[r] = s.hi[r];
-        q.lo[r] = s.lo[r];
-        acc_add(q.hi[r], q.lo[r], d[r]);
-    }
+    for (int r = 0; r < DIM; ++r) q.add(r, d[r]);
 }
 
 // ------------------------------------------------------------ integration
@@ -193,6 +228,8 @@ __device__ __forceinline__ void advance(bool fast, const PState<DIM, float> &s, 
 //   Snk::put(idx, st)      receives the end state (PState; get() converts)
 //   perm (optional, shared memory): the k-th point of the range is
 //   ws_base + perm[k - ws_base] (a cell-sorted order inside the tile).
+//   start_cells (optional, with perm): cell of point perm_base + i at [i],
+//   as computed by the caller's sort pass (same lookup, same point).
 //   claim (optional, shared memory, zero on entry): all warps of the CTA
 //   share one queue over [ws, we) -- a warp whose lanes finish claims the next
 //   points of the whole tile, so no warp idles at the end-of-tile barrier
@@ -208,11 +245,11 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
                                                 unsigned long long &c_fast, unsigned long long &c_fb,
                                                 unsigned long long &c_sub, unsigned long long &c_pts,
                                                 const int *perm = nullptr, int64_t perm_base = 0,
-                                                unsigned long long *claim = nullptr)
+                                                unsigned long long *claim = nullptr,
+                                                const int *start_cells = nullptr)
 {
     constexpr int NE = DIM * (DIM + 1);
     constexpr bool kTwoPart = TableLayout<Real>::kTParts == 2;
-    const int tab = t.nC * NE;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     int64_t next = ws + 32;
@@ -230,7 +267,7 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
     int steps_left = 0, sub_left = 0, c = 0;
     if (active) {
         src.load(idx, st);
-        c = cell_of<DIM, TESS>(t, st);
+        c = start_cells ? start_cells[idx - perm_base] : cell_of<DIM, TESS>(t, st);
         steps_left = nT;
         sub_left = (SCHEME == SCHEME_SIMPLE) ? nT * nODE : 0;
     }
@@ -239,7 +276,8 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
         if (active) {
             const bool fast = (SCHEME == SCHEME_REF) && sub_left == 0;
             PState<DIM, Real> q;
-            advance<DIM>(fast, st, sA + c * NE, sT + c * NE, kTwoPart ? sT + tab + c * NE : nullptr, h, q);
+            // float tables interleave (T-I)_hi and (T-I)_lo per cell
+            advance<DIM>(fast, st, sA + c * NE, sT + (kTwoPart ? 2 : 1) * c * NE, nullptr, h, q);
             const int cq = cell_of<DIM, TESS>(t, q);
             if (fast && cq != c) {
                 // the end point left the cell: redo the step with nStepsODE sub-steps from p
@@ -279,7 +317,7 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
                 if (active) {
                     idx = perm ? perm_base + perm[k - perm_base] : k;
                     src.load(idx, st);
-                    c = cell_of<DIM, TESS>(t, st);
+                    c = start_cells ? start_cells[idx - perm_base] : cell_of<DIM, TESS>(t, st);
                     steps_left = nT;
                     sub_left = (SCHEME == SCHEME_SIMPLE) ? nT * nODE : 0;
                 }

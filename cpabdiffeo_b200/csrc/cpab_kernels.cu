@@ -146,7 +146,8 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
         }
         // every warp works on the whole tile through the shared claim counter
         integrate_range<DIM, TESS, Real, SCHEME>(a.t, a.nTimeSteps, a.nStepsODE, sA, sT, ti.start, ti.end, h, src,
-                                                 snk, c_fast, c_fb, c_sub, c_pts, perm, ti.start, &s_claim);
+                                                 snk, c_fast, c_fb, c_sub, c_pts, perm, ti.start, &s_claim,
+                                                 perm ? s_cell : nullptr);
         __syncthreads();
     }
     if (a.counters) {
@@ -447,7 +448,7 @@ static cudaError_t launch_integrate_t(const IntegrateArgs &a, const LaunchCfg &c
     size_t smem = (size_t)(1 + TableLayout<Real>::kTParts) * a.t.nC * NE * sizeof(Real);
     if (a.sort) smem += ((size_t)a.t.nC + 2 * (size_t)a.batch.tile_pts) * sizeof(int);
     auto kern = k_integrate<DIM, TESS, Real, SCHEME>;
-    if (smem > 48 * 1024) {
+    if (smem > kSmemOptInAbove) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
@@ -490,7 +491,7 @@ static cudaError_t launch_traj_t(const IntegrateArgs &a, int64_t nPts, cudaStrea
     constexpr int NE = DIM * (DIM + 1);
     size_t smem = (size_t)2 * a.t.nC * NE * sizeof(double);
     auto kern = k_trajectory<DIM, TESS>;
-    if (smem > 48 * 1024) {
+    if (smem > kSmemOptInAbove) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
@@ -527,7 +528,7 @@ static cudaError_t launch_v_t(const Tess &t, const double *A, const double *pts,
     constexpr int NE = DIM * (DIM + 1);
     size_t smem = (size_t)t.nC * NE * sizeof(double);
     auto kern = k_calc_v<DIM, TESS>;
-    if (smem > 48 * 1024) {
+    if (smem > kSmemOptInAbove) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }

@@ -17,6 +17,10 @@ struct LaunchCfg {
     int sort = 0;          // cell-sort the points of each tile
 };
 
+// Kernels opt in to more than the default 48 KB of shared memory when their
+// dynamic size exceeds this (their static shared memory comes on top).
+constexpr size_t kSmemOptInAbove = 40 * 1024;
+
 int num_sms();
 int persistent_grid_impl(const void *kern, const LaunchCfg &cfg, size_t smem);
 template <typename K>

@@ -1,0 +1,48 @@
+// cpab_reduce.cuh -- deterministic per-instance sums over tiles: each CTA
+// reduces its tile in a fixed lane / warp order, stores the tile's partial,
+// and the last tile of an instance to finish (atomic ticket with fences) adds
+// that instance's partials in index order.  A result is therefore the same
+// alone and inside any batch, whatever the launch shape.
+#pragma once
+
+#include "cpab_device.cuh"
+
+namespace cpab {
+
+__device__ __forceinline__ double warp_sum_f64(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
+    return v;
+}
+
+// Reduce `acc` over the CTA (fixed order) and hand the tile's partial to the
+// per-image bookkeeping.  All threads of the CTA must call this.
+__device__ __forceinline__ void finish_tile(double acc, int64_t tile, int inst, int tiles_of_inst, int64_t first_tile_of_inst,
+                            double *partials, unsigned *tickets, double *ll_out)
+{
+    __shared__ double s_w[32];
+    __shared__ bool s_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    acc = warp_sum_f64(acc);
+    if (lane == 0) s_w[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += s_w[w];
+        partials[tile] = s;
+        __threadfence();
+        unsigned ticket = atomicAdd(tickets + inst, 1u);
+        s_last = (ticket == (unsigned)tiles_of_inst - 1u);
+        if (s_last) {
+            __threadfence();
+            double tot = 0.0;
+            for (int k = 0; k < tiles_of_inst; ++k) tot += ((volatile double *)partials)[first_tile_of_inst + k];
+            ll_out[inst] = tot;
+            tickets[inst] = 0u;  // ready for the next call
+        }
+    }
+    __syncthreads();
+}
+
+}  // namespace cpab

@@ -18,127 +18,110 @@
 // (lanes, then warps), writes its partial, and the last tile of an image to
 // finish (atomic ticket with fences) adds that image's partials in index
 // order.  A result is therefore the same alone and inside any batch.
+#include <math_constants.h>
+
+#include "cpab_bulk.cuh"
 #include "cpab_integrate.cuh"
 #include "cpab_launch.h"
+#include "cpab_reduce.cuh"
 #include "cpab_register.h"
 
 namespace cpab {
 
-// Bilinear sample of a float image at pixel coordinates (px, py), zero outside.
-__device__ __forceinline__ double tap(const float *img, int H, int W, int r, int c)
-{
-    return (r >= 0 && r < H && c >= 0 && c < W) ? (double)__ldg(img + (int64_t)r * W + c) : 0.0;
-}
-
-__device__ __forceinline__ double bilinear(const float *img, int H, int W, double px, double py)
-{
-    double fx0 = floor(px), fy0 = floor(py);
-    if (!(fx0 > -2.0 && fx0 < (double)W + 1.0 && fy0 > -2.0 && fy0 < (double)H + 1.0)) return 0.0;
-    double fx = px - fx0, fy = py - fy0;
-    int c0 = (int)fx0, r0 = (int)fy0;
-    double top = (1 - fx) * tap(img, H, W, r0, c0) + fx * tap(img, H, W, r0, c0 + 1);
-    double bot = (1 - fx) * tap(img, H, W, r0 + 1, c0) + fx * tap(img, H, W, r0 + 1, c0 + 1);
-    return (1 - fy) * top + fy * bot;
-}
-
-__device__ __forceinline__ double warp_sum_f64(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
-    return v;
-}
-
-// Reduce `acc` over the CTA (fixed order) and hand the tile's partial to the
-// per-image bookkeeping.  All threads of the CTA must call this.
-__device__ void finish_tile(double acc, int64_t tile, int inst, int tiles_of_inst, int64_t first_tile_of_inst,
-                            double *partials, unsigned *tickets, double *ll_out)
-{
-    __shared__ double s_w[32];
-    __shared__ bool s_last;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    acc = warp_sum_f64(acc);
-    if (lane == 0) s_w[warp] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int w = 0; w < nw; ++w) s += s_w[w];
-        partials[tile] = s;
-        __threadfence();
-        unsigned ticket = atomicAdd(tickets + inst, 1u);
-        s_last = (ticket == (unsigned)tiles_of_inst - 1u);
-        if (s_last) {
-            __threadfence();
-            double tot = 0.0;
-            for (int k = 0; k < tiles_of_inst; ++k) tot += ((volatile double *)partials)[first_tile_of_inst + k];
-            ll_out[inst] = tot;
-            tickets[inst] = 0u;  // ready for the next call
-        }
-    }
-    __syncthreads();
-}
-
-// ------------------------------------------------------------ standalone remap (+ SSD)
-
-__device__ __forceinline__ void load_pair(const float *p, float &x, float &y)
-{
-    const float2 v = __ldg(reinterpret_cast<const float2 *>(p));
-    x = v.x;
-    y = v.y;
-}
-
-__device__ __forceinline__ void load_pair(const double *p, double &x, double &y)
-{
-    const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
-    x = v.x;
-    y = v.y;
-}
-
-// Bilinear sampling split in two halves so that a thread can issue the tap
-// loads of several pixels before it needs any of them: same arithmetic as
-// bilinear().
-struct TapSet {
+// Bilinear sample of a float image at pixel coordinates (px, py), zero
+// outside (cv2 conventions).  floor and fraction are taken in double -- floor
+// by adding 1.5 * 2^52 with rounding toward -inf, which leaves floor(px) as an
+// integer in the low word, so no conversion instruction is needed.  The taps
+// are combined in double for double maps / the FP64 likelihood, and in float
+// (weights rounded to float, error <= 3 ulp of the value) for float maps /
+// the FP32 likelihood.
+struct Taps {
     float v[4];      // (r0, c0), (r0, c0 + 1), (r0 + 1, c0), (r0 + 1, c0 + 1)
     double fx, fy;
-    bool inside;
+    bool in;
 };
 
-__device__ __forceinline__ void taps_issue(const float *img, int H, int W, double px, double py, TapSet &t)
+__device__ __forceinline__ void taps_issue(const float *img, int H, int W, double px, double py, Taps &t)
 {
-    const double fx0 = floor(px), fy0 = floor(py);
-    t.inside = fx0 > -2.0 && fx0 < (double)W + 1.0 && fy0 > -2.0 && fy0 < (double)H + 1.0;
+    constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52
+    const double sx = __dadd_rd(px, kRound), sy = __dadd_rd(py, kRound);
+    const double fx0 = sx - kRound, fy0 = sy - kRound;  // floor(px), floor(py) for |p| < 2^51
+    t.in = fx0 > -2.0 && fx0 < (double)W + 1.0 && fy0 > -2.0 && fy0 < (double)H + 1.0;  // false for NaN
     t.fx = px - fx0;
     t.fy = py - fy0;
-    const int c0 = t.inside ? (int)fx0 : -2, r0 = t.inside ? (int)fy0 : -2;
+    const int c0 = t.in ? __double2loint(sx) : -2, r0 = t.in ? __double2loint(sy) : -2;
+    if (c0 >= 0 && c0 + 1 < W && r0 >= 0 && r0 + 1 < H) {
+        // the whole 2x2 footprint is inside (the common case): four unconditional loads
+        const float *q = img + (r0 * W + c0);
+        t.v[0] = __ldg(q);
+        t.v[1] = __ldg(q + 1);
+        t.v[2] = __ldg(q + W);
+        t.v[3] = __ldg(q + W + 1);
+    } else {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int r = r0 + (k >> 1), c = c0 + (k & 1);
-        t.v[k] = (r >= 0 && r < H && c >= 0 && c < W) ? __ldg(img + (int64_t)r * W + c) : 0.0f;
+        for (int k = 0; k < 4; ++k) {
+            const int r = r0 + (k >> 1), c = c0 + (k & 1);
+            t.v[k] = (r >= 0 && r < H && c >= 0 && c < W) ? __ldg(img + (r * W + c)) : 0.0f;
+        }
     }
 }
 
-__device__ __forceinline__ double taps_combine(const TapSet &t)
+template <typename Real>
+__device__ __forceinline__ Real taps_combine(const Taps &t);
+
+template <>
+__device__ __forceinline__ double taps_combine<double>(const Taps &t)
 {
-    if (!t.inside) return 0.0;
+    if (!t.in) return 0.0;
     const double top = (1 - t.fx) * (double)t.v[0] + t.fx * (double)t.v[1];
     const double bot = (1 - t.fx) * (double)t.v[2] + t.fx * (double)t.v[3];
     return (1 - t.fy) * top + t.fy * bot;
 }
 
-// Each thread handles kRemapBatch pixels per round (stride blockDim.x, so a
-// warp's accesses stay coalesced): all map and dst loads of the round are
-// issued first, then all tap loads, then the arithmetic -- enough loads in
-// flight per SM to stream HBM.  Per-thread sums keep pixel order.
-constexpr int kRemapBatch = 4;
+template <>
+__device__ __forceinline__ float taps_combine<float>(const Taps &t)
+{
+    if (!t.in) return 0.0f;
+    const float wx = (float)t.fx, wy = (float)t.fy;
+    const float top = fmaf(wx, t.v[1] - t.v[0], t.v[0]);
+    const float bot = fmaf(wx, t.v[3] - t.v[2], t.v[2]);
+    return fmaf(wy, bot - top, top);
+}
 
+template <typename Real>
+__device__ __forceinline__ Real bilinear(const float *img, int H, int W, double px, double py)
+{
+    Taps t;
+    taps_issue(img, H, W, px, py, t);
+    return taps_combine<Real>(t);
+}
+
+// ------------------------------------------------------------ standalone remap (+ SSD)
+
+// (x, y) of one map entry in shared memory with one 8- or 16-byte load.
+__device__ __forceinline__ void load_pair(const float *p, float &x, float &y)
+{
+    const float2 v = *reinterpret_cast<const float2 *>(p);
+    x = v.x;
+    y = v.y;
+}
+__device__ __forceinline__ void load_pair(const double *p, double &x, double &y)
+{
+    const double2 v = *reinterpret_cast<const double2 *>(p);
+    x = v.x;
+    y = v.y;
+}
+
+// Plain path (any alignment, any image size): one pixel per thread and
+// iteration, pixels in increasing order per thread.
 template <typename MapT>
-__global__ void __launch_bounds__(256, 3) k_remap_ssd(RemapArgs a)
+__global__ void __launch_bounds__(256) k_remap_ssd(RemapArgs a)
 {
     const int inst = blockIdx.y;
     const int64_t npx = (int64_t)a.H * a.W;
     const int64_t tile = blockIdx.x;
     const int64_t start = tile * a.tile_px;
-    const int n = (int)(min(start + (int64_t)a.tile_px, npx) - start);   // pixels of this tile
-    // tile-relative pointers: the per-pixel indices below are 32-bit
+    const int n = (int)(min(start + (int64_t)a.tile_px, npx) - start);
     const int64_t off = (int64_t)inst * npx + start;
     const MapT *map = static_cast<const MapT *>(a.map) + 2 * off;
     const float *src = a.src + (int64_t)inst * npx;
@@ -146,43 +129,13 @@ __global__ void __launch_bounds__(256, 3) k_remap_ssd(RemapArgs a)
     float *warped = a.warped ? a.warped + off : nullptr;
     const double k = -0.5 / (a.sigma * a.sigma);
     double acc = 0.0;
-    // one vector load per (x, y) pair when the map is aligned for it (uniform over the launch)
-    const bool vec = (reinterpret_cast<uintptr_t>(a.map) & (2 * sizeof(MapT) - 1)) == 0;
-    for (int j0 = threadIdx.x; j0 < n; j0 += kRemapBatch * blockDim.x) {
-        MapT mx[kRemapBatch], my[kRemapBatch];
-        float dv[kRemapBatch];
-#pragma unroll
-        for (int u = 0; u < kRemapBatch; ++u) {
-            const int j = j0 + u * blockDim.x;
-            mx[u] = my[u] = 0;
-            dv[u] = 0.0f;
-            if (j < n) {
-                if (vec) {
-                    load_pair(map + 2 * j, mx[u], my[u]);
-                } else {
-                    mx[u] = map[2 * j];
-                    my[u] = map[2 * j + 1];
-                }
-                if (dst) dv[u] = __ldg(dst + j);
-            }
-        }
-        TapSet ts[kRemapBatch];
-#pragma unroll
-        for (int u = 0; u < kRemapBatch; ++u) {
-            if (j0 + u * (int)blockDim.x < n)
-                taps_issue(src, a.H, a.W, (double)mx[u] * a.sx + a.ox, (double)my[u] * a.sy + a.oy, ts[u]);
-        }
-#pragma unroll
-        for (int u = 0; u < kRemapBatch; ++u) {
-            const int j = j0 + u * blockDim.x;
-            if (j < n) {
-                const double w = taps_combine(ts[u]);
-                if (warped) warped[j] = (float)w;
-                if (dst) {
-                    const double e = w - (double)dv[u];
-                    acc += e * e * k;
-                }
-            }
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const MapT w = bilinear<MapT>(src, a.H, a.W, (double)map[2 * j] * a.sx + a.ox,
+                                      (double)map[2 * j + 1] * a.sy + a.oy);
+        if (warped) warped[j] = (float)w;
+        if (dst) {
+            const double e = (double)w - (double)__ldg(dst + j);
+            acc += e * e * k;
         }
     }
     if (dst) {
@@ -191,9 +144,108 @@ __global__ void __launch_bounds__(256, 3) k_remap_ssd(RemapArgs a)
     }
 }
 
+// Bulk path (16-byte aligned map and dst, H*W a multiple of 4): a persistent
+// grid walks the (image, tile) list; while a CTA samples one tile, the map
+// and dst of its next tile stream into the other shared-memory stage by
+// cp.async.bulk, so the only loads the threads wait on are the source taps.
+// Same per-pixel arithmetic and per-thread order as the plain path, hence
+// the same results.  A stage whose copy does not complete within the wait
+// bound makes that image's ll NaN and leaves its warped tile unwritten.
+template <typename MapT>
+__global__ void __launch_bounds__(256) k_remap_ssd_bulk(RemapArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t s_bar[2];
+    const int TP = a.tile_px;
+    // stage s: map at s_map0 + s * 2 TP, dst at s_dst0 + s * TP
+    MapT *const s_map0 = reinterpret_cast<MapT *>(smem_raw);
+    float *const s_dst0 = reinterpret_cast<float *>(s_map0 + 4 * TP);
+    const int64_t npx = (int64_t)a.H * a.W;
+    const int tpi = (int)((npx + TP - 1) / TP);
+    const int64_t ntiles = (int64_t)tpi * a.N;
+    const double k = -0.5 / (a.sigma * a.sigma);
+    const MapT *gmap = static_cast<const MapT *>(a.map);
+    if (threadIdx.x == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    auto issue = [&](int64_t tile, int stage) {
+        const int inst = (int)(tile / tpi);
+        const int64_t start = (tile - (int64_t)inst * tpi) * TP;
+        const int n = (int)min((int64_t)TP, npx - start);
+        const int64_t off = (int64_t)inst * npx + start;
+        const uint32_t mb = (uint32_t)n * 2u * (uint32_t)sizeof(MapT), db = a.dst ? (uint32_t)n * 4u : 0u;
+        mbar_arrive_expect_tx(&s_bar[stage], mb + db);
+        bulk_g2s(s_map0 + stage * 2 * TP, gmap + 2 * off, mb, &s_bar[stage]);
+        if (db) bulk_g2s(s_dst0 + stage * TP, a.dst + off, db, &s_bar[stage]);
+    };
+    if (threadIdx.x == 0 && (int64_t)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    int it = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const int stage = it & 1;
+        const uint32_t parity = (uint32_t)(it >> 1) & 1u;
+        // the other stage was released by the previous iteration's closing barrier
+        if (threadIdx.x == 0 && tile + gridDim.x < ntiles) issue(tile + gridDim.x, stage ^ 1);
+        const bool ok = mbar_wait(&s_bar[stage], parity);
+        const int inst = (int)(tile / tpi);
+        const int64_t start = (tile - (int64_t)inst * tpi) * TP;
+        const int n = (int)min((int64_t)TP, npx - start);
+        const int64_t off = (int64_t)inst * npx + start;
+        const float *src = a.src + (int64_t)inst * npx;
+        float *warped = a.warped ? a.warped + off : nullptr;
+        double acc = 0.0;
+        if (ok) {
+            const MapT *m = s_map0 + stage * 2 * TP;
+            const float *dv = s_dst0 + stage * TP;
+            for (int j = threadIdx.x; j < n; j += blockDim.x) {
+                MapT mx, my;
+                load_pair(m + 2 * j, mx, my);
+                const MapT w = bilinear<MapT>(src, a.H, a.W, (double)mx * a.sx + a.ox, (double)my * a.sy + a.oy);
+                if (warped) warped[j] = (float)w;
+                if (a.dst) {
+                    const double e = (double)w - (double)dv[j];
+                    acc += e * e * k;
+                }
+            }
+        } else {
+            acc = CUDART_NAN;
+        }
+        if (a.dst) finish_tile(acc, tile, inst, tpi, (int64_t)inst * tpi, a.partials, a.tickets, a.ll);
+        else __syncthreads();
+    }
+    // every copy this CTA issued was waited for above (the last issue targets the last tile)
+}
+
+template <typename MapT>
+static cudaError_t launch_remap_bulk(const RemapArgs &a, cudaStream_t s)
+{
+    auto kern = k_remap_ssd_bulk<MapT>;
+    const size_t smem = 2 * (size_t)a.tile_px * (2 * sizeof(MapT) + sizeof(float));
+    if (smem > kSmemOptInAbove) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    LaunchCfg cfg;
+    cfg.block = 256;
+    const int64_t npx = (int64_t)a.H * a.W;
+    const int64_t ntiles = ((npx + a.tile_px - 1) / a.tile_px) * a.N;
+    int64_t grid = persistent_grid(kern, cfg, smem);
+    if (grid > ntiles) grid = ntiles;
+    kern<<<(unsigned)grid, 256, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_remap_ssd(const RemapArgs &a, int map_prec, cudaStream_t s)
 {
     const int64_t npx = (int64_t)a.H * a.W;
+    // bulk copies need 16-byte aligned sources and sizes: aligned bases and 4 | H*W
+    // (tiles then start at multiples of 4 pixels and hold a multiple of 4)
+    const bool bulk = (npx % 4 == 0) && (a.tile_px % 4 == 0) &&
+                      (reinterpret_cast<uintptr_t>(a.map) % 16 == 0) &&
+                      (!a.dst || reinterpret_cast<uintptr_t>(a.dst) % 16 == 0);
+    if (bulk) return map_prec == PREC_F64 ? launch_remap_bulk<double>(a, s) : launch_remap_bulk<float>(a, s);
     dim3 grid((unsigned)((npx + a.tile_px - 1) / a.tile_px), (unsigned)a.N);
     if (map_prec == PREC_F64) k_remap_ssd<double><<<grid, 256, 0, s>>>(a);
     else k_remap_ssd<float><<<grid, 256, 0, s>>>(a);
@@ -236,9 +288,9 @@ struct SsdSnk {
         const int64_t j = i - base;
         double p[2];
         st.get(p);
-        double w = bilinear(src, H, W, p[0] * W - 0.5, p[1] * H - 0.5);
+        const Real w = bilinear<Real>(src, H, W, p[0] * W - 0.5, p[1] * H - 0.5);
         if (warped) warped[j] = (float)w;
-        double e = w - (double)__ldg(dst + j);
+        const double e = (double)w - (double)__ldg(dst + j);
         term[i - tile_start] = e * e * k;
     }
 };
@@ -307,7 +359,7 @@ static cudaError_t launch_register_t(const RegisterArgs &a, const LaunchCfg &cfg
     size_t smem = (size_t)(1 + TableLayout<Real>::kTParts) * a.t.nC * 6 * sizeof(Real) +
                   (size_t)a.tile_px * sizeof(double);
     auto kern = k_register_ll<TESS, Real>;
-    if (smem > 48 * 1024) {
+    if (smem > kSmemOptInAbove) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }

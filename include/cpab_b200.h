@@ -233,6 +233,27 @@ int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
                      int nStepsODE, double *ll, float *warped, void *workspace, size_t workspace_bytes,
                      uint64_t *counters, void *stream);
 
+/* Scratch bytes of cpab_landmark_ll for N instances of n_lm landmarks. */
+size_t cpab_landmark_workspace_bytes(const cpab_ctx *ctx, int N, int n_lm);
+
+/* The Gaussian landmark log-likelihood of N instances in one launch
+ * (ScaleDependentLogLikelihoodGaussian.calc_ll of
+ * cpab/cpa2d/model/transformations/landmarks/_ScaleDependentLogLikelihoodGaussian.py:29-73
+ * with calc_err_per_sample / calc_ll_per_sample of its gpu/gaussian.py:12-22;
+ * 1D: cpab/cpa1d/model/transformations/landmarks/, same formula):
+ *   ll[n] = sum_i -0.5 |T_n(src_i) - dst_i|^2 / sigma^2,
+ * T_n = calc_T_fwd with instance n's tables (REF scheme), any dimension and
+ * tessellation.  src / dst are float64 [*, n_lm, dim]; instance n reads its
+ * landmarks at src + n * src_stride * dim (src_stride 0: one set shared by
+ * all instances; likewise dst).  The sum is taken in a fixed order (the
+ * reference's __call__ then divides by n_lm in 2D).  transformed
+ * [N, n_lm, dim] float64 receives T_n(src_i) unless NULL.  precision sets the
+ * integration arithmetic (CPAB_F64: the transformed points are bit-exact). */
+int cpab_landmark_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, int N, const double *src,
+                     int64_t src_stride, const double *dst, int64_t dst_stride, int n_lm, double sigma,
+                     int precision, double dt, int nTimeSteps, int nStepsODE, double *ll, double *transformed,
+                     void *workspace, size_t workspace_bytes, uint64_t *counters, void *stream);
+
 /* ------------------------------------------------------------------ inference */
 
 /* Random-walk proposals for C chains (Proposal.__call__,

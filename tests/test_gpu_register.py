@@ -58,6 +58,35 @@ def test_remap_unaligned_map_same_result(dt):
     assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_remap_ssd_bulk_and_plain_paths_agree(oracle_mod, dt):
+    """Aligned maps of 4 | H*W pixels take the bulk-copy kernel; a map 8 bytes
+    off a 16-byte boundary and an odd-sized image take the plain kernel.  Both
+    give the same bits, and the oracle's values."""
+    O = oracle_mod
+    rng = np.random.default_rng(11)
+    for H, W in ((72, 96), (63, 65)):
+        N = 3
+        src = np.stack([smooth_image(rng, H, W, 2.0) for _ in range(N)])
+        dst = np.stack([smooth_image(rng, H, W, 2.0) for _ in range(N)])
+        pts = pixel_centers(H, W)[None] + rng.normal(0, 0.03, size=(N, H * W, 2))
+        m = torch.as_tensor(pts, dtype=dt, device=DEV).contiguous()
+        buf = torch.empty(N * H * W * 2 + 16, dtype=dt, device=DEV)
+        shift = 8 // m.element_size()                       # 8 bytes
+        mu = buf[shift:shift + m.numel()].view(N, H * W, 2)
+        mu.copy_(m)
+        s_t, d_t = torch.as_tensor(src, device=DEV), torch.as_tensor(dst, device=DEV)
+        wa, wb = torch.empty_like(s_t), torch.empty_like(s_t)
+        la = remap_ssd(m, s_t, d_t, 0.1, pixel_map=UNIT(H, W), warped=wa)
+        lb = remap_ssd(mu, s_t, d_t, 0.1, pixel_map=UNIT(H, W), warped=wb)
+        assert torch.equal(la, lb) and torch.equal(wa, wb)
+        for n in range(N):
+            mp = pts[n] if dt == torch.float64 else pts[n].astype(np.float32).astype(np.float64)
+            ll, warped = O.remap_ssd(mp, src[n], dst[n], 0.1, *UNIT(H, W))
+            assert abs(la[n].item() - ll) <= 1e-6 * abs(ll)
+            assert np.abs(wa[n].cpu().numpy() - warped).max() < 1e-5
+
+
 def test_remap_identity_pixel_units():
     rng = np.random.default_rng(1)
     H, W = 33, 47
