@@ -217,6 +217,9 @@ int cpab_landmark_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
     a.dt = dt;
     a.nTimeSteps = nTimeSteps;
     a.nStepsODE = nStepsODE;
+    a.clamp = ctx->clamp;
+    a.clamp_lo = ctx->clamp_lo;
+    a.clamp_hi = ctx->clamp_hi;
     a.cancel = ctx->cancel_dev;
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(a.tickets, 0, (size_t)N * sizeof(unsigned), s);

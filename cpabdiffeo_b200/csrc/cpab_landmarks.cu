@@ -44,12 +44,19 @@ struct LandmarkSnk {
     int64_t base, tile_start;
     double k;             // -0.5 / sigma^2
     double *term;
+    int clamp;
+    double lo, hi;
     template <typename Real>
     __device__ __forceinline__ void put(int64_t i, const PState<DIM, Real> &st)
     {
         const int64_t j = i - base;
         double x[DIM];
         st.get(x);
+        if (clamp) {
+            // calc_T's end-point clamp (threshold_krnl)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) x[d] = clamp_ref(x[d], lo, hi);
+        }
         double e2 = 0.0;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
@@ -92,7 +99,8 @@ __global__ void __launch_bounds__(256) k_landmark_ll(LandmarkArgs a)
         }
         LandmarkSrc<DIM> src{a.src + (int64_t)inst * a.src_stride * DIM, base};
         LandmarkSnk<DIM> snk{a.dst + (int64_t)inst * a.dst_stride * DIM,
-                             a.transformed ? a.transformed + base * DIM : nullptr, base, start, k, s_term};
+                             a.transformed ? a.transformed + base * DIM : nullptr,
+                             base, start, k, s_term, a.clamp, a.clamp_lo, a.clamp_hi};
         if (threadIdx.x == 0) s_claim = 0ull;
         __syncthreads();
         integrate_range<DIM, TESS, Real, SCHEME_REF>(a.t, a.nTimeSteps, a.nStepsODE, sA, sT, start, end, h, src,

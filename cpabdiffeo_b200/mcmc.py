@@ -19,17 +19,20 @@ import torch
 
 from . import _lib
 from .cpa_space import CpaSpace
+from .landmarks import LandmarkLogLikelihood
 from .registration import GaussianLogLikelihood
 
 
 class BatchedMetropolis:
-    def __init__(self, ll: GaussianLogLikelihood, theta0: torch.Tensor, prop_std: np.ndarray, scale: float = 0.05,
+    def __init__(self, ll: GaussianLogLikelihood | LandmarkLogLikelihood, theta0: torch.Tensor, prop_std: np.ndarray, scale: float = 0.05,
                  seed: int = 0, rule: str = "reference", use_ave_ll: bool = True,
                  prior_precision: np.ndarray | None = None, wlp: float = 1.0):
         self.ll_fn = ll
         sp: CpaSpace = ll.space
         self.space = sp
         dev = sp.device
+        # image likelihoods integrate with calc_T_inv tables, landmark ones with calc_T_fwd
+        self.sign = int(getattr(ll, "sign", -1))
         self.C = ll.N
         self.d = sp.d
         self.theta = torch.as_tensor(theta0, dtype=torch.float64, device=dev).reshape(self.C, self.d).clone()
@@ -63,7 +66,7 @@ class BatchedMetropolis:
         c.check(c.lib.cpab_mcmc_propose(c.h, self.C, self.d, _lib.ptr(self.theta), _lib.ptr(self.prop_std), self.scale,
                                         self.seed, _lib.ptr(self.step), _lib.ptr(self.theta_prop), s))
         c.check(c.lib.cpab_theta_to_trels(c.h, _lib.ptr(sp.B), self.d, _lib.ptr(self.theta_prop), self.C,
-                                          self.ll_fn.dt, -1, None, _lib.ptr(self.sA), _lib.ptr(self.Tr), s))
+                                          self.ll_fn.dt, self.sign, None, _lib.ptr(self.sA), _lib.ptr(self.Tr), s))
         self.ll_fn.batch_tables((self.sA, self.Tr), ll=self.ll_prop)
         c.check(c.lib.cpab_mcmc_accept(c.h, self.C, self.d, _lib.ptr(self.theta), _lib.ptr(self.theta_prop),
                                        _lib.ptr(self.ll), _lib.ptr(self.ll_prop), self.inv_npts,

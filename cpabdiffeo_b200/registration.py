@@ -155,6 +155,7 @@ class GaussianLogLikelihood:
         self.dst = self.dst.contiguous()
         self.N, self.H, self.W = self.src.shape
         self.nPts = self.H * self.W
+        self.sign = -1        # the image is pulled back: calc_T_inv of the pixel grid
         self.sigma = float(sigma_signal)
         p = default_params_flow_int(2)
         if params_flow_int:
