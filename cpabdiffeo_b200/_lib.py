@@ -60,6 +60,12 @@ SIGNATURES = {
     "cpab_register_workspace_bytes": (_sz, [_vp, _i, _i, _i]),
     "cpab_register_ll": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _i, _i, _d, _i, _d, _i, _i, _vp, _vp, _vp, _sz, _vp,
                               _vp]),
+    "cpab_remap3d_workspace_bytes": (_sz, [_i, _i, _i, _i]),
+    "cpab_remap3d_ssd": (_i, [_vp, _vp, _i, _vp, _vp, _i, _i, _i, _i, _d, _d, _d, _d, _d, _d, _d, _vp, _vp, _vp,
+                              _sz, _vp]),
+    "cpab_register3d_workspace_bytes": (_sz, [_vp, _i, _i, _i, _i]),
+    "cpab_register3d_ll": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _i, _i, _i, _d, _i, _d, _i, _i, _vp, _vp, _vp, _sz,
+                                _vp, _vp]),
     "cpab_landmark_workspace_bytes": (_sz, [_vp, _i, _i]),
     "cpab_landmark_ll": (_i, [_vp, _vp, _vp, _i, _vp, _i64, _vp, _i64, _i, _d, _i, _d, _i, _i, _vp, _vp, _vp, _sz,
                               _vp, _vp]),

@@ -5,6 +5,7 @@
 #include "cpab_ctx.h"
 #include "cpab_landmarks.h"
 #include "cpab_register.h"
+#include "cpab_register3d.h"
 
 using namespace cpab;
 
@@ -155,6 +156,139 @@ int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
     if (e != cudaSuccess) return cuda_status(ctx, e, "ticket reset");
     return cuda_status(ctx, launch_register_ll(a, precision == CPAB_F64 ? PREC_F64 : PREC_F32, ctx->cfg, s),
                        "register_ll launch");
+}
+
+static int check_volumes(cpab_ctx *ctx, int N, int H, int W, int D)
+{
+    if (N < 0) return fail(ctx, CPAB_BAD_SHAPE, "N < 0");
+    if (H < 1 || W < 1 || D < 1) return fail(ctx, CPAB_BAD_SHAPE, "volume size %d x %d x %d", H, W, D);
+    if ((int64_t)H * W * D > (int64_t)1 << 31) return fail(ctx, CPAB_BAD_SHAPE, "volume too large");
+    return CPAB_OK;
+}
+
+static int64_t tiles_of3(int H, int W, int D, int tile_px)
+{
+    return ((int64_t)H * W * D + tile_px - 1) / tile_px;
+}
+
+size_t cpab_remap3d_workspace_bytes(int N, int H, int W, int D)
+{
+    if (N < 0 || H < 1 || W < 1 || D < 1) return 0;
+    return ws_layout(N, tiles_of3(H, W, D, kRemapTilePx)).total;
+}
+
+int cpab_remap3d_ssd(cpab_ctx *ctx, const void *map, int map_precision, const float *src, const float *dst, int N,
+                     int H, int W, int D, double sx, double ox, double sy, double oy, double sz, double oz,
+                     double sigma, float *warped, double *ll, void *workspace, size_t workspace_bytes, void *stream)
+{
+    int st = check_volumes(ctx, N, H, W, D);
+    if (st != CPAB_OK) return st;
+    if (N == 0) return CPAB_OK;
+    if (map_precision != CPAB_F64 && map_precision != CPAB_F32)
+        return fail(ctx, CPAB_BAD_DTYPE, "map precision must be CPAB_F64 or CPAB_F32");
+    if (!map || !src) return fail(ctx, CPAB_BAD_ARG, "map/src is NULL");
+    if (!dst && !warped) return fail(ctx, CPAB_BAD_ARG, "nothing to compute: dst and warped are both NULL");
+    if (dst && !ll) return fail(ctx, CPAB_BAD_ARG, "ll is NULL (needed with dst)");
+    if (dst && !(sigma > 0)) return fail(ctx, CPAB_BAD_ARG, "sigma must be positive");
+    if (!std::isfinite(sx) || !std::isfinite(ox) || !std::isfinite(sy) || !std::isfinite(oy) || !std::isfinite(sz) ||
+        !std::isfinite(oz))
+        return fail(ctx, CPAB_BAD_ARG, "voxel mapping is not finite");
+    CPAB_CHECK_ALIGN(ctx, {map, map_precision == CPAB_F64 ? 8u : 4u, "map"}, {src, 4, "src"}, {dst, 4, "dst"},
+                     {warped, 4, "warped"}, {ll, 8, "ll"}, {workspace, 8, "workspace"});
+    const WsLayout L = ws_layout(N, tiles_of3(H, W, D, kRemapTilePx));
+    if (dst && (!workspace || workspace_bytes < L.total))
+        return fail(ctx, CPAB_NO_MEMORY, "workspace of %zu bytes needed", L.total);
+    Remap3dArgs a;
+    memset(&a, 0, sizeof(a));
+    a.map = map;
+    a.src = src;
+    a.dst = dst;
+    a.warped = warped;
+    a.ll = ll;
+    a.N = N;
+    a.H = H;
+    a.W = W;
+    a.D = D;
+    a.tile_px = kRemapTilePx;
+    a.sx = sx;
+    a.ox = ox;
+    a.sy = sy;
+    a.oy = oy;
+    a.sz = sz;
+    a.oz = oz;
+    a.sigma = sigma;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (dst) {
+        char *w = static_cast<char *>(workspace);
+        a.partials = reinterpret_cast<double *>(w + L.partials_off);
+        a.tickets = reinterpret_cast<unsigned *>(w + L.tickets_off);
+        cudaError_t e = cudaMemsetAsync(a.tickets, 0, (size_t)N * sizeof(unsigned), s);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "ticket reset");
+    }
+    return cuda_status(ctx, launch_remap3d_ssd(a, map_precision == CPAB_F64 ? PREC_F64 : PREC_F32, s),
+                       "remap3d launch");
+}
+
+size_t cpab_register3d_workspace_bytes(const cpab_ctx *ctx, int N, int H, int W, int D)
+{
+    if (!ctx || N < 0 || H < 1 || W < 1 || D < 1) return 0;
+    return ws_layout(N, tiles_of3(H, W, D, ctx->cfg.tile_pts)).total;
+}
+
+int cpab_register3d_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, int N, const float *src,
+                       const float *dst, int H, int W, int D, double sigma, int precision, double dt, int nTimeSteps,
+                       int nStepsODE, double *ll, float *warped, void *workspace, size_t workspace_bytes,
+                       uint64_t *counters, void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (ctx->t.dim != 3) return fail(ctx, CPAB_UNSUPPORTED, "the 3D registration likelihood needs a 3D space");
+    int st = check_volumes(ctx, N, H, W, D);
+    if (st != CPAB_OK) return st;
+    if (N == 0) return CPAB_OK;
+    if (precision != CPAB_F64 && precision != CPAB_F32)
+        return fail(ctx, CPAB_BAD_DTYPE, "precision must be CPAB_F64 or CPAB_F32");
+    if (!signedA || !Trels || !src || !dst || !ll) return fail(ctx, CPAB_BAD_ARG, "NULL argument");
+    if (!(sigma > 0)) return fail(ctx, CPAB_BAD_ARG, "sigma must be positive");
+    if (nTimeSteps < 1 || nStepsODE < 1) return fail(ctx, CPAB_BAD_ARG, "nTimeSteps and nStepsODE must be >= 1");
+    if ((long long)nTimeSteps * nStepsODE > 0x7fffffffLL)
+        return fail(ctx, CPAB_BAD_ARG, "nTimeSteps * nStepsODE overflows");
+    if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
+    CPAB_CHECK_ALIGN(ctx, {signedA, 8, "signedA"}, {Trels, 8, "Trels"}, {src, 4, "src"}, {dst, 4, "dst"},
+                     {ll, 8, "ll"}, {warped, 4, "warped"}, {workspace, 8, "workspace"}, {counters, 8, "counters"});
+    const int prec = precision == CPAB_F64 ? PREC_F64 : PREC_F32;
+    const int tile_px = ctx->cfg.tile_pts;
+    if (register3d_smem_bytes(ctx->t.nC, tile_px, prec) > (size_t)max_smem_optin())
+        return fail(ctx, CPAB_UNSUPPORTED, "cell tables and tile scratch exceed shared memory");
+    const WsLayout L = ws_layout(N, tiles_of3(H, W, D, tile_px));
+    if (!workspace || workspace_bytes < L.total)
+        return fail(ctx, CPAB_NO_MEMORY, "workspace of %zu bytes needed", L.total);
+    Register3dArgs a;
+    memset(&a, 0, sizeof(a));
+    a.t = ctx->t;
+    a.A = signedA;
+    a.T = Trels;
+    a.src = src;
+    a.dst = dst;
+    a.warped = warped;
+    a.ll = ll;
+    char *w = static_cast<char *>(workspace);
+    a.partials = reinterpret_cast<double *>(w + L.partials_off);
+    a.tickets = reinterpret_cast<unsigned *>(w + L.tickets_off);
+    a.counters = reinterpret_cast<unsigned long long *>(counters);
+    a.N = N;
+    a.H = H;
+    a.W = W;
+    a.D = D;
+    a.tile_px = tile_px;
+    a.sigma = sigma;
+    a.dt = dt;
+    a.nTimeSteps = nTimeSteps;
+    a.nStepsODE = nStepsODE;
+    a.cancel = ctx->cancel_dev;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(a.tickets, 0, (size_t)N * sizeof(unsigned), s);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "ticket reset");
+    return cuda_status(ctx, launch_register3d_ll(a, prec, ctx->cfg, s), "register3d_ll launch");
 }
 
 size_t cpab_landmark_workspace_bytes(const cpab_ctx *ctx, int N, int n_lm)

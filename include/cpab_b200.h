@@ -233,6 +233,40 @@ int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
                      int nStepsODE, double *ll, float *warped, void *workspace, size_t workspace_bytes,
                      uint64_t *counters, void *stream);
 
+/* Scratch bytes of cpab_remap3d_ssd for N volumes of H x W x D (needed with dst). */
+size_t cpab_remap3d_workspace_bytes(int N, int H, int W, int D);
+
+/* Trilinear remap of N float32 volumes [N, H, W, D] (remap3d of the external
+ * of.gpu.remap, called from remap_fwd / remap_inv at
+ * cpab/cpa3d/TransformWrapper.py:230-286).  Volumes are indexed
+ * [row][col][slice], the order of the reference's dense 3D grid
+ * (np.mgrid[0:Ny, 0:Nx, 0:Nz], cpab/cpa3d/calcs/_CpaCalcs.py:45-76); a map
+ * point (x, y, z) = (column, row, slice) is sampled at voxel coordinates
+ * (x*sx + ox, y*sy + oy, z*sz + oz), integer coordinates at voxel centres,
+ * taps outside the volume read 0.  map [N, H*W*D, 3] float64 or float32.
+ * With dst the same pass gives ll[n] = sum -0.5 (warped - dst)^2 / sigma^2 in
+ * a fixed order; warped may then be NULL. */
+int cpab_remap3d_ssd(cpab_ctx *ctx, const void *map, int map_precision, const float *src, const float *dst,
+                     int N, int H, int W, int D, double sx, double ox, double sy, double oy, double sz, double oz,
+                     double sigma, float *warped, double *ll, void *workspace, size_t workspace_bytes,
+                     void *stream);
+
+/* Scratch bytes of cpab_register3d_ll. */
+size_t cpab_register3d_workspace_bytes(const cpab_ctx *ctx, int N, int H, int W, int D);
+
+/* The registration log-likelihood of N (theta, src, dst) volume triples in
+ * one launch: the 3D form of cpab_register_ll (the reference's registration
+ * likelihood, cpab/cpa2d/model/transformations/register/
+ * _ScaleDependentLogLikelihoodGaussian.py:34-109, exists for 2D images; the
+ * 3D remap it would use is remap3d above).  Every voxel centre
+ * ((c+0.5)/W, (r+0.5)/H, (k+0.5)/D) of the unit cube is integrated with
+ * instance n's tables (sign -1 for calc_T_inv), src[n] is sampled there
+ * (trilinear) and compared with dst[n].  3D spaces; REF scheme. */
+int cpab_register3d_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, int N, const float *src,
+                       const float *dst, int H, int W, int D, double sigma, int precision, double dt,
+                       int nTimeSteps, int nStepsODE, double *ll, float *warped, void *workspace,
+                       size_t workspace_bytes, uint64_t *counters, void *stream);
+
 /* Scratch bytes of cpab_landmark_ll for N instances of n_lm landmarks. */
 size_t cpab_landmark_workspace_bytes(const cpab_ctx *ctx, int N, int n_lm);
 

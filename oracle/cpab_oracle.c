@@ -565,3 +565,64 @@ double oracle_remap_ssd(const double *map, const float *src, const float *dst, i
     }
     return s;
 }
+
+/* ------------------------------------------------------------------ */
+/* trilinear remap (3D) and its Gaussian log-likelihood                 */
+/* ------------------------------------------------------------------ */
+
+/* The 3D counterpart of bilinear() for remap3d (external of.gpu.remap,
+ * called at cpab/cpa3d/TransformWrapper.py:254-286): a volume img [H, W, D]
+ * indexed img[row][col][slice] -- the order of the reference's dense 3D grid,
+ * np.mgrid[0:Ny, 0:Nx, 0:Nz] raveled with z fastest
+ * (cpab/cpa3d/calcs/_CpaCalcs.py:45-76) -- is sampled at a point (x, y, z) =
+ * (column, row, slice) in voxel coordinates, integer coordinates at voxel
+ * centres, taps outside the volume read 0.  Interpolation along x, then y,
+ * then z. */
+static inline double tap3(const float *img, int H, int W, int D, int r, int c, int k)
+{
+    return (r >= 0 && r < H && c >= 0 && c < W && k >= 0 && k < D) ? (double)img[((int64_t)r * W + c) * D + k] : 0.0;
+}
+static inline double trilinear(const float *img, int H, int W, int D, double px, double py, double pz)
+{
+    double fx0 = floor(px), fy0 = floor(py), fz0 = floor(pz);
+    if (!(fx0 > -2.0 && fx0 < (double)W + 1.0 && fy0 > -2.0 && fy0 < (double)H + 1.0 && fz0 > -2.0 &&
+          fz0 < (double)D + 1.0))
+        return 0.0;
+    double fx = px - fx0, fy = py - fy0, fz = pz - fz0;
+    int c0 = (int)fx0, r0 = (int)fy0, k0 = (int)fz0;
+    double v[2];
+    for (int dk = 0; dk < 2; ++dk) {
+        double top = (1 - fx) * tap3(img, H, W, D, r0, c0, k0 + dk) + fx * tap3(img, H, W, D, r0, c0 + 1, k0 + dk);
+        double bot = (1 - fx) * tap3(img, H, W, D, r0 + 1, c0, k0 + dk) +
+                     fx * tap3(img, H, W, D, r0 + 1, c0 + 1, k0 + dk);
+        v[dk] = (1 - fy) * top + fy * bot;
+    }
+    return (1 - fz) * v[0] + fz * v[1];
+}
+
+/* map [H*W*D, 3] (x, y, z); voxel coordinates px = x*sx + ox etc. */
+void oracle_remap3d(const double *map, const float *src, double *out, int H, int W, int D, double sx, double ox,
+                    double sy, double oy, double sz, double oz)
+{
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)H * W * D; ++i)
+        out[i] = trilinear(src, H, W, D, map[3 * i] * sx + ox, map[3 * i + 1] * sy + oy, map[3 * i + 2] * sz + oz);
+}
+
+double oracle_remap3d_ssd(const double *map, const float *src, const float *dst, int H, int W, int D, double sx,
+                          double ox, double sy, double oy, double sz, double oz, double sigma, double *warped)
+{
+    double s = 0, comp = 0;
+    double k = -0.5 / (sigma * sigma);
+    for (int64_t i = 0; i < (int64_t)H * W * D; ++i) {
+        double w = trilinear(src, H, W, D, map[3 * i] * sx + ox, map[3 * i + 1] * sy + oy, map[3 * i + 2] * sz + oz);
+        if (warped) warped[i] = w;
+        double e = w - (double)dst[i];
+        double term = e * e * k;
+        double y = term - comp;
+        double tt = s + y;
+        comp = (tt - s) - y;
+        s = tt;
+    }
+    return s;
+}

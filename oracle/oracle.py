@@ -58,6 +58,7 @@ def lib() -> C.CDLL:
         L.oracle_calc_T.restype = C.c_int64
         L.oracle_closed_form_1d.restype = C.c_int64
         L.oracle_remap_ssd.restype = C.c_double
+        L.oracle_remap3d_ssd.restype = C.c_double
         _ora = L
     return _ora
 
@@ -269,6 +270,32 @@ def remap_ssd(map_pts, src, dst, sigma, sx, ox, sy, oy):
                                 C.c_double(sx), C.c_double(ox), C.c_double(sy), C.c_double(oy),
                                 C.c_double(sigma), _d(warped))
     return float(ll), warped.reshape(H, W)
+
+
+def remap3d(map_pts, src, sx, ox, sy, oy, sz, oz) -> np.ndarray:
+    """warped [H, W, D] float64 from a map [H*W*D, 3] and a float32 volume [H, W, D]
+    (cpab_oracle.c oracle_remap3d: img[row][col][slice], trilinear, zero outside)."""
+    src = np.ascontiguousarray(src, dtype=np.float32)
+    H, W, D = src.shape
+    mp = _c64(map_pts)
+    out = np.empty(H * W * D)
+    lib().oracle_remap3d(_d(mp), src.ctypes.data_as(_fp), _d(out), C.c_int(H), C.c_int(W), C.c_int(D),
+                         C.c_double(sx), C.c_double(ox), C.c_double(sy), C.c_double(oy), C.c_double(sz),
+                         C.c_double(oz))
+    return out.reshape(H, W, D)
+
+
+def remap3d_ssd(map_pts, src, dst, sigma, sx, ox, sy, oy, sz, oz):
+    """(ll, warped) of the trilinear remap, ll = sum -0.5 (warped - dst)^2 / sigma^2 (Kahan sum)."""
+    src = np.ascontiguousarray(src, dtype=np.float32)
+    dst = np.ascontiguousarray(dst, dtype=np.float32)
+    H, W, D = src.shape
+    mp = _c64(map_pts)
+    warped = np.empty(H * W * D)
+    ll = lib().oracle_remap3d_ssd(_d(mp), src.ctypes.data_as(_fp), dst.ctypes.data_as(_fp), C.c_int(H), C.c_int(W),
+                                  C.c_int(D), C.c_double(sx), C.c_double(ox), C.c_double(sy), C.c_double(oy),
+                                  C.c_double(sz), C.c_double(oz), C.c_double(sigma), _d(warped))
+    return float(ll), warped.reshape(H, W, D)
 
 
 def register_ll(t: OracleTess, Trels_inv, sA_inv, src, dst, sigma, dt, nT, nODE):
