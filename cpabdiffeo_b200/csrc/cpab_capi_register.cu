@@ -403,6 +403,39 @@ int cpab_mcmc_propose(cpab_ctx *ctx, int C, int d, const double *theta, const do
     return cuda_status(ctx, launch_mcmc_propose(a, (cudaStream_t)stream), "mcmc_propose launch");
 }
 
+int cpab_mcmc_propose_local(cpab_ctx *ctx, int C, int d, const double *theta, int nV, const double *E,
+                            const double *G, const int32_t *bdry, double s, uint64_t seed, const int64_t *step,
+                            double *theta_prop, void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    int st = check_mcmc(ctx, C, d, theta, theta_prop, step);
+    if (st != CPAB_OK) return st;
+    if (C == 0) return CPAB_OK;
+    if (nV < 1) return fail(ctx, CPAB_BAD_SHAPE, "nV < 1");
+    if (!E || !G || !bdry) return fail(ctx, CPAB_BAD_ARG, "E/G/bdry is NULL");
+    if (!std::isfinite(s)) return fail(ctx, CPAB_BAD_ARG, "s is not finite");
+    if ((int64_t)C * 32 > 0x7fffffffLL) return fail(ctx, CPAB_BAD_SHAPE, "too many chains");
+    CPAB_CHECK_ALIGN(ctx, {theta, 8, "theta"}, {E, 8, "E"}, {G, 8, "G"}, {bdry, 4, "bdry"}, {step, 8, "step"},
+                     {theta_prop, 8, "theta_prop"});
+    if (overlaps(theta, (size_t)C * d * 8, theta_prop, (size_t)C * d * 8))
+        return fail(ctx, CPAB_ALIAS, "theta and theta_prop overlap");
+    LocalProposalArgs a;
+    memset(&a, 0, sizeof(a));
+    a.C = C;
+    a.d = d;
+    a.dim = ctx->t.dim;
+    a.nV = nV;
+    a.theta = theta;
+    a.theta_prop = theta_prop;
+    a.E = E;
+    a.G = G;
+    a.bdry = bdry;
+    a.s = s;
+    a.seed = seed;
+    a.step = step;
+    return cuda_status(ctx, launch_mcmc_propose_local(a, (cudaStream_t)stream), "mcmc_propose_local launch");
+}
+
 int cpab_mcmc_accept(cpab_ctx *ctx, int C, int d, double *theta, const double *theta_prop, double *ll,
                      const double *ll_prop, double inv_npts, const double *prior_prec, double wlp, double *lp,
                      int rule, uint64_t seed, int64_t *step, int64_t *n_accepted, void *stream)

@@ -62,7 +62,7 @@ __device__ __forceinline__ double u53(unsigned hi, unsigned lo)
     return ((double)m + 0.5) * (1.0 / 9007199254740992.0);
 }
 
-enum { STREAM_PROPOSAL = 0, STREAM_ACCEPT = 1 };
+enum { STREAM_PROPOSAL = 0, STREAM_ACCEPT = 1, STREAM_LOCAL = 2 };
 
 // One thread per (chain, pair of coordinates).
 __global__ void k_mcmc_propose(McmcArgs a)
@@ -137,6 +137,56 @@ __global__ void k_mcmc_accept(McmcArgs a)
     }
 }
 
+// Local proposal (cpab/cpaNd/inference/Proposal.py:65-130): pick a vertex k
+// uniformly, add s * z (z ~ N(0, I_dim)) to its velocity -- or, for a vertex
+// on the domain boundary, set its velocity to 0 -- and map the change to
+// theta: theta' = theta + G[k] dv.  One warp per chain; Philox stream 2,
+// word 0 of counter (chain, step, 2, 0) picks k, counters (.., 1 + p) give the
+// normal pairs.
+__global__ void k_mcmc_propose_local(LocalProposalArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t step = *a.step;
+    const unsigned k0 = (unsigned)a.seed, k1 = (unsigned)(a.seed >> 32);
+    const unsigned hi = (unsigned)(((unsigned long long)step >> 32) << 8 | STREAM_LOCAL);
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int chain = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; chain < a.C; chain += nwarps) {
+        const U4 r0 = philox4x32_10(U4{(unsigned)chain, (unsigned)step, hi, 0u}, k0, k1);
+        int k = (int)(u53(r0.x, r0.y) * (double)a.nV);
+        k = k < a.nV ? k : a.nV - 1;
+        const double *th = a.theta + (int64_t)chain * a.d;
+        double dv[3] = {0.0, 0.0, 0.0};
+        if (a.bdry[k]) {
+            // dv = -v_k = -E[k] theta (lanes split the dot products, fixed-order warp sum)
+            for (int r = 0; r < a.dim; ++r) {
+                const double *e = a.E + ((int64_t)k * a.dim + r) * a.d;
+                double acc = 0.0;
+                for (int i = lane; i < a.d; i += 32) acc += e[i] * th[i];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
+                dv[r] = -acc;
+            }
+        } else {
+            for (int p = 0; 2 * p < a.dim; ++p) {
+                const U4 r = philox4x32_10(U4{(unsigned)chain, (unsigned)step, hi, 1u + (unsigned)p}, k0, k1);
+                const double u1 = u53(r.x, r.y), u2 = u53(r.z, r.w);
+                const double rad = sqrt(-2.0 * log(u1));
+                double sn, cs;
+                sincospi(2.0 * u2, &sn, &cs);
+                dv[2 * p] = a.s * rad * cs;
+                if (2 * p + 1 < a.dim) dv[2 * p + 1] = a.s * rad * sn;
+            }
+        }
+        double *tp = a.theta_prop + (int64_t)chain * a.d;
+        const double *g = a.G + (int64_t)k * a.d * a.dim;
+        for (int i = lane; i < a.d; i += 32) {
+            double v = th[i];
+            for (int r = 0; r < a.dim; ++r) v += g[(int64_t)i * a.dim + r] * dv[r];
+            tp[i] = v;
+        }
+    }
+}
+
 __global__ void k_mcmc_advance(int64_t *step) { *step += 1; }
 
 cudaError_t launch_mcmc_propose(const McmcArgs &a, cudaStream_t s)
@@ -145,6 +195,14 @@ cudaError_t launch_mcmc_propose(const McmcArgs &a, cudaStream_t s)
     int grid = (int)((n + 255) / 256);
     if (grid < 1) grid = 1;
     k_mcmc_propose<<<grid, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mcmc_propose_local(const LocalProposalArgs &a, cudaStream_t s)
+{
+    int grid = (a.C * 32 + 255) / 256;
+    if (grid < 1) grid = 1;
+    k_mcmc_propose_local<<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

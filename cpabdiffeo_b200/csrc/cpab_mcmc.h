@@ -24,7 +24,21 @@ struct McmcArgs {
     int64_t *n_accepted;        // [C] or nullptr
 };
 
+// Local (vertex-velocity) proposal tables and draws.
+struct LocalProposalArgs {
+    int C, d, dim, nV;
+    const double *theta;        // [C, d]
+    double *theta_prop;         // [C, d]
+    const double *E;            // [nV, dim, d]  velocity at vertex k = E[k] theta
+    const double *G;            // [nV, d, dim]  theta change for a velocity change at vertex k
+    const int *bdry;            // [nV] vertex on the domain boundary
+    double s;                   // step of the velocity perturbation
+    uint64_t seed;
+    const int64_t *step;
+};
+
 cudaError_t launch_mcmc_propose(const McmcArgs &a, cudaStream_t s);
+cudaError_t launch_mcmc_propose_local(const LocalProposalArgs &a, cudaStream_t s);
 cudaError_t launch_mcmc_accept(const McmcArgs &a, cudaStream_t s);
 cudaError_t launch_mcmc_advance(int64_t *step, cudaStream_t s);
 

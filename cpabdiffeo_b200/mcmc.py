@@ -1,10 +1,12 @@
-"""Batched Metropolis-Hastings image registration: C independent chains,
-each with its own (src, dst) image pair, advanced in lock-step on the GPU.
+"""Batched Metropolis-Hastings registration: C independent chains, each with
+its own data (an image pair, a volume pair or a landmark set), advanced in
+lock-step on the GPU.
 
 One step per chain (cpab/cpaNd/inference/Metropolis.py:41-85,
-cpab/cpaNd/inference/Proposal.py:29-64):
-  theta' = theta + scale * sqrt(diag Sigma_CPA) * z
-  ll'    = registration log-likelihood of theta' (fused kernel, map never stored)
+cpab/cpaNd/inference/Proposal.py:29-130):
+  theta' = theta + scale * sqrt(diag Sigma_CPA) * z   (random walk), or the
+           local proposal: one vertex velocity perturbed (use_local=True)
+  ll'    = log-likelihood of theta' (fused kernel, map never stored)
   log_ratio = (ll' - ll) / nPts  [+ wlp * (lp' - lp)]
   accept if log_ratio > 0, else by u ~ U(0,1) with the reference's own test
   log(u) > log_ratio (rule="reference", the default) or the textbook test
@@ -19,14 +21,17 @@ import torch
 
 from . import _lib
 from .cpa_space import CpaSpace
-from .landmarks import LandmarkLogLikelihood
-from .registration import GaussianLogLikelihood
 
 
 class BatchedMetropolis:
-    def __init__(self, ll: GaussianLogLikelihood | LandmarkLogLikelihood, theta0: torch.Tensor, prop_std: np.ndarray, scale: float = 0.05,
+    def __init__(self, ll, theta0: torch.Tensor, prop_std: np.ndarray | None = None, scale: float = 0.05,
                  seed: int = 0, rule: str = "reference", use_ave_ll: bool = True,
-                 prior_precision: np.ndarray | None = None, wlp: float = 1.0):
+                 prior_precision: np.ndarray | None = None, wlp: float = 1.0, use_local: bool = False,
+                 scale_local_proposal: float = 10.0):
+        """ll: GaussianLogLikelihood(3D) or LandmarkLogLikelihood.  use_local
+        selects the local (vertex-velocity) proposal of Proposal.py:65-130 with
+        step scale_local_proposal * min(XMAXS) (0.01 in 1D, :96-103) instead of
+        the Gaussian random walk with prop_std."""
         self.ll_fn = ll
         sp: CpaSpace = ll.space
         self.space = sp
@@ -37,7 +42,20 @@ class BatchedMetropolis:
         self.d = sp.d
         self.theta = torch.as_tensor(theta0, dtype=torch.float64, device=dev).reshape(self.C, self.d).clone()
         self.theta_prop = torch.empty_like(self.theta)
-        self.prop_std = torch.as_tensor(np.asarray(prop_std, dtype=np.float64), device=dev).contiguous()
+        self.use_local = bool(use_local)
+        if self.use_local:
+            from .space import local_proposal_tables
+            tabs = local_proposal_tables(sp.geo)
+            self.local_nV = int(tabs.vertices.shape[0])
+            self.local_E = torch.as_tensor(tabs.E, device=dev).contiguous()
+            self.local_G = torch.as_tensor(tabs.G, device=dev).contiguous()
+            self.local_bdry = torch.as_tensor(tabs.bdry.astype(np.int32), device=dev).contiguous()
+            self.local_s = float(scale_local_proposal) * float(np.min(sp.XMAXS)) if sp.dim > 1 else 0.01
+            self.prop_std = None
+        else:
+            if prop_std is None:
+                raise ValueError("prop_std is needed for the random-walk proposal")
+            self.prop_std = torch.as_tensor(np.asarray(prop_std, dtype=np.float64), device=dev).contiguous()
         self.scale = float(scale)
         self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
         self.rule = {"reference": 0, "standard": 1}[rule]
@@ -63,8 +81,14 @@ class BatchedMetropolis:
     def _step_launches(self) -> None:
         sp, c = self.space, self.space._ctx
         s = _lib.stream_ptr()
-        c.check(c.lib.cpab_mcmc_propose(c.h, self.C, self.d, _lib.ptr(self.theta), _lib.ptr(self.prop_std), self.scale,
-                                        self.seed, _lib.ptr(self.step), _lib.ptr(self.theta_prop), s))
+        if self.use_local:
+            c.check(c.lib.cpab_mcmc_propose_local(c.h, self.C, self.d, _lib.ptr(self.theta), self.local_nV,
+                                                  _lib.ptr(self.local_E), _lib.ptr(self.local_G),
+                                                  _lib.ptr(self.local_bdry), self.local_s, self.seed,
+                                                  _lib.ptr(self.step), _lib.ptr(self.theta_prop), s))
+        else:
+            c.check(c.lib.cpab_mcmc_propose(c.h, self.C, self.d, _lib.ptr(self.theta), _lib.ptr(self.prop_std),
+                                            self.scale, self.seed, _lib.ptr(self.step), _lib.ptr(self.theta_prop), s))
         c.check(c.lib.cpab_theta_to_trels(c.h, _lib.ptr(sp.B), self.d, _lib.ptr(self.theta_prop), self.C,
                                           self.ll_fn.dt, self.sign, None, _lib.ptr(self.sA), _lib.ptr(self.Tr), s))
         self.ll_fn.batch_tables((self.sA, self.Tr), ll=self.ll_prop)

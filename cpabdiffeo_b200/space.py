@@ -376,3 +376,56 @@ def pixel_centers(H: int, W: int) -> np.ndarray:
     """[H*W, 2] points ((col+0.5)/W, (row+0.5)/H), row-major (row outer)."""
     ys, xs = np.meshgrid((np.arange(H) + 0.5) / H, (np.arange(W) + 0.5) / W, indexing="ij")
     return np.stack([xs.ravel(), ys.ravel()], axis=1)
+
+
+# --------------------------------------------------------------------------- local proposal
+
+
+@dataclass(frozen=True)
+class LocalProposalTables:
+    """The linear maps behind the local (vertex-velocity) proposal of
+    cpab/cpaNd/inference/Proposal.py:65-130.  With velTess the velocities at
+    the tessellation's vertices (cpa_space.Avees2velTess / velTess2Avees):
+      E[k] (dim x d): velocity at vertex k of theta, v_k = E[k] theta;
+      G[k] (d x dim): theta change for a velocity change dv at vertex k alone,
+                      B^T (A(velTess + e_k dv) - A(velTess)) = G[k] dv,
+                      velTess2Avees then Avees2theta (B^T, :377-390);
+      bdry[k]:        vertex k on the domain boundary (the reference then sets
+                      its velocity to 0, :104-120).
+    Simplicial tessellations only (1D, or type I), as in the reference (:73-74)."""
+    vertices: np.ndarray   # [nV, dim]
+    E: np.ndarray          # [nV, dim, d]
+    G: np.ndarray          # [nV, d, dim]
+    bdry: np.ndarray       # [nV] bool
+
+
+def local_proposal_tables(geo: SpaceGeometry) -> LocalProposalTables:
+    dim, nC, ne = geo.dim, geo.nC, geo.lengthAvee
+    if dim != 1 and geo.tess != TESS_I:
+        raise NotImplementedError("the local proposal needs a simplicial tessellation (1D or type I)")
+    V_all = geo.cells[:, :, :dim].reshape(-1, dim)
+    key = np.round(V_all * 2 ** 30).astype(np.int64)
+    uniq, inv = np.unique(key, axis=0, return_inverse=True)
+    inv = inv.reshape(nC, dim + 1)
+    nV = uniq.shape[0]
+    verts = np.zeros((nV, dim))
+    verts[inv.ravel()] = V_all
+    B = geo.B.reshape(nC, dim, dim + 1, -1)                # A_c[r, j] = B[c, r, j, :] theta
+    d = B.shape[-1]
+    E = np.zeros((nV, dim, d))
+    G = np.zeros((nV, d, dim))
+    for c in range(nC):
+        Vh = np.concatenate([geo.cells[c, :, :dim], np.ones((dim + 1, 1))], axis=1).T   # [dim+1, dim+1], columns [v_i; 1]
+        Vinv = np.linalg.inv(Vh)
+        for i in range(dim + 1):
+            k = inv[c, i]
+            if not E[k].any():
+                E[k] = np.einsum("rjd,j->rd", B[c], Vh[:, i])     # v_k = A_c [v_k; 1]
+            # A_c = Vel Vh^-1: a change dv at vertex i changes A_c by dv (x) Vh^-1[i, :]
+            for r in range(dim):
+                G[k, :, r] += np.einsum("jd,j->d", B[c, r], Vinv[i, :])
+    lo, hi = np.asarray(geo.xmins), np.asarray(geo.xmaxs)
+    bdry = np.any(np.isclose(verts, lo[None]) | np.isclose(verts, hi[None]), axis=1)
+    if not any(geo.zero_v_across_bdry):
+        bdry[:] = False
+    return LocalProposalTables(verts, E, G, bdry)

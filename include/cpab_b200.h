@@ -298,6 +298,21 @@ int cpab_landmark_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
 int cpab_mcmc_propose(cpab_ctx *ctx, int C, int d, const double *theta, const double *prop_std, double scale,
                       uint64_t seed, const int64_t *step, double *theta_prop, void *stream);
 
+/* Local proposals for C chains (the use_local branch of Proposal.__call__,
+ * cpab/cpaNd/inference/Proposal.py:65-130): with velTess the velocities at the
+ * tessellation's nV vertices, pick a vertex k uniformly (Philox stream 2,
+ * counter (chain, *step, 2, 0)), add s * z to its velocity (z ~ N(0, I_dim),
+ * counters (chain, *step, 2, 1 + pair)) -- or set it to 0 when bdry[k] (the
+ * reference's boundary rule, :104-120) -- and map the change to theta:
+ *   theta_prop[c] = theta[c] + G[k] dv,   v_k = E[k] theta.
+ * E [nV, dim, d], G [nV, d, dim] float64 and bdry [nV] int32 come from the
+ * space's geometry (local_proposal_tables in cpabdiffeo_b200/space.py); the
+ * reference's s is scale_local_proposal * min(XMAXS) (0.01 in 1D).  Simplicial
+ * tessellations (1D, type I), as in the reference. */
+int cpab_mcmc_propose_local(cpab_ctx *ctx, int C, int d, const double *theta, int nV, const double *E,
+                            const double *G, const int32_t *bdry, double s, uint64_t seed, const int64_t *step,
+                            double *theta_prop, void *stream);
+
 /* Accept/reject for C chains and advance *step by one (Metropolis.step,
  * cpab/cpaNd/inference/Metropolis.py:41-85): log_ratio = (ll_prop - ll) *
  * inv_npts (+ wlp * (lp' - lp) with the prior precision prior_prec [d, d]);

@@ -349,6 +349,27 @@ def mcmc_normals(seed: int, step: int, C: int, d: int) -> np.ndarray:
     return z[:, :d]
 
 
+def mcmc_local_draws(seed: int, step: int, C: int, nV: int, dim: int):
+    """(k [C], z [C, dim]) of the local proposal at `step` (Philox stream 2): the
+    vertex from word 0 of counter (chain, step, 2, 0), the normals from
+    counters (chain, step, 2, 1 + pair), as the GPU draws them."""
+    key = (seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF)
+    hi = ((step >> 32) << 8) | 2
+    ch = np.arange(C)
+    c0 = np.stack([ch, np.full_like(ch, step & 0xFFFFFFFF), np.full_like(ch, hi), np.zeros_like(ch)], -1)
+    r0 = philox4x32_10(c0.astype(np.uint64), key)
+    k = np.minimum((_u53(r0[..., 0], r0[..., 1]) * nV).astype(np.int64), nV - 1)
+    z = np.empty((C, 2 * ((dim + 1) // 2)))
+    for p in range((dim + 1) // 2):
+        c = np.stack([ch, np.full_like(ch, step & 0xFFFFFFFF), np.full_like(ch, hi), np.full_like(ch, 1 + p)], -1)
+        r = philox4x32_10(c.astype(np.uint64), key)
+        u1, u2 = _u53(r[..., 0], r[..., 1]), _u53(r[..., 2], r[..., 3])
+        rad = np.sqrt(-2.0 * np.log(u1))
+        z[:, 2 * p] = rad * np.cos(2 * np.pi * u2)
+        z[:, 2 * p + 1] = rad * np.sin(2 * np.pi * u2)
+    return k, z[:, :dim]
+
+
 def mcmc_log_uniform(seed: int, step: int, C: int) -> np.ndarray:
     ch = np.arange(C)
     c = np.stack([ch, np.full_like(ch, step & 0xFFFFFFFF), np.full_like(ch, ((step >> 32) << 8) | 1),

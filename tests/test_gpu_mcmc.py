@@ -76,3 +76,47 @@ def test_mcmc_graph_replay_equals_eager():
     torch.cuda.synchronize()
     assert torch.equal(a.theta, b.theta) and torch.equal(a.ll, b.ll)
     assert torch.equal(a.n_accepted, b.n_accepted) and int(b.step.item()) == 10
+
+
+def test_local_proposal_matches_oracle_draws(oracle_mod):
+    """theta' = theta + G[k] dv with the oracle's Philox stream-2 draws: dv = s z at
+    an interior vertex, -E[k] theta (velocity set to 0) at a boundary vertex."""
+    from cpabdiffeo_b200 import _lib
+    from cpabdiffeo_b200.space import local_proposal_tables
+    O = oracle_mod
+    sp, src, dst, prop_std = _problem(C=64)
+    ll = GaussianLogLikelihood(sp, torch.as_tensor(src, device=DEV), torch.as_tensor(dst, device=DEV), 0.05, P)
+    rng = np.random.default_rng(2)
+    theta0 = Prior.create(sp.geo, 0.1, 1.0).sample(64, rng)
+    mh = BatchedMetropolis(ll, torch.as_tensor(theta0, device=DEV), use_local=True, scale_local_proposal=0.3, seed=21)
+    mh.step.fill_(5)
+    c = sp._ctx
+    c.check(c.lib.cpab_mcmc_propose_local(c.h, mh.C, mh.d, _lib.ptr(mh.theta), mh.local_nV, _lib.ptr(mh.local_E),
+                                          _lib.ptr(mh.local_G), _lib.ptr(mh.local_bdry), mh.local_s, mh.seed,
+                                          _lib.ptr(mh.step), _lib.ptr(mh.theta_prop), _lib.stream_ptr()))
+    tabs = local_proposal_tables(sp.geo)
+    k, z = O.mcmc_local_draws(21, 5, 64, tabs.vertices.shape[0], 2)
+    assert tabs.bdry[k].any() and (~tabs.bdry[k]).any()          # both kinds drawn
+    want = np.empty_like(theta0)
+    for ch in range(64):
+        dv = -tabs.E[k[ch]] @ theta0[ch] if tabs.bdry[k[ch]] else mh.local_s * z[ch]
+        want[ch] = theta0[ch] + tabs.G[k[ch]] @ dv
+    np.testing.assert_allclose(mh.theta_prop.cpu().numpy(), want, rtol=0, atol=1e-12)
+    # the proposal moves exactly one vertex velocity
+    for ch in range(8):
+        v_old = np.einsum("krd,d->kr", tabs.E, theta0[ch])
+        v_new = np.einsum("krd,d->kr", tabs.E, mh.theta_prop[ch].cpu().numpy())
+        moved = np.abs(v_new - v_old).max(axis=1) > 1e-12
+        assert moved.sum() <= 1 and (not moved.any() or moved[k[ch]])
+
+
+def test_local_proposal_chains_run_and_improve():
+    sp, src, dst, prop_std = _problem(C=8)
+    ll = GaussianLogLikelihood(sp, torch.as_tensor(src, device=DEV), torch.as_tensor(dst, device=DEV), 0.05, P)
+    mh = BatchedMetropolis(ll, torch.zeros((8, sp.d), device=DEV), use_local=True, scale_local_proposal=0.05,
+                           seed=4)
+    ll0 = mh.ll.clone()
+    mh.run(60, graph_steps=20)
+    torch.cuda.synchronize()
+    assert (mh.ll > ll0).float().mean() >= 0.75
+    torch.testing.assert_close(mh.ll, ll.batch(mh.theta), rtol=0, atol=0)
