@@ -216,6 +216,16 @@ def measured_peaks(torch) -> dict:
     return out
 
 
+# DRAM bytes per launch measured with ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum, one captured launch of the timed region):
+#  * k_exact1d on the 2048-theta case (42.7 M points): 301.0 MB, 7.04 B/point,
+#    scaled to a launch by the points it processes;
+#  * k_integrate on the 2D 4096 x 8192-point workload: 884.3 MB per launch;
+#  * k_remap_ssd_bulk on 256 pairs of 256^2 images: 272.1 MB per launch.
+TRAFFIC_EXACT1D_BYTES_PER_POINT = 301.0e6 / 42737756
+TRAFFIC_2D_BYTES_PER_LAUNCH = 884.34e6
+TRAFFIC_REMAP_BYTES_PER_LAUNCH = 272.09e6
+
 # Closed-form segment cost model (FP64 operations): per cell visit the
 # crossing test and hitting time take 10 arithmetic operations plus one log,
 # the final in-cell evaluation 6 plus one exp; log and exp are counted as 20
@@ -518,7 +528,8 @@ def bench_2d(args, torch, dev) -> dict:
                          "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off",
                          "flop_model": f"per step 2*{C_CELL_2D}+{M_2D}, per midpoint sub-step "
                                        f"{C_CELL_2D}+2*{M_2D}+8 (algorithmic, before compensation)",
-                         "kernel_ms": kern_ms, "algorithmic_flop_per_launch": flops, "traffic": None},
+                         "kernel_ms": kern_ms, "algorithmic_flop_per_launch": flops,
+                         "traffic": TRAFFIC_2D_BYTES_PER_LAUNCH},
             "error_vs_fp64_oracle": {"max_abs": err, "points_checked": 4 * npt, "tolerance": 1e-5}}
 
 
@@ -586,7 +597,7 @@ def bench_remap(args, torch, dev) -> dict:
             "roofline": {"bound": "hbm", "kernel": "k_remap_ssd<float>", "achieved": r["achieved_gbs"],
                          "peak": r["hbm_peak_gbs"], "unit": "GB/s", "frac": r["frac"],
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
-                         "bytes_per_pixel": 16, "traffic": None}}
+                         "bytes_per_pixel": 16, "traffic": TRAFFIC_REMAP_BYTES_PER_LAUNCH}}
 
 
 def main():
@@ -770,7 +781,9 @@ def main():
                             "peak_source": "measured here: cuBLAS DGEMM 4096^3",
                             "flop_model": f"{EXACT_FLOP_PER_VISIT} per cell visit + {EXACT_FLOP_PER_POINT} per point "
                                           "(log/exp counted as 20)",
-                            "kernel_ms": kern_ms, "traffic": None,
+                            "kernel_ms": kern_ms,
+                            "traffic": TRAFFIC_EXACT1D_BYTES_PER_POINT * n_total,
+                            "traffic_note": "ncu DRAM bytes of one launch on the 2048-theta case, scaled by points",
                             "algorithmic_flop_per_launch": flops,
                             "hbm_achieved_gbs": 2 * pts_h.nbytes / (kern_ms * 1e-3) / 1e9,
                             "hbm_peak_gbs": peaks.get("hbm_gbs")}
