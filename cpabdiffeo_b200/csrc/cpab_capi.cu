@@ -11,8 +11,8 @@ thread_local char cpab::g_thread_err[512];
 
 static size_t tables_smem(const cpab_ctx *c, int prec)
 {
-    // float64: A and T; float32: A and the (T - I) hi/lo pair
-    return (size_t)c->t.nC * cell_len(c) * (prec == CPAB_F64 ? 2 * 8 : 3 * 4);
+    // float64: A and T; float32: A and T - I
+    return (size_t)c->t.nC * cell_len(c) * (prec == CPAB_F64 ? 2 * 8 : 2 * 4);
 }
 
 int cpab::max_smem_optin()

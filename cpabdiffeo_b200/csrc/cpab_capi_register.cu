@@ -123,7 +123,7 @@ int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
     if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
     const int tile_px = ctx->cfg.tile_pts;
     // cell tables plus one double per pixel of a tile
-    if ((size_t)ctx->t.nC * 6 * (precision == CPAB_F64 ? 2 * 8 : 3 * 4) + (size_t)tile_px * 8 >
+    if ((size_t)ctx->t.nC * 6 * (precision == CPAB_F64 ? 2 * 8 : 2 * 4) + (size_t)tile_px * 8 >
         (size_t)max_smem_optin())
         return fail(ctx, CPAB_UNSUPPORTED, "cell tables and tile scratch exceed shared memory");
     const WsLayout L = ws_layout(N, tiles_of(H, W, tile_px));

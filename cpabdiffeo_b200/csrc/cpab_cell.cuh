@@ -271,6 +271,16 @@ CPAB_HD int fast_box_coord(float p, int n, float inv)
 
 CPAB_HD int fast_cell_2d_tri(const Tess &t, const float *p)
 {
+    if (p[0] > 0.0f && p[0] < t.fhi[0] && p[1] > 0.0f && p[1] < t.fhi[1]) {
+        // strictly inside the domain (the common case): the clamps below are
+        // no-ops and none of the boundary rules applies -- same result
+        const float u = p[0] * t.finv_inc[0], w = p[1] * t.finv_inc[1];
+        const float kx = floorf(u), ky = floorf(w);
+        const float x = u - kx, y = w - ky;
+        const int c = ((int)fminf(kx, (float)(t.nC0 - 1)) + (int)fminf(ky, (float)(t.nC1 - 1)) * t.nC0) * 4;
+        const float omx = 1.0f - x;
+        return c + ((x < y) ? ((omx < y) ? 2 : 3) : ((omx < y) ? 1 : 0));
+    }
     float p0 = fminf(t.fhi[0], fmaxf(0.0f, p[0]));
     float p1 = fminf(t.fhi[1], fmaxf(0.0f, p[1]));
     float u = p0 * t.finv_inc[0], w = p1 * t.finv_inc[1];

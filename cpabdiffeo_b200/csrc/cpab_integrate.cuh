@@ -18,14 +18,14 @@ namespace cpab {
 //    adds its increment d to hi and the rounding error of that addition
 //    (Fast2Sum; |d| is a small step, and where |hi| < |d| the error term is
 //    below ulp(d)) to lo, so the many small increments of the integration are
-//    not lost to float rounding.  The closed-form step table holds T - I
-//    split into a float pair (hi, lo), so rounding T to float does not bias
-//    every step; the velocity table A is plain float.
+//    not lost to float rounding.  The closed-form step table holds T - I in
+//    float: its rounding is relative to the small step dt*A, not to the
+//    position, so it does not bias every step; the velocity table A is float.
 // Shared-memory tables per cell (ne = DIM * (DIM + 1)):
 //  double: A[ne], T[ne], row-major as in global memory;
-//  float:  A[ne], then per cell (T-I)_hi[ne] followed by (T-I)_lo[ne], each
-//          column-major (the DIM columns of the linear part, then the
-//          offset) so that a cell's matrix is read with 8- or 16-byte loads.
+//  float:  A[ne] and (T - I)[ne], column-major (the DIM columns of the
+//          linear part, then the offset) so that a cell's matrix is read with
+//          8-byte (1D/2D) or 16-byte (3D) loads.
 
 template <int DIM, typename Real>
 struct PState;
@@ -86,8 +86,8 @@ struct PState<DIM, float> {
 
 template <typename Real>
 struct TableLayout {
-    // floats per cell of the closed-form table (double: T; float: (T-I) hi and lo)
-    static constexpr int kTParts = sizeof(Real) == 8 ? 1 : 2;
+    // tables of the closed-form step per cell (double: T; float: T - I)
+    static constexpr int kTParts = 1;
 };
 
 // Stage one instance's tables in shared memory (layout above).
@@ -105,12 +105,7 @@ __device__ __forceinline__ void stage_tables(const double *gA, const double *gT,
             const int c = i / NE, e = i - c * NE, r = e / (DIM + 1), col = e - r * (DIM + 1);
             const int cm = col * DIM + r;
             sA[c * NE + cm] = (Real)gA[i];
-            if (with_T) {
-                const double d = gT[i] - (r == col ? 1.0 : 0.0);
-                const float hi = (float)d;
-                sT[c * 2 * NE + cm] = hi;
-                sT[c * 2 * NE + NE + cm] = (float)(d - (double)hi);
-            }
+            if (with_T) sT[c * NE + cm] = (float)(gT[i] - (r == col ? 1.0 : 0.0));
         }
     }
 }
@@ -194,12 +189,9 @@ __device__ __forceinline__ void advance(bool fast, const PState<DIM, float> &s, 
     load_cell<DIM>(fast ? T : A, m);
     cm_affine<DIM>(y, m, s.x);
     if (fast) {
-        // d = (T - I)[x; 1], the lo part of the table added first
-        float l[NE], e[DIM];
-        load_cell<DIM>(T + NE, l);
-        cm_affine<DIM>(e, l, s.x);
+        // d = (T - I)[x; 1]: the increment of the step, from the small matrix T - I
 #pragma unroll
-        for (int r = 0; r < DIM; ++r) d[r] = y[r] + e[r];
+        for (int r = 0; r < DIM; ++r) d[r] = y[r];
     } else {
         float pm[DIM];
         const float hh = 0.5f * h;
@@ -249,7 +241,6 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
                                                 const int *start_cells = nullptr)
 {
     constexpr int NE = DIM * (DIM + 1);
-    constexpr bool kTwoPart = TableLayout<Real>::kTParts == 2;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     int64_t next = ws + 32;
@@ -276,8 +267,7 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
         if (active) {
             const bool fast = (SCHEME == SCHEME_REF) && sub_left == 0;
             PState<DIM, Real> q;
-            // float tables interleave (T-I)_hi and (T-I)_lo per cell
-            advance<DIM>(fast, st, sA + c * NE, sT + (kTwoPart ? 2 : 1) * c * NE, nullptr, h, q);
+            advance<DIM>(fast, st, sA + c * NE, sT + c * NE, nullptr, h, q);
             const int cq = cell_of<DIM, TESS>(t, q);
             if (fast && cq != c) {
                 // the end point left the cell: redo the step with nStepsODE sub-steps from p

@@ -151,7 +151,7 @@ cudaError_t launch_dt(const LandmarkArgs &a, int prec, const LaunchCfg &cfg, cud
 size_t landmark_smem_bytes(const Tess &t, int tile_pts, int prec)
 {
     const int ne = t.dim * (t.dim + 1);
-    const size_t tables = prec == PREC_F64 ? (size_t)t.nC * ne * 2 * 8 : (size_t)t.nC * ne * 3 * 4;
+    const size_t tables = prec == PREC_F64 ? (size_t)t.nC * ne * 2 * 8 : (size_t)t.nC * ne * 2 * 4;
     return tables + (size_t)tile_pts * sizeof(double);
 }
 

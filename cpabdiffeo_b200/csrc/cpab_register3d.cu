@@ -251,7 +251,7 @@ cudaError_t launch_register3d_t(const Register3dArgs &a, const LaunchCfg &cfg, c
 
 size_t register3d_smem_bytes(int nC, int tile_px, int prec)
 {
-    const size_t tables = prec == PREC_F64 ? (size_t)nC * 12 * 2 * 8 : (size_t)nC * 12 * 3 * 4;
+    const size_t tables = prec == PREC_F64 ? (size_t)nC * 12 * 2 * 8 : (size_t)nC * 12 * 2 * 4;
     return tables + (size_t)tile_px * sizeof(double);
 }
 
