@@ -45,20 +45,27 @@ int cpab_ctx_create(cpab_ctx **out, int dim, int tess, const int *nCs, const dou
         return fail(nullptr, CPAB_BAD_ARG, "invalid nCs/incs (need nCs >= 1, finite incs > 0, at most 2^20 cells)");
     }
     for (int k = 0; k < 3; ++k) c->nCs[k] = k < dim ? nCs[k] : 1;
-    // cancel flag in mapped host memory (only where a device is present)
+    // cancel flag (only where a device is present)
     int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0) {
-        void *h = nullptr;
-        if (cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped) == cudaSuccess) {
-            void *d = nullptr;
-            if (cudaHostGetDevicePointer(&d, h, 0) == cudaSuccess) {
-                c->cancel_host = static_cast<int *>(h);
+    if (cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0 && cudaGetDevice(&c->device) == cudaSuccess) {
+        void *d = nullptr, *h = nullptr;
+        cudaStream_t st = nullptr;
+        if (cudaMalloc(&d, sizeof(int)) == cudaSuccess && cudaHostAlloc(&h, 2 * sizeof(int), 0) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess) {
+            static_cast<int *>(h)[0] = 0;
+            static_cast<int *>(h)[1] = 1;
+            if (cudaMemcpy(d, h, sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess) {
                 c->cancel_dev = static_cast<int *>(d);
-                *c->cancel_host = 0;
-            } else {
-                cudaFreeHost(h);
+                c->cancel_src = static_cast<int *>(h);
+                c->cancel_stream = st;
+                d = h = nullptr;
+                st = nullptr;
             }
         }
+        if (d) cudaFree(d);
+        if (h) cudaFreeHost(h);
+        if (st) cudaStreamDestroy(st);
+        if (!c->cancel_dev) c->device = -1;
     }
     cudaGetLastError();  // a missing device is not an error here
     *out = c;
@@ -67,30 +74,43 @@ int cpab_ctx_create(cpab_ctx **out, int dim, int tess, const int *nCs, const dou
 
 int cpab_ctx_destroy(cpab_ctx *ctx)
 {
-    if (ctx && ctx->cancel_host) cudaFreeHost(ctx->cancel_host);
+    if (ctx && ctx->cancel_dev) {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->cancel_stream);
+        cudaStreamDestroy(ctx->cancel_stream);
+        cudaFree(ctx->cancel_dev);
+        cudaFreeHost(ctx->cancel_src);
+        cudaSetDevice(prev);
+    }
     delete ctx;
     return CPAB_OK;
 }
 
-int cpab_cancel(cpab_ctx *ctx)
+// Write the device flag (0 or 1) and wait for that 4-byte copy only.
+static int set_cancel_flag(cpab_ctx *ctx, int v)
 {
     if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
-    if (!ctx->cancel_host) return fail(ctx, CPAB_UNSUPPORTED, "this context has no cancel flag");
-    __atomic_store_n(ctx->cancel_host, 1, __ATOMIC_SEQ_CST);
-    return CPAB_OK;
+    if (!ctx->cancel_dev) return fail(ctx, CPAB_UNSUPPORTED, "this context has no cancel flag");
+    __atomic_store_n(&ctx->cancel_state, v, __ATOMIC_SEQ_CST);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != ctx->device) cudaSetDevice(ctx->device);
+    cudaError_t e = cudaMemcpyAsync(ctx->cancel_dev, ctx->cancel_src + v, sizeof(int), cudaMemcpyHostToDevice,
+                                    ctx->cancel_stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->cancel_stream);
+    if (prev != ctx->device) cudaSetDevice(prev);
+    return cuda_status(ctx, e, "cancel flag");
 }
 
-int cpab_clear_cancel(cpab_ctx *ctx)
-{
-    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
-    if (!ctx->cancel_host) return fail(ctx, CPAB_UNSUPPORTED, "this context has no cancel flag");
-    __atomic_store_n(ctx->cancel_host, 0, __ATOMIC_SEQ_CST);
-    return CPAB_OK;
-}
+int cpab_cancel(cpab_ctx *ctx) { return set_cancel_flag(ctx, 1); }
+
+int cpab_clear_cancel(cpab_ctx *ctx) { return set_cancel_flag(ctx, 0); }
 
 int cpab_cancel_requested(const cpab_ctx *ctx)
 {
-    return (ctx && ctx->cancel_host) ? __atomic_load_n(ctx->cancel_host, __ATOMIC_SEQ_CST) : 0;
+    return ctx ? __atomic_load_n(&ctx->cancel_state, __ATOMIC_SEQ_CST) : 0;
 }
 
 const char *cpab_last_error_string(const cpab_ctx *ctx) { return ctx ? ctx->err : g_thread_err; }
@@ -114,7 +134,7 @@ int cpab_set_launch(cpab_ctx *ctx, int block, int ctas_per_sm, int tile_pts)
     if (block && (block < 32 || block > 256 || block % 32))
         return fail(ctx, CPAB_BAD_ARG, "block must be a multiple of 32 in [32, 256] (got %d)", block);
     if (ctas_per_sm < 0 || ctas_per_sm > 64) return fail(ctx, CPAB_BAD_ARG, "ctas_per_sm out of range");
-    if (tile_pts < 0) return fail(ctx, CPAB_BAD_ARG, "tile_pts < 0");
+    if (tile_pts < 0 || tile_pts > 65536) return fail(ctx, CPAB_BAD_ARG, "tile_pts out of [1, 65536] (got %d)", tile_pts);
     if (block) ctx->cfg.block = block;
     if (ctas_per_sm) ctx->cfg.ctas_per_sm = ctas_per_sm;
     if (tile_pts) ctx->cfg.tile_pts = tile_pts;
@@ -238,7 +258,7 @@ static IntegrateArgs make_args(cpab_ctx *ctx, const double *signedA, const doubl
     a.counters = reinterpret_cast<unsigned long long *>(counters);
     a.max_crossings = 4 * ctx->t.nC + 8;
     a.sort = ctx->cfg.sort;
-    a.cancel = ctx->cancel_dev;
+    a.cancel = cancel_ptr(ctx);
     return a;
 }
 

@@ -150,7 +150,7 @@ int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
     a.dt = dt;
     a.nTimeSteps = nTimeSteps;
     a.nStepsODE = nStepsODE;
-    a.cancel = ctx->cancel_dev;
+    a.cancel = cancel_ptr(ctx);
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(a.tickets, 0, (size_t)N * sizeof(unsigned), s);
     if (e != cudaSuccess) return cuda_status(ctx, e, "ticket reset");
@@ -284,7 +284,7 @@ int cpab_register3d_ll(cpab_ctx *ctx, const double *signedA, const double *Trels
     a.dt = dt;
     a.nTimeSteps = nTimeSteps;
     a.nStepsODE = nStepsODE;
-    a.cancel = ctx->cancel_dev;
+    a.cancel = cancel_ptr(ctx);
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(a.tickets, 0, (size_t)N * sizeof(unsigned), s);
     if (e != cudaSuccess) return cuda_status(ctx, e, "ticket reset");
@@ -354,7 +354,7 @@ int cpab_landmark_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
     a.clamp = ctx->clamp;
     a.clamp_lo = ctx->clamp_lo;
     a.clamp_hi = ctx->clamp_hi;
-    a.cancel = ctx->cancel_dev;
+    a.cancel = cancel_ptr(ctx);
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(a.tickets, 0, (size_t)N * sizeof(unsigned), s);
     if (e != cudaSuccess) return cuda_status(ctx, e, "ticket reset");

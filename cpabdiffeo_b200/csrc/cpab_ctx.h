@@ -18,8 +18,15 @@ struct cpab_ctx {
     int clamp = 0;
     double clamp_lo = 0, clamp_hi = 0;
     cpab::LaunchCfg cfg;
-    int *cancel_host = nullptr;  // mapped pinned host flag
-    int *cancel_dev = nullptr;   // its device-side address
+    // Cancellation: a flag in device memory that the persistent kernels poll
+    // (an L2 read), written by a 4-byte DMA from a pinned {0, 1} pair on a
+    // private non-blocking stream -- no SM is needed to set it while kernels
+    // occupy the GPU, and the kernels never read host memory over PCIe.
+    int *cancel_dev = nullptr;
+    int *cancel_src = nullptr;         // pinned host {0, 1}
+    cudaStream_t cancel_stream = nullptr;
+    int cancel_state = 0;              // host mirror (atomic)
+    int device = -1;                   // the device the flag lives on
     char err[512] = {0};
 };
 
@@ -70,6 +77,14 @@ inline const char *misaligned(std::initializer_list<AlignReq> reqs)
         if (const char *m_ = ::cpab::misaligned({__VA_ARGS__}))                                             \
             return fail(ctx, CPAB_BAD_ARG, "%s is not aligned to its element size", m_);                   \
     } while (0)
+
+// The cancel flag to hand to a launch: the context's device flag when the
+// launch goes to the device the flag lives on, else none (no polling).
+inline const volatile int *cancel_ptr(const cpab_ctx *c)
+{
+    int d = -1;
+    return (c->cancel_dev && cudaGetDevice(&d) == cudaSuccess && d == c->device) ? c->cancel_dev : nullptr;
+}
 
 int max_smem_optin();
 

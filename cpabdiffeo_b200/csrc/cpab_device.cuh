@@ -82,7 +82,7 @@ __device__ __forceinline__ TileInfo decode_tile(const Batch &b, int64_t tile)
 
 // True (in every thread of the CTA) once the context's cancel flag is set;
 // call at a point all threads reach.  The persistent kernels poll it every
-// 8th tile (a read of mapped host memory costs about a microsecond).
+// 8th tile (the flag is in device memory: an L2 read).
 __device__ __forceinline__ bool cta_cancelled(const volatile int *flag, unsigned long long *counters)
 {
     __shared__ int s_stop;

@@ -79,38 +79,37 @@ __device__ __forceinline__ double cf_phi(const Exact1D &e, int c, double x, doub
 // Every visit after the first starts at a nudged vertex (x_k + 1e-12 when
 // entering cell k from the left, x_{k+1} - 1e-12 from the right), so its
 // hitting time depends on (cell, direction) only.  Those are evaluated once
-// per instance with the same function (cf_crossing) into shared memory:
-//   enter[0][k], enter[1][k]  entry point from the left / right,
-//   tc[0][k], nx[0][k]        hitting time and next cell from the left entry,
-//   tc[1][k], nx[1][k]        ... from the right entry.
-// The walk then reads the table; the results are those of evaluating
+// per instance with the same function (cf_crossing) into shared memory, one
+// record per (cell k, direction dir) at index 2 k + dir:
+//   te[.] = {hitting time, entry point},  cn[.] = {cell of the entry point, next cell}
+// (dir 0: entered from the left, 1: from the right), so a step of the walk
+// is one 16-byte and one 8-byte load.  The results are those of evaluating
 // cf_crossing at every visit.
 struct Transit {
-    double *enter0, *enter1, *tc0, *tc1;
-    int *nx0, *nx1, *cell0, *cell1;
+    double2 *te;
+    int2 *cn;
 };
 
 __device__ void build_transit(const Exact1D &e, Transit tr)
 {
     for (int k = threadIdx.x; k < e.nC; k += blockDim.x) {
-        double x0 = fmin(1.0, fmax(0.0, vert(e, k) + 1e-12));
-        double x1 = fmin(1.0, fmax(0.0, vert(e, k + 1) - 1e-12));
-        tr.enter0[k] = x0;
-        tr.enter1[k] = x1;
-        int c0 = cf_cell(e, x0), c1 = cf_cell(e, x1), n0, n1;
-        tr.cell0[k] = c0;
-        tr.cell1[k] = c1;
-        tr.tc0[k] = cf_crossing(e, x0, c0, n0);
-        tr.nx0[k] = n0;
-        tr.tc1[k] = cf_crossing(e, x1, c1, n1);
-        tr.nx1[k] = n1;
+        const double x0 = fmin(1.0, fmax(0.0, vert(e, k) + 1e-12));
+        const double x1 = fmin(1.0, fmax(0.0, vert(e, k + 1) - 1e-12));
+        const int c0 = cf_cell(e, x0), c1 = cf_cell(e, x1);
+        int n0, n1;
+        const double t0 = cf_crossing(e, x0, c0, n0);
+        const double t1 = cf_crossing(e, x1, c1, n1);
+        tr.te[2 * k] = make_double2(t0, x0);
+        tr.te[2 * k + 1] = make_double2(t1, x1);
+        tr.cn[2 * k] = make_int2(c0, n0);
+        tr.cn[2 * k + 1] = make_int2(c1, n1);
     }
 }
 
 // calc_phi for one point; returns false when the crossing cap is hit
 // (the reference raises ValueError, ClosedFormInt.py:155-160).
 __device__ bool cf_point(const Exact1D &e, const Transit &tr, double x, double t, int cap, double &out,
-                         unsigned long long &visits)
+                         unsigned &visits)
 {
     double x_old = x, t_rem = t;
     if (0 < x_old && x_old < 1) {
@@ -131,42 +130,40 @@ __device__ bool cf_point(const Exact1D &e, const Transit &tr, double x, double t
     // after the loop so that all lanes of a warp evaluate it together
     for (int counter = 0;;) {
         ++visits;
-        if (tc >= t_rem) break;
+        // stop when the remaining time ends inside this cell, when no further
+        // crossing exists (cn < 0), and on NaN (comparisons with NaN are false)
+        if (!(tc < t_rem) || cn < 0 || cn >= e.nC) break;
         t_rem -= tc;
+        // enter cell cn at the nudged vertex: from the left when moving right
+        const int idx = 2 * cn + (cn > c ? 0 : 1);
+        const double2 te = tr.te[idx];
         if (++counter >= cap) {
             // the point would have been left at the crossing it just made
-            x_old = (cn > c) ? tr.enter0[cn] : tr.enter1[cn];
+            x_old = te.y;
             ok = false;
             break;
         }
-        // enter cell cn at the nudged vertex and read its transit from the table
-        if (cn > c) {
-            x_old = tr.enter0[cn];
-            c = tr.cell0[cn];
-            tc = tr.tc0[cn];
-            cn = tr.nx0[cn];
-        } else {
-            x_old = tr.enter1[cn];
-            c = tr.cell1[cn];
-            tc = tr.tc1[cn];
-            cn = tr.nx1[cn];
-        }
+        const int2 nn = tr.cn[idx];
+        x_old = te.y;
+        tc = te.x;
+        c = nn.x;
+        cn = nn.y;
     }
     out = ok ? fmin(1.0, fmax(0.0, cf_phi(e, c, x_old, t_rem))) : x_old;
     return ok;
 }
 
-// Shared memory of k_exact1d: per cell A (2 doubles), b/a and 1/a (2),
-// entry points and hitting times (4 doubles), next and entry cells (4 ints)
-// -- 80 bytes, so what follows is 16-byte aligned -- and, when cell-sorting,
-// sorted start points and results in input order [tile_pts] (Real), the
-// permutation [tile_pts] and the histogram [nC] (int).
+// Shared memory of k_exact1d: per cell A (2 doubles), b/a and 1/a (2), and
+// two transit records (2 x (16 + 8) bytes) -- 80 bytes, so what follows is
+// 16-byte aligned -- and, when cell-sorting, sorted start points and results
+// in input order [tile_pts] (Real), the permutation [tile_pts] (16-bit) and
+// the histogram [nC] (int).
 size_t exact1d_smem_bytes(int nC, int tile_pts, int sort, int prec)
 {
-    size_t b = (size_t)nC * (8 * sizeof(double) + 4 * sizeof(int));
+    size_t b = (size_t)nC * (4 * sizeof(double) + 2 * (sizeof(double2) + sizeof(int2)));
     if (sort)
         b += 2 * (size_t)tile_pts * (prec == PREC_F64 ? sizeof(double) : sizeof(float)) +
-             ((size_t)nC + (size_t)tile_pts) * sizeof(int);
+             (size_t)tile_pts * sizeof(unsigned short) + ((size_t)nC + 2) * sizeof(int);
     return b;
 }
 
@@ -178,26 +175,22 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
     double *sA = reinterpret_cast<double *>(smem_raw);
     double *s_ba = sA + 2 * nC, *s_ia = s_ba + nC;
     Transit tr;
-    tr.enter0 = s_ia + nC;
-    tr.enter1 = tr.enter0 + nC;
-    tr.tc0 = tr.enter1 + nC;
-    tr.tc1 = tr.tc0 + nC;
-    tr.nx0 = reinterpret_cast<int *>(tr.tc1 + nC);
-    tr.nx1 = tr.nx0 + nC;
-    tr.cell0 = tr.nx1 + nC;
-    tr.cell1 = tr.cell0 + nC;
+    tr.te = reinterpret_cast<double2 *>(s_ia + nC);
+    tr.cn = reinterpret_cast<int2 *>(tr.te + 2 * nC);
     // cell-sort scratch (see exact1d_smem_bytes)
     const int tp = a.batch.tile_pts;
-    Real *s_xs = reinterpret_cast<Real *>(tr.cell1 + nC);
+    Real *s_xs = reinterpret_cast<Real *>(tr.cn + 2 * nC);
     Real *s_y = s_xs + tp;
-    int *s_perm = reinterpret_cast<int *>(s_y + tp);
-    int *s_hist = s_perm + tp;
+    unsigned short *s_perm = reinterpret_cast<unsigned short *>(s_y + tp);
+    // the histogram after the 16-bit permutation, rounded up to a 4-byte boundary
+    int *s_hist = reinterpret_cast<int *>(s_perm + ((tp + 1) & ~1));
     __shared__ TileInfo s_tile;
     __shared__ int s_claim;
     const double T_total = a.dt * (double)a.nTimeSteps;
     const int64_t ntiles = total_tiles(a.batch);
     const int lane = threadIdx.x & 31;
     unsigned long long c_pts = 0, c_fail = 0, c_visits = 0, c_nan = 0;
+    unsigned visits = 0;  // folded into c_visits after every tile
     int loaded = -1;
     Exact1D e;
     e.A = sA;
@@ -247,7 +240,7 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
             for (int j = threadIdx.x; j < n; j += blockDim.x) {
                 const Real xin = s_y[j];
                 const int pos = atomicAdd(s_hist + cf_cell(e, (double)xin), 1);
-                s_perm[pos] = j;
+                s_perm[pos] = (unsigned short)j;
                 s_xs[pos] = xin;
             }
             __syncthreads();
@@ -264,7 +257,7 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
                 if (a.sort) xin = s_xs[k];
                 else load_pt<1, Real>(a.pts_in, ti.start + k, &xin);
                 double y;
-                bool ok = cf_point(e, tr, (double)xin, T_total, cap, y, c_visits);
+                bool ok = cf_point(e, tr, (double)xin, T_total, cap, y, visits);
                 if (a.clamp) y = clamp_ref(y, a.clamp_lo, a.clamp_hi);
                 Real yo = (Real)y;
                 if (a.sort) s_y[s_perm[k]] = yo;
@@ -274,6 +267,8 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
                 c_nan += (y != y) ? 1 : 0;
             }
         }
+        c_visits += visits;
+        visits = 0;
         __syncthreads();
         if (a.sort) {
             for (int j = threadIdx.x; j < n; j += blockDim.x) store_pt<1, Real>(a.pts_out, ti.start + j, s_y + j);

@@ -46,7 +46,7 @@ struct IntegrateArgs {
     unsigned long long *counters;  // [4] or nullptr: fast steps, fallback steps, sub-steps, points
     int max_crossings;    // EXACT: give up after this many boundary crossings
     int sort;             // REF/SIMPLE: process each tile's points in order of their start cell
-    const volatile int *cancel;  // host-mapped flag polled between tiles, or nullptr
+    const volatile int *cancel;  // the context's cancel flag (device memory), polled between tiles, or nullptr
 };
 
 // Counters slots.

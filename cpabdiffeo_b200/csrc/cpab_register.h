@@ -37,7 +37,7 @@ struct RegisterArgs {
     int N, H, W, tile_px;
     double sigma, dt;
     int nTimeSteps, nStepsODE;
-    const volatile int *cancel;  // host-mapped flag polled between tiles, or nullptr
+    const volatile int *cancel;  // the context's cancel flag (device memory), polled between tiles, or nullptr
 };
 
 cudaError_t launch_remap_ssd(const RemapArgs &a, int map_prec, cudaStream_t s);

@@ -85,14 +85,18 @@ const char *cpab_last_error_string(const cpab_ctx *ctx);
 int cpab_ctx_num_cells(const cpab_ctx *ctx);
 int cpab_ctx_cell_len(const cpab_ctx *ctx);
 
-/* Cancellation.  Each context owns a flag in mapped host memory that the
- * persistent integration, exact and registration kernels read before every
- * tile; once it is set they finish the tile in hand, skip the rest and count
- * themselves in CPAB_CNT_CANCELLED (no device fault, no trap).  cpab_cancel
- * may be called from any host thread while a launch runs; the flag stays set
- * until cpab_clear_cancel.  CPAB_UNSUPPORTED if the context has no flag (it is
- * allocated at cpab_ctx_create when a device is present).  No counterpart in
- * the reference (its launches cannot be stopped). */
+/* Cancellation.  Each context owns a flag in device memory (on the device
+ * current at cpab_ctx_create) that the persistent integration, exact,
+ * registration and landmark kernels read every 8th tile; once it is set they
+ * finish the tile in hand, skip the rest and count themselves in
+ * CPAB_CNT_CANCELLED (no device fault, no trap).  cpab_cancel /
+ * cpab_clear_cancel write the flag with a 4-byte copy on the context's own
+ * stream (the copy engine, so no SM is needed while kernels occupy the GPU)
+ * and return once it has landed; they may be called from any host thread
+ * while a launch runs.  The flag stays set until cpab_clear_cancel.
+ * CPAB_UNSUPPORTED if the context has no flag (it is created with the context
+ * when a device is present).  No counterpart in the reference (its launches
+ * cannot be stopped). */
 int cpab_cancel(cpab_ctx *ctx);
 int cpab_clear_cancel(cpab_ctx *ctx);
 int cpab_cancel_requested(const cpab_ctx *ctx);

@@ -1,5 +1,5 @@
 """Failure handling without faulting the GPU: cancellation through the
-context's host-mapped flag (before a launch and from another host thread
+context's flag (before a launch and from another host thread
 during one), NaN inputs surfacing as a counter instead of a hang, and the
 context staying usable afterwards."""
 import threading
