@@ -218,12 +218,12 @@ def measured_peaks(torch) -> dict:
 
 # DRAM bytes per launch measured with ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum, one captured launch of the timed region):
-#  * k_exact1d on the 2048-theta case (42.7 M points): 301.0 MB, 7.04 B/point,
+#  * k_exact1d on the 2048-theta case (42.7 M points): 299.7 MB, 7.01 B/point,
 #    scaled to a launch by the points it processes;
-#  * k_integrate on the 2D 4096 x 8192-point workload: 884.3 MB per launch;
+#  * k_integrate on the 2D 4096 x 8192-point workload: 587.9 MB per launch;
 #  * k_remap_ssd_bulk on 256 pairs of 256^2 images: 272.1 MB per launch.
-TRAFFIC_EXACT1D_BYTES_PER_POINT = 301.0e6 / 42737756
-TRAFFIC_2D_BYTES_PER_LAUNCH = 884.34e6
+TRAFFIC_EXACT1D_BYTES_PER_POINT = 299.69e6 / 42737756
+TRAFFIC_2D_BYTES_PER_LAUNCH = 587.94e6
 TRAFFIC_REMAP_BYTES_PER_LAUNCH = 272.09e6
 
 # Closed-form segment cost model (FP64 operations): per cell visit the
