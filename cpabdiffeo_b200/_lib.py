@@ -72,6 +72,9 @@ SIGNATURES = {
     "cpab_mcmc_propose": (_i, [_vp, _i, _i, _vp, _vp, _d, C.c_uint64, _vp, _vp, _vp]),
     "cpab_mcmc_propose_local": (_i, [_vp, _i, _i, _vp, _i, _vp, _vp, _vp, _d, C.c_uint64, _vp, _vp, _vp]),
     "cpab_mcmc_accept": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _d, _vp, _d, _vp, _i, C.c_uint64, _vp, _vp, _vp]),
+    "cpab_mcmc_run_workspace_bytes": (_sz, [_vp, _i, _i, _i, _i]),
+    "cpab_mcmc_run": (_i, [_vp, _vp, _i, _i, _vp, _vp, _d, _vp, _vp, _i, _i, _d, _i, _d, _i, _i, _d, _i, C.c_uint64,
+                           _vp, _i, _vp, _vp, _vp, _sz, _vp]),
     "cpab_grad_workspace_bytes": (_sz, [_vp, _i, _i64, _i, _i]),
     "cpab_grad_theta": (_i, [_vp, _vp, _i, _vp, _i, _vp, _i64, _vp, _d, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp,
                              _sz, _vp]),

@@ -472,6 +472,72 @@ int cpab_mcmc_accept(cpab_ctx *ctx, int C, int d, double *theta, const double *t
                        "mcmc_advance launch");
 }
 
+// Scratch of cpab_mcmc_run: theta_prop [C, d], signed A and Trel [C, D],
+// ll_prop [C], then the registration likelihood's own scratch.
+struct McmcRunLayout {
+    size_t theta_prop, sA, Tr, ll_prop, reg, total, reg_bytes;
+};
+
+static McmcRunLayout mcmc_run_layout(const cpab_ctx *ctx, int C, int d, int H, int W)
+{
+    McmcRunLayout L;
+    const size_t D = (size_t)ctx->t.nC * cell_len(ctx);
+    L.theta_prop = 0;
+    L.sA = L.theta_prop + align256((size_t)C * d * sizeof(double));
+    L.Tr = L.sA + align256((size_t)C * D * sizeof(double));
+    L.ll_prop = L.Tr + align256((size_t)C * D * sizeof(double));
+    L.reg = L.ll_prop + align256((size_t)C * sizeof(double));
+    L.reg_bytes = cpab_register_workspace_bytes(ctx, C, H, W);
+    L.total = L.reg + align256(L.reg_bytes);
+    return L;
+}
+
+size_t cpab_mcmc_run_workspace_bytes(const cpab_ctx *ctx, int C, int d, int H, int W)
+{
+    if (!ctx || C < 0 || d < 1 || H < 1 || W < 1) return 0;
+    return mcmc_run_layout(ctx, C, d, H, W).total;
+}
+
+int cpab_mcmc_run(cpab_ctx *ctx, const double *B, int d, int C, double *theta, const double *prop_std, double scale,
+                  const float *src, const float *dst, int H, int W, double sigma, int precision, double dt,
+                  int nTimeSteps, int nStepsODE, double inv_npts, int rule, uint64_t seed, int64_t *step,
+                  int n_steps, double *ll, int64_t *n_accepted, void *workspace, size_t workspace_bytes,
+                  void *stream)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (ctx->t.dim != 2) return fail(ctx, CPAB_UNSUPPORTED, "the registration chains are built for 2D spaces");
+    if (C < 0 || d < 1 || n_steps < 0) return fail(ctx, CPAB_BAD_SHAPE, "need C >= 0, d >= 1, n_steps >= 0");
+    if (C == 0) return CPAB_OK;
+    if (!B || !theta || !prop_std || !src || !dst || !step || !ll)
+        return fail(ctx, CPAB_BAD_ARG, "B/theta/prop_std/src/dst/step/ll is NULL");
+    const McmcRunLayout L = mcmc_run_layout(ctx, C, d, H, W);
+    if (!workspace || workspace_bytes < L.total)
+        return fail(ctx, CPAB_NO_MEMORY, "workspace of %zu bytes needed", L.total);
+    CPAB_CHECK_ALIGN(ctx, {workspace, 256, "workspace"});
+    char *w = static_cast<char *>(workspace);
+    double *theta_prop = reinterpret_cast<double *>(w + L.theta_prop);
+    double *sA = reinterpret_cast<double *>(w + L.sA);
+    double *Tr = reinterpret_cast<double *>(w + L.Tr);
+    double *ll_prop = reinterpret_cast<double *>(w + L.ll_prop);
+    void *reg = w + L.reg;
+    // the likelihood of the current state, then n_steps Metropolis steps
+    int st = cpab_theta_to_trels(ctx, B, d, theta, C, dt, -1, nullptr, sA, Tr, stream);
+    if (st == CPAB_OK)
+        st = cpab_register_ll(ctx, sA, Tr, C, src, dst, H, W, sigma, precision, dt, nTimeSteps, nStepsODE, ll,
+                              nullptr, reg, L.reg_bytes, nullptr, stream);
+    for (int k = 0; k < n_steps && st == CPAB_OK; ++k) {
+        st = cpab_mcmc_propose(ctx, C, d, theta, prop_std, scale, seed, step, theta_prop, stream);
+        if (st == CPAB_OK) st = cpab_theta_to_trels(ctx, B, d, theta_prop, C, dt, -1, nullptr, sA, Tr, stream);
+        if (st == CPAB_OK)
+            st = cpab_register_ll(ctx, sA, Tr, C, src, dst, H, W, sigma, precision, dt, nTimeSteps, nStepsODE,
+                                  ll_prop, nullptr, reg, L.reg_bytes, nullptr, stream);
+        if (st == CPAB_OK)
+            st = cpab_mcmc_accept(ctx, C, d, theta, theta_prop, ll, ll_prop, inv_npts, nullptr, 0.0, nullptr, rule,
+                                  seed, step, n_accepted, stream);
+    }
+    return st;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

@@ -45,4 +45,34 @@ __device__ __forceinline__ void finish_tile(double acc, int64_t tile, int inst, 
     __syncthreads();
 }
 
+// finish_tile for CTAs that loop over tiles: the same sums, with one barrier
+// instead of two.  Thread 0 stores the tile's partial and takes the ticket
+// after the barrier while the other warps go on with the next tile; the warp
+// sums are double-buffered by tile parity, so a buffer is written again only
+// after the next barrier, which thread 0 reaches once it is done reading.
+__device__ __forceinline__ void finish_tile_overlapped(double acc, int parity, int64_t tile, int inst,
+                                                       int tiles_of_inst, int64_t first_tile_of_inst,
+                                                       double *partials, unsigned *tickets, double *ll_out)
+{
+    __shared__ double s_w2[2][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    acc = warp_sum_f64(acc);
+    if (lane == 0) s_w2[parity][warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += s_w2[parity][w];
+        partials[tile] = s;
+        __threadfence();
+        const unsigned ticket = atomicAdd(tickets + inst, 1u);
+        if (ticket == (unsigned)tiles_of_inst - 1u) {
+            __threadfence();
+            double tot = 0.0;
+            for (int k = 0; k < tiles_of_inst; ++k) tot += ((volatile double *)partials)[first_tile_of_inst + k];
+            ll_out[inst] = tot;
+            tickets[inst] = 0u;  // ready for the next call
+        }
+    }
+}
+
 }  // namespace cpab

@@ -18,6 +18,8 @@
 // (lanes, then warps), writes its partial, and the last tile of an image to
 // finish (atomic ticket with fences) adds that image's partials in index
 // order.  A result is therefore the same alone and inside any batch.
+#include <cmath>
+
 #include <math_constants.h>
 
 #include "cpab_bulk.cuh"
@@ -96,6 +98,48 @@ __device__ __forceinline__ Real bilinear(const float *img, int H, int W, double 
     return taps_combine<Real>(t);
 }
 
+// Float coordinates for float maps whose pixel mapping is exact in float: px
+// = fma(x, sx, ox) with sx a power of two and ox 0 or -0.5 is exact except
+// for points left of the image, where it is off by at most ~1e-7 pixel (the
+// host sets RemapArgs::fcoord only then).  floor by adding 1.5 * 2^23 with
+// rounding toward -inf; taps combined in float as taps_combine<float>.
+__device__ __forceinline__ float bilinear_f(const float *img, int H, int W, float px, float py)
+{
+    constexpr float kRound = 12582912.0f;  // 1.5 * 2^23
+    const float sx = __fadd_rd(px, kRound), sy = __fadd_rd(py, kRound);
+    const float fx0 = sx - kRound, fy0 = sy - kRound;  // floor(px), floor(py) for |p| < 2^22
+    if (!(fx0 > -2.0f && fx0 < (float)W + 1.0f && fy0 > -2.0f && fy0 < (float)H + 1.0f)) return 0.0f;  // and NaN
+    const float wx = px - fx0, wy = py - fy0;
+    const int c0 = __float_as_int(sx) - 0x4B400000, r0 = __float_as_int(sy) - 0x4B400000;
+    float v[4];
+    if ((unsigned)c0 < (unsigned)(W - 1) && (unsigned)r0 < (unsigned)(H - 1)) {
+        const float *q = img + (r0 * W + c0);
+        v[0] = __ldg(q);
+        v[1] = __ldg(q + 1);
+        v[2] = __ldg(q + W);
+        v[3] = __ldg(q + W + 1);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int r = r0 + (k >> 1), c = c0 + (k & 1);
+            v[k] = (r >= 0 && r < H && c >= 0 && c < W) ? __ldg(img + (r * W + c)) : 0.0f;
+        }
+    }
+    const float top = fmaf(wx, v[1] - v[0], v[0]);
+    const float bot = fmaf(wx, v[3] - v[2], v[2]);
+    return fmaf(wy, bot - top, top);
+}
+
+// One remap sample in the map's arithmetic (FCOORD: float coordinates).
+template <typename MapT, bool FCOORD>
+__device__ __forceinline__ MapT remap_sample(const RemapArgs &a, const float *src, MapT mx, MapT my)
+{
+    if (FCOORD)
+        return (MapT)bilinear_f(src, a.H, a.W, fmaf((float)mx, (float)a.sx, (float)a.ox),
+                                fmaf((float)my, (float)a.sy, (float)a.oy));
+    return bilinear<MapT>(src, a.H, a.W, (double)mx * a.sx + a.ox, (double)my * a.sy + a.oy);
+}
+
 // ------------------------------------------------------------ standalone remap (+ SSD)
 
 // (x, y) of one map entry in shared memory with one 8- or 16-byte load.
@@ -114,7 +158,7 @@ __device__ __forceinline__ void load_pair(const double *p, double &x, double &y)
 
 // Plain path (any alignment, any image size): one pixel per thread and
 // iteration, pixels in increasing order per thread.
-template <typename MapT>
+template <typename MapT, bool FCOORD>
 __global__ void __launch_bounds__(256) k_remap_ssd(RemapArgs a)
 {
     const int inst = blockIdx.y;
@@ -130,8 +174,7 @@ __global__ void __launch_bounds__(256) k_remap_ssd(RemapArgs a)
     const double k = -0.5 / (a.sigma * a.sigma);
     double acc = 0.0;
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        const MapT w = bilinear<MapT>(src, a.H, a.W, (double)map[2 * j] * a.sx + a.ox,
-                                      (double)map[2 * j + 1] * a.sy + a.oy);
+        const MapT w = remap_sample<MapT, FCOORD>(a, src, map[2 * j], map[2 * j + 1]);
         if (warped) warped[j] = (float)w;
         if (dst) {
             const double e = (double)w - (double)__ldg(dst + j);
@@ -151,7 +194,7 @@ __global__ void __launch_bounds__(256) k_remap_ssd(RemapArgs a)
 // Same per-pixel arithmetic and per-thread order as the plain path, hence
 // the same results.  A stage whose copy does not complete within the wait
 // bound makes that image's ll NaN and leaves its warped tile unwritten.
-template <typename MapT>
+template <typename MapT, bool FCOORD>
 __global__ void __launch_bounds__(256) k_remap_ssd_bulk(RemapArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -202,7 +245,7 @@ __global__ void __launch_bounds__(256) k_remap_ssd_bulk(RemapArgs a)
             for (int j = threadIdx.x; j < n; j += blockDim.x) {
                 MapT mx, my;
                 load_pair(m + 2 * j, mx, my);
-                const MapT w = bilinear<MapT>(src, a.H, a.W, (double)mx * a.sx + a.ox, (double)my * a.sy + a.oy);
+                const MapT w = remap_sample<MapT, FCOORD>(a, src, mx, my);
                 if (warped) warped[j] = (float)w;
                 if (a.dst) {
                     const double e = (double)w - (double)dv[j];
@@ -212,16 +255,18 @@ __global__ void __launch_bounds__(256) k_remap_ssd_bulk(RemapArgs a)
         } else {
             acc = CUDART_NAN;
         }
-        if (a.dst) finish_tile(acc, tile, inst, tpi, (int64_t)inst * tpi, a.partials, a.tickets, a.ll);
-        else __syncthreads();
+        if (a.dst)
+            finish_tile_overlapped(acc, it & 1, tile, inst, tpi, (int64_t)inst * tpi, a.partials, a.tickets, a.ll);
+        else
+            __syncthreads();
     }
     // every copy this CTA issued was waited for above (the last issue targets the last tile)
 }
 
-template <typename MapT>
+template <typename MapT, bool FCOORD>
 static cudaError_t launch_remap_bulk(const RemapArgs &a, cudaStream_t s)
 {
-    auto kern = k_remap_ssd_bulk<MapT>;
+    auto kern = k_remap_ssd_bulk<MapT, FCOORD>;
     const size_t smem = 2 * (size_t)a.tile_px * (2 * sizeof(MapT) + sizeof(float));
     if (smem > kSmemOptInAbove) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -237,18 +282,32 @@ static cudaError_t launch_remap_bulk(const RemapArgs &a, cudaStream_t s)
     return cudaGetLastError();
 }
 
+static bool pow2(double v)
+{
+    int e = 0;
+    return v > 0 && std::frexp(v, &e) == 0.5;
+}
+
 cudaError_t launch_remap_ssd(const RemapArgs &a, int map_prec, cudaStream_t s)
 {
     const int64_t npx = (int64_t)a.H * a.W;
+    // float coordinates are exact for power-of-two scales with offsets 0 or -0.5
+    const bool fcoord = map_prec == PREC_F32 && pow2(a.sx) && pow2(a.sy) && a.sx <= 4194304.0 &&
+                        a.sy <= 4194304.0 && (a.ox == 0.0 || a.ox == -0.5) && (a.oy == 0.0 || a.oy == -0.5) &&
+                        a.W < (1 << 22) && a.H < (1 << 22);
     // bulk copies need 16-byte aligned sources and sizes: aligned bases and 4 | H*W
     // (tiles then start at multiples of 4 pixels and hold a multiple of 4)
     const bool bulk = (npx % 4 == 0) && (a.tile_px % 4 == 0) &&
                       (reinterpret_cast<uintptr_t>(a.map) % 16 == 0) &&
                       (!a.dst || reinterpret_cast<uintptr_t>(a.dst) % 16 == 0);
-    if (bulk) return map_prec == PREC_F64 ? launch_remap_bulk<double>(a, s) : launch_remap_bulk<float>(a, s);
+    if (bulk) {
+        if (map_prec == PREC_F64) return launch_remap_bulk<double, false>(a, s);
+        return fcoord ? launch_remap_bulk<float, true>(a, s) : launch_remap_bulk<float, false>(a, s);
+    }
     dim3 grid((unsigned)((npx + a.tile_px - 1) / a.tile_px), (unsigned)a.N);
-    if (map_prec == PREC_F64) k_remap_ssd<double><<<grid, 256, 0, s>>>(a);
-    else k_remap_ssd<float><<<grid, 256, 0, s>>>(a);
+    if (map_prec == PREC_F64) k_remap_ssd<double, false><<<grid, 256, 0, s>>>(a);
+    else if (fcoord) k_remap_ssd<float, true><<<grid, 256, 0, s>>>(a);
+    else k_remap_ssd<float, false><<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -329,6 +329,25 @@ int cpab_mcmc_accept(cpab_ctx *ctx, int C, int d, double *theta, const double *t
                      const double *ll_prop, double inv_npts, const double *prior_prec, double wlp, double *lp,
                      int rule, uint64_t seed, int64_t *step, int64_t *n_accepted, void *stream);
 
+/* Scratch bytes of cpab_mcmc_run (256-byte aligned workspace). */
+size_t cpab_mcmc_run_workspace_bytes(const cpab_ctx *ctx, int C, int d, int H, int W);
+
+/* n_steps Metropolis steps of C image-registration chains in one call
+ * (Metropolis.run, cpab/cpaNd/inference/Metropolis.py:41-85, with the
+ * random-walk Proposal.py:29-64 and the registration likelihood of
+ * cpab_register_ll): ll[c] is first set to the likelihood of theta[c], then
+ * every step enqueues cpab_mcmc_propose, cpab_theta_to_trels (sign -1),
+ * cpab_register_ll and cpab_mcmc_accept on `stream` -- the same kernels in the
+ * same order as a caller stepping one call at a time, so the chains are
+ * identical.  theta [C, d], ll [C], *step and n_accepted (may be NULL) are
+ * updated in place on the device; B [D, d] is the space's basis; no prior.
+ * 2D spaces.  Asynchronous: returns after enqueueing. */
+int cpab_mcmc_run(cpab_ctx *ctx, const double *B, int d, int C, double *theta, const double *prop_std, double scale,
+                  const float *src, const float *dst, int H, int W, double sigma, int precision, double dt,
+                  int nTimeSteps, int nStepsODE, double inv_npts, int rule, uint64_t seed, int64_t *step,
+                  int n_steps, double *ll, int64_t *n_accepted, void *workspace, size_t workspace_bytes,
+                  void *stream);
+
 /* ------------------------------------------------------------------ gradient */
 
 /* Scratch bytes of cpab_grad_theta: checkpoints every ck time steps. */

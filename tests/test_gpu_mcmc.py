@@ -120,3 +120,29 @@ def test_local_proposal_chains_run_and_improve():
     torch.cuda.synchronize()
     assert (mh.ll > ll0).float().mean() >= 0.75
     torch.testing.assert_close(mh.ll, ll.batch(mh.theta), rtol=0, atol=0)
+
+
+def test_mcmc_run_entry_point_equals_stepwise_chains():
+    """cpab_mcmc_run (one C call for n steps) enqueues the same kernels in the
+    same order as BatchedMetropolis: identical chains."""
+    from cpabdiffeo_b200 import _lib
+    sp, src, dst, prop_std = _problem(C=4)
+    srcg, dstg = torch.as_tensor(src, device=DEV), torch.as_tensor(dst, device=DEV)
+    ll_fn = GaussianLogLikelihood(sp, srcg, dstg, 0.05, P)
+    mh = BatchedMetropolis(ll_fn, torch.zeros((4, sp.d), device=DEV), prop_std, scale=0.05, seed=17)
+    mh.run(12)
+    c = sp._ctx
+    H, W = src.shape[1:]
+    theta = torch.zeros((4, sp.d), dtype=torch.float64, device=DEV)
+    ll = torch.empty(4, dtype=torch.float64, device=DEV)
+    step = torch.zeros(1, dtype=torch.int64, device=DEV)
+    acc = torch.zeros(4, dtype=torch.int64, device=DEV)
+    ws = torch.empty(int(c.lib.cpab_mcmc_run_workspace_bytes(c.h, 4, sp.d, H, W)), dtype=torch.uint8, device=DEV)
+    std = torch.as_tensor(prop_std, device=DEV)
+    c.check(c.lib.cpab_mcmc_run(c.h, _lib.ptr(sp.B), sp.d, 4, _lib.ptr(theta), _lib.ptr(std), 0.05,
+                                _lib.ptr(srcg), _lib.ptr(dstg), H, W, 0.05, _lib.CPAB_F64, P["dt"], P["nTimeSteps"],
+                                P["nStepsODEsolver"], 1.0 / (H * W), 0, 17, _lib.ptr(step), 12, _lib.ptr(ll),
+                                _lib.ptr(acc), _lib.ptr(ws), ws.numel(), _lib.stream_ptr()))
+    torch.cuda.synchronize()
+    assert torch.equal(theta, mh.theta) and torch.equal(ll, mh.ll)
+    assert torch.equal(acc, mh.n_accepted) and int(step.item()) == 12
