@@ -103,31 +103,52 @@ __device__ __forceinline__ Real bilinear(const float *img, int H, int W, double 
 // for points left of the image, where it is off by at most ~1e-7 pixel (the
 // host sets RemapArgs::fcoord only then).  floor by adding 1.5 * 2^23 with
 // rounding toward -inf; taps combined in float as taps_combine<float>.
-__device__ __forceinline__ float bilinear_f(const float *img, int H, int W, float px, float py)
+// Split in issue (the four loads) and combine so that a thread can keep the
+// taps of several pixels in flight.
+struct TapsF {
+    float v[4];
+    float wx, wy;
+    bool in;
+};
+
+__device__ __forceinline__ void tapsf_issue(const float *img, int H, int W, float px, float py, TapsF &t)
 {
     constexpr float kRound = 12582912.0f;  // 1.5 * 2^23
     const float sx = __fadd_rd(px, kRound), sy = __fadd_rd(py, kRound);
     const float fx0 = sx - kRound, fy0 = sy - kRound;  // floor(px), floor(py) for |p| < 2^22
-    if (!(fx0 > -2.0f && fx0 < (float)W + 1.0f && fy0 > -2.0f && fy0 < (float)H + 1.0f)) return 0.0f;  // and NaN
-    const float wx = px - fx0, wy = py - fy0;
-    const int c0 = __float_as_int(sx) - 0x4B400000, r0 = __float_as_int(sy) - 0x4B400000;
-    float v[4];
+    t.in = fx0 > -2.0f && fx0 < (float)W + 1.0f && fy0 > -2.0f && fy0 < (float)H + 1.0f;  // false for NaN
+    t.wx = px - fx0;
+    t.wy = py - fy0;
+    const int c0 = t.in ? __float_as_int(sx) - 0x4B400000 : -2;
+    const int r0 = t.in ? __float_as_int(sy) - 0x4B400000 : -2;
     if ((unsigned)c0 < (unsigned)(W - 1) && (unsigned)r0 < (unsigned)(H - 1)) {
         const float *q = img + (r0 * W + c0);
-        v[0] = __ldg(q);
-        v[1] = __ldg(q + 1);
-        v[2] = __ldg(q + W);
-        v[3] = __ldg(q + W + 1);
+        t.v[0] = __ldg(q);
+        t.v[1] = __ldg(q + 1);
+        t.v[2] = __ldg(q + W);
+        t.v[3] = __ldg(q + W + 1);
     } else {
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int r = r0 + (k >> 1), c = c0 + (k & 1);
-            v[k] = (r >= 0 && r < H && c >= 0 && c < W) ? __ldg(img + (r * W + c)) : 0.0f;
+            t.v[k] = (r >= 0 && r < H && c >= 0 && c < W) ? __ldg(img + (r * W + c)) : 0.0f;
         }
     }
-    const float top = fmaf(wx, v[1] - v[0], v[0]);
-    const float bot = fmaf(wx, v[3] - v[2], v[2]);
-    return fmaf(wy, bot - top, top);
+}
+
+__device__ __forceinline__ float tapsf_combine(const TapsF &t)
+{
+    if (!t.in) return 0.0f;
+    const float top = fmaf(t.wx, t.v[1] - t.v[0], t.v[0]);
+    const float bot = fmaf(t.wx, t.v[3] - t.v[2], t.v[2]);
+    return fmaf(t.wy, bot - top, top);
+}
+
+__device__ __forceinline__ float bilinear_f(const float *img, int H, int W, float px, float py)
+{
+    TapsF t;
+    tapsf_issue(img, H, W, px, py, t);
+    return tapsf_combine(t);
 }
 
 // One remap sample in the map's arithmetic (FCOORD: float coordinates).
@@ -195,7 +216,7 @@ __global__ void __launch_bounds__(256) k_remap_ssd(RemapArgs a)
 // the same results.  A stage whose copy does not complete within the wait
 // bound makes that image's ll NaN and leaves its warped tile unwritten.
 template <typename MapT, bool FCOORD>
-__global__ void __launch_bounds__(256) k_remap_ssd_bulk(RemapArgs a)
+__global__ void __launch_bounds__(256, 4) k_remap_ssd_bulk(RemapArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t s_bar[2];
@@ -239,7 +260,38 @@ __global__ void __launch_bounds__(256) k_remap_ssd_bulk(RemapArgs a)
         const float *src = a.src + (int64_t)inst * npx;
         float *warped = a.warped ? a.warped + off : nullptr;
         double acc = 0.0;
-        if (ok) {
+        if (ok && FCOORD) {
+            // four pixels' taps in flight per thread; sums still in pixel order
+            constexpr int kB = 4;
+            const MapT *m = s_map0 + stage * 2 * TP;
+            const float *dv = s_dst0 + stage * TP;
+            for (int j0 = threadIdx.x; j0 < n; j0 += kB * blockDim.x) {
+                TapsF t[kB];
+#pragma unroll
+                for (int u = 0; u < kB; ++u) {
+                    const int j = j0 + u * blockDim.x;
+                    t[u].in = false;
+                    if (j < n) {
+                        MapT mx, my;
+                        load_pair(m + 2 * j, mx, my);
+                        tapsf_issue(src, a.H, a.W, fmaf((float)mx, (float)a.sx, (float)a.ox),
+                                    fmaf((float)my, (float)a.sy, (float)a.oy), t[u]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kB; ++u) {
+                    const int j = j0 + u * blockDim.x;
+                    if (j < n) {
+                        const float w = tapsf_combine(t[u]);
+                        if (warped) warped[j] = w;
+                        if (a.dst) {
+                            const double e = (double)w - (double)dv[j];
+                            acc += e * e * k;
+                        }
+                    }
+                }
+            }
+        } else if (ok) {
             const MapT *m = s_map0 + stage * 2 * TP;
             const float *dv = s_dst0 + stage * TP;
             for (int j = threadIdx.x; j < n; j += blockDim.x) {
