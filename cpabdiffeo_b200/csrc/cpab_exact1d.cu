@@ -73,7 +73,7 @@ __device__ __forceinline__ double cf_phi(const Exact1D &e, int c, double x, doub
     if (!(0 <= x && x <= 1)) { a = 0; b = 0; }
     if (a == 0) return x + t * b;
     const double ea = exp(t * a);
-    return ea * x + b * (ea - 1) / a;
+    return ea * x + b * (ea - 1) * e.ia[c];  // b (e^{at} - 1) / a with the cell's precomputed 1/a
 }
 
 // Every visit after the first starts at a nudged vertex (x_k + 1e-12 when

@@ -75,4 +75,22 @@ __device__ __forceinline__ void finish_tile_overlapped(double acc, int parity, i
     }
 }
 
+// The tile's partial only (fixed lane / warp order, one barrier, warp sums
+// double-buffered by tile parity as above): for kernels whose per-instance
+// sums are finished by sum_partials_in_order afterwards, so no fence or
+// atomic sits in the tile loop.
+__device__ __forceinline__ void store_tile_partial(double acc, int parity, int64_t tile, double *partials)
+{
+    __shared__ double s_w3[2][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    acc = warp_sum_f64(acc);
+    if (lane == 0) s_w3[parity][warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += s_w3[parity][w];
+        partials[tile] = s;
+    }
+}
+
 }  // namespace cpab

@@ -202,10 +202,7 @@ __global__ void __launch_bounds__(256) k_remap_ssd(RemapArgs a)
             acc += e * e * k;
         }
     }
-    if (dst) {
-        const int tpi = (int)gridDim.x;
-        finish_tile(acc, (int64_t)inst * tpi + tile, inst, tpi, (int64_t)inst * tpi, a.partials, a.tickets, a.ll);
-    }
+    if (dst) store_tile_partial(acc, 0, (int64_t)inst * gridDim.x + tile, a.partials);
 }
 
 // Bulk path (16-byte aligned map and dst, H*W a multiple of 4): a persistent
@@ -308,7 +305,7 @@ __global__ void __launch_bounds__(256, 4) k_remap_ssd_bulk(RemapArgs a)
             acc = CUDART_NAN;
         }
         if (a.dst)
-            finish_tile_overlapped(acc, it & 1, tile, inst, tpi, (int64_t)inst * tpi, a.partials, a.tickets, a.ll);
+            store_tile_partial(acc, it & 1, tile, a.partials);
         else
             __syncthreads();
     }
@@ -334,6 +331,18 @@ static cudaError_t launch_remap_bulk(const RemapArgs &a, cudaStream_t s)
     return cudaGetLastError();
 }
 
+// ll[inst] = sum of the instance's tile partials in index order (the same
+// order, hence the same value, as the last-tile summation of finish_tile).
+static __global__ void k_sum_partials(const double *partials, int tiles_per_inst, int N, double *ll)
+{
+    const int inst = blockIdx.x * blockDim.x + threadIdx.x;
+    if (inst >= N) return;
+    const double *p = partials + (int64_t)inst * tiles_per_inst;
+    double tot = 0.0;
+    for (int k = 0; k < tiles_per_inst; ++k) tot += p[k];
+    ll[inst] = tot;
+}
+
 static bool pow2(double v)
 {
     int e = 0;
@@ -352,14 +361,21 @@ cudaError_t launch_remap_ssd(const RemapArgs &a, int map_prec, cudaStream_t s)
     const bool bulk = (npx % 4 == 0) && (a.tile_px % 4 == 0) &&
                       (reinterpret_cast<uintptr_t>(a.map) % 16 == 0) &&
                       (!a.dst || reinterpret_cast<uintptr_t>(a.dst) % 16 == 0);
+    cudaError_t e;
     if (bulk) {
-        if (map_prec == PREC_F64) return launch_remap_bulk<double, false>(a, s);
-        return fcoord ? launch_remap_bulk<float, true>(a, s) : launch_remap_bulk<float, false>(a, s);
+        if (map_prec == PREC_F64) e = launch_remap_bulk<double, false>(a, s);
+        else e = fcoord ? launch_remap_bulk<float, true>(a, s) : launch_remap_bulk<float, false>(a, s);
+    } else {
+        dim3 grid((unsigned)((npx + a.tile_px - 1) / a.tile_px), (unsigned)a.N);
+        if (map_prec == PREC_F64) k_remap_ssd<double, false><<<grid, 256, 0, s>>>(a);
+        else if (fcoord) k_remap_ssd<float, true><<<grid, 256, 0, s>>>(a);
+        else k_remap_ssd<float, false><<<grid, 256, 0, s>>>(a);
+        e = cudaGetLastError();
     }
-    dim3 grid((unsigned)((npx + a.tile_px - 1) / a.tile_px), (unsigned)a.N);
-    if (map_prec == PREC_F64) k_remap_ssd<double, false><<<grid, 256, 0, s>>>(a);
-    else if (fcoord) k_remap_ssd<float, true><<<grid, 256, 0, s>>>(a);
-    else k_remap_ssd<float, false><<<grid, 256, 0, s>>>(a);
+    if (e != cudaSuccess || !a.dst) return e;
+    // per-image sums of the tile partials, in tile order
+    const int tpi = (int)((npx + a.tile_px - 1) / a.tile_px);
+    k_sum_partials<<<(a.N + 127) / 128, 128, 0, s>>>(a.partials, tpi, a.N, a.ll);
     return cudaGetLastError();
 }
 
