@@ -84,3 +84,29 @@ def test_misaligned_pointers_are_rejected_before_launch():
     assert b"map is not aligned" in lib.cpab_last_error_string(h)
     assert lib.cpab_ctx_destroy(h) == 0
 
+
+
+def test_mcmc_run_validation_before_launch():
+    """cpab_mcmc_run checks its arguments before enqueueing anything."""
+    lib = _lib.load()
+    h = C.c_void_p()
+    nCs = (C.c_int * 3)(2, 2, 2)
+    incs = (C.c_double * 3)(0.5, 0.5, 0.5)
+    assert lib.cpab_ctx_create(C.byref(h), 3, 1, nCs, incs) == 0
+    base = 1 << 20
+    args = [h, base, 10, 4, base, base, 0.05, base, base, 8, 8, 0.05, 0, 0.02, 50, 100, 1 / 64, 0, 1, base, 5, base,
+            None, base, 1 << 20, None]
+    assert lib.cpab_mcmc_run(*args) == 10                      # 3D space: UNSUPPORTED
+    assert lib.cpab_ctx_destroy(h) == 0
+    nCs2 = (C.c_int * 3)(4, 4, 1)
+    incs2 = (C.c_double * 3)(0.25, 0.25, 1.0)
+    assert lib.cpab_ctx_create(C.byref(h), 2, 1, nCs2, incs2) == 0
+    args[0] = h
+    bad = list(args)
+    bad[4] = None                                              # theta NULL
+    assert lib.cpab_mcmc_run(*bad) == 1
+    small = list(args)
+    small[24] = 16                                             # workspace too small
+    assert lib.cpab_mcmc_run(*small) == 5
+    assert b"workspace" in lib.cpab_last_error_string(h)
+    assert lib.cpab_ctx_destroy(h) == 0
