@@ -221,10 +221,10 @@ def measured_peaks(torch) -> dict:
 #  * k_exact1d on the 2048-theta case (42.7 M points): 299.7 MB, 7.01 B/point,
 #    scaled to a launch by the points it processes;
 #  * k_integrate on the 2D 4096 x 8192-point workload: 587.9 MB per launch;
-#  * k_remap_ssd_bulk on 256 pairs of 256^2 images: 272.1 MB per launch.
+#  * k_remap_ssd_bulk on 256 pairs of 256^2 images: 273.4 MB per launch.
 TRAFFIC_EXACT1D_BYTES_PER_POINT = 299.69e6 / 42737756
 TRAFFIC_2D_BYTES_PER_LAUNCH = 587.94e6
-TRAFFIC_REMAP_BYTES_PER_LAUNCH = 272.09e6
+TRAFFIC_REMAP_BYTES_PER_LAUNCH = 273.43e6
 
 # Closed-form segment cost model (FP64 operations): per cell visit the
 # crossing test and hitting time take 10 arithmetic operations plus one log,
@@ -593,8 +593,8 @@ def bench_remap(args, torch, dev) -> dict:
             "steps": max(args.steps, 3), "warmup": 3, "ms_per_step": r["ms"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (smoothed noise images)",
             "config": {"workload": "remap_ssd_256images_256x256_f32_maps", "l2": r["l2"]},
-            "gpu_launches": max(args.steps, 3), "clocks": clk.summary(),
-            "roofline": {"bound": "hbm", "kernel": "k_remap_ssd<float>", "achieved": r["achieved_gbs"],
+            "gpu_launches": 2 * max(args.steps, 3), "clocks": clk.summary(),
+            "roofline": {"bound": "hbm", "kernel": "k_remap_ssd_bulk<float> + k_sum_partials", "achieved": r["achieved_gbs"],
                          "peak": r["hbm_peak_gbs"], "unit": "GB/s", "frac": r["frac"],
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                          "bytes_per_pixel": 16, "traffic": TRAFFIC_REMAP_BYTES_PER_LAUNCH}}
