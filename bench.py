@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the cpu baseline and the 2D plain-vs-batched leg")
     ap.add_argument("--theta", type=int, default=N_THETA)
+    ap.add_argument("--e2e-chunks", type=int, default=16,
+                    help="instance groups of the host-buffer pipeline (copy in / integrate / copy out overlap)")
     ap.add_argument("--serve-seconds", type=float, default=0.5,
                     help="seconds of Poisson arrivals (2000 req/s) for the serving leg; 0 skips it")
     ap.add_argument("--workload", default="batched_1d", choices=["batched_1d", "batched_2d_nc64", "remap_ssd"],
@@ -682,7 +684,8 @@ def main():
 
     def e2e_step():
         # the public host-buffer entry point: chunked copy-in / integrate / copy-out on three streams
-        sp.calc_T_batched_host(th_pin, pts_pin, out_pin, offsets_h, mysign=1, scheme=_lib.SCHEME_EXACT, chunks=8,
+        sp.calc_T_batched_host(th_pin, pts_pin, out_pin, offsets_h, mysign=1, scheme=_lib.SCHEME_EXACT,
+                               chunks=args.e2e_chunks,
                                **p)
 
     for _ in range(2):
@@ -721,6 +724,31 @@ def main():
         lb.synchronize()
         link_ms.append(la.elapsed_time(lb))
     link_ms = min(link_ms)
+    # the same copies cut into the pipeline's chunks, chunk k copied out after it was copied in (no
+    # compute): the end-to-end pipeline's own copy schedule, whose start (first chunk in alone) and
+    # end (last chunk out alone) run one direction only
+    cuts = np.linspace(0, n_total, args.e2e_chunks + 1).astype(np.int64)
+    chunk_ms = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        la, lb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        la.record(stream)
+        s_a.wait_stream(stream)
+        for k in range(args.e2e_chunks):
+            o0, o1 = int(cuts[k]), int(cuts[k + 1])
+            with torch.cuda.stream(s_a):
+                pts[o0:o1].copy_(pts_pin[o0:o1], non_blocking=True)
+                ev_k = torch.cuda.Event()
+                ev_k.record(s_a)
+            s_b.wait_event(ev_k)
+            with torch.cuda.stream(s_b):
+                out_pin[o0:o1].copy_(out[o0:o1], non_blocking=True)
+        stream.wait_stream(s_a)
+        stream.wait_stream(s_b)
+        lb.record(stream)
+        lb.synchronize()
+        chunk_ms.append(la.elapsed_time(lb))
+    chunk_ms = min(chunk_ms)
 
     # work accounting (counters) of the timed scheme
     cnt = torch.zeros(_lib.CNT_N, dtype=torch.int64, device=dev)
@@ -765,7 +793,9 @@ def main():
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "link_only_ms": link_ms,
                     "link_bound_points_per_s": n_total * world / (link_ms * 1e-3),
-                    "pipeline": "8 chunks, 3 streams (copy in / integrate / copy out), pinned host buffers"},
+                    "chunked_copies_only_ms": chunk_ms,
+                    "chunked_copies_points_per_s": n_total * world / (chunk_ms * 1e-3),
+                    "pipeline": f"{args.e2e_chunks} chunks, 3 streams (copy in / integrate / copy out), pinned host buffers"},
             "gpu_launches": 3 * args.steps,
             "clocks": clk.summary(),
             "work": {"cell_visits": int(cnt_h[0]), "points": int(cnt_h[3]), "failed": int(cnt_h[4])},

@@ -252,6 +252,7 @@ static IntegrateArgs make_args(cpab_ctx *ctx, const double *signedA, const doubl
     a.dt = dt;
     a.nTimeSteps = nTimeSteps;
     a.nStepsODE = nStepsODE;
+    a.h_sub = dt / (double)nStepsODE;
     a.clamp = ctx->clamp;
     a.clamp_lo = ctx->clamp_lo;
     a.clamp_hi = ctx->clamp_hi;

@@ -122,8 +122,8 @@ int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
     if (nTimeSteps < 1 || nStepsODE < 1) return fail(ctx, CPAB_BAD_ARG, "nTimeSteps and nStepsODE must be >= 1");
     if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
     const int tile_px = ctx->cfg.tile_pts;
-    // cell tables plus one double per pixel of a tile
-    if ((size_t)ctx->t.nC * 6 * (precision == CPAB_F64 ? 2 * 8 : 2 * 4) + (size_t)tile_px * 8 >
+    // cell tables plus one point slot per pixel of a tile
+    if (register_smem_bytes(ctx->t.nC, tile_px, precision == CPAB_F64 ? PREC_F64 : PREC_F32) >
         (size_t)max_smem_optin())
         return fail(ctx, CPAB_UNSUPPORTED, "cell tables and tile scratch exceed shared memory");
     const WsLayout L = ws_layout(N, tiles_of(H, W, tile_px));
@@ -150,6 +150,7 @@ int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
     a.dt = dt;
     a.nTimeSteps = nTimeSteps;
     a.nStepsODE = nStepsODE;
+    a.h_sub = dt / (double)nStepsODE;
     a.cancel = cancel_ptr(ctx);
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(a.tickets, 0, (size_t)N * sizeof(unsigned), s);
@@ -284,6 +285,7 @@ int cpab_register3d_ll(cpab_ctx *ctx, const double *signedA, const double *Trels
     a.dt = dt;
     a.nTimeSteps = nTimeSteps;
     a.nStepsODE = nStepsODE;
+    a.h_sub = dt / (double)nStepsODE;
     a.cancel = cancel_ptr(ctx);
     cudaStream_t s = (cudaStream_t)stream;
     cudaError_t e = cudaMemsetAsync(a.tickets, 0, (size_t)N * sizeof(unsigned), s);
@@ -351,6 +353,7 @@ int cpab_landmark_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
     a.dt = dt;
     a.nTimeSteps = nTimeSteps;
     a.nStepsODE = nStepsODE;
+    a.h_sub = dt / (double)nStepsODE;
     a.clamp = ctx->clamp;
     a.clamp_lo = ctx->clamp_lo;
     a.clamp_hi = ctx->clamp_hi;

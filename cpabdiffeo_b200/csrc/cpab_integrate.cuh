@@ -18,12 +18,18 @@ namespace cpab {
 //    adds its increment d to hi and the rounding error of that addition
 //    (Fast2Sum; |d| is a small step, and where |hi| < |d| the error term is
 //    below ulp(d)) to lo, so the many small increments of the integration are
-//    not lost to float rounding.  The closed-form step table holds T - I in
-//    float: its rounding is relative to the small step dt*A, not to the
-//    position, so it does not bias every step; the velocity table A is float.
+//    not lost to float rounding.  Both step kinds are increments from a
+//    small matrix: the closed-form step adds (T - I)[x; 1]; an explicit
+//    midpoint sub-step of length h with the cell's velocity v(x) = A[x; 1]
+//    (both evaluations in the cell of x, calc_2Dto2D.cu:177-196) is, inside
+//    one cell, the affine map x + h v(x + h/2 v(x)) = x + (S - I)[x; 1] with
+//        S - I = [h L + h^2/2 L^2 | h b + h^2/2 L b]      (A = [L | b]),
+//    evaluated in double when the tables are staged.  Table roundings are
+//    relative to the small increments, not to the position, so they do not
+//    bias every step.
 // Shared-memory tables per cell (ne = DIM * (DIM + 1)):
 //  double: A[ne], T[ne], row-major as in global memory;
-//  float:  A[ne] and (T - I)[ne], column-major (the DIM columns of the
+//  float:  (S - I)[ne] and (T - I)[ne], column-major (the DIM columns of the
 //          linear part, then the offset) so that a cell's matrix is read with
 //          8-byte (1D/2D) or 16-byte (3D) loads.
 
@@ -90,13 +96,18 @@ struct TableLayout {
     static constexpr int kTParts = 1;
 };
 
-// Stage one instance's tables in shared memory (layout above).
+// Stage one instance's tables in shared memory (layout above); h is the
+// sub-step length dt / nStepsODE (float tables only), passed from the
+// kernel's parameters so that no register holds it during integration.
 template <int DIM, typename Real>
-__device__ __forceinline__ void stage_tables(const double *gA, const double *gT, int nC, bool with_T, Real *sA,
-                                             Real *sT)
+__device__ __forceinline__ void stage_tables(const double *gA, const double *gT, int nC, bool with_T, double h,
+                                             Real *sA, Real *sT)
 {
     constexpr int NE = DIM * (DIM + 1);
     const int tab = nC * NE;
+    // not unrolled: the staging loop's loads in flight would otherwise set
+    // the register count of the integration loop that follows
+#pragma unroll 1
     for (int i = threadIdx.x; i < tab; i += blockDim.x) {
         if (sizeof(Real) == 8) {
             sA[i] = (Real)gA[i];
@@ -104,7 +115,12 @@ __device__ __forceinline__ void stage_tables(const double *gA, const double *gT,
         } else {
             const int c = i / NE, e = i - c * NE, r = e / (DIM + 1), col = e - r * (DIM + 1);
             const int cm = col * DIM + r;
-            sA[c * NE + cm] = (Real)gA[i];
+            // (S - I)[r][col] = h (A[r][col] + h/2 sum_k L[r][k] A[k][col])
+            const double *a = gA + (size_t)c * NE;
+            double l2 = 0.0;
+#pragma unroll 1
+            for (int k = 0; k < DIM; ++k) l2 += a[r * (DIM + 1) + k] * a[k * (DIM + 1) + col];
+            sA[c * NE + cm] = (float)(h * (a[r * (DIM + 1) + col] + 0.5 * h * l2));
             if (with_T) sT[c * NE + cm] = (float)(gT[i] - (r == col ? 1.0 : 0.0));
         }
     }
@@ -165,9 +181,10 @@ __device__ __forceinline__ int cell_of(const Tess &t, const PState<DIM, float> &
 // is kept when that is still c (calc_2Dto2D.cu:380-400), a sub-step always
 // is, and its end cell is the cell of the next sub-step's start point.
 //   double: the reference's arithmetic (exact_affine / exact_midpoint).
-//   float:  both kinds share the first matrix-vector product (T - I)_hi [p; 1]
-//           resp. A [p; 1] and the compensated update, so a warp whose lanes
-//           mix closed-form steps and sub-steps diverges only in between.
+//   float:  one matrix-vector product with the cell's (T - I) or (S - I)
+//           and the compensated update -- the same instructions for both
+//           kinds, so lanes that mix closed-form steps and sub-steps do not
+//           diverge.
 template <int DIM>
 __device__ __forceinline__ void advance(bool fast, const PState<DIM, double> &s, const double *A, const double *T,
                                         const double *, double h, PState<DIM, double> &q)
@@ -181,26 +198,13 @@ __device__ __forceinline__ void advance(bool fast, const PState<DIM, double> &s,
 }
 template <int DIM>
 __device__ __forceinline__ void advance(bool fast, const PState<DIM, float> &s, const float *A, const float *T,
-                                        const float *, float h, PState<DIM, float> &q)
+                                        const float *, float, PState<DIM, float> &q)
 {
     constexpr int NE = DIM * (DIM + 1);
-    float m[NE], y[DIM], d[DIM];
-    // (T - I)_hi for a closed-form step, A for a sub-step
+    float m[NE], d[DIM];
+    // d = (T - I)[x; 1] for a closed-form step, (S - I)[x; 1] for a sub-step
     load_cell<DIM>(fast ? T : A, m);
-    cm_affine<DIM>(y, m, s.x);
-    if (fast) {
-        // d = (T - I)[x; 1]: the increment of the step, from the small matrix T - I
-#pragma unroll
-        for (int r = 0; r < DIM; ++r) d[r] = y[r];
-    } else {
-        float pm[DIM];
-        const float hh = 0.5f * h;
-#pragma unroll
-        for (int i = 0; i < DIM; ++i) pm[i] = fmaf(hh, y[i], s.x[i]);
-        cm_affine<DIM>(y, m, pm);
-#pragma unroll
-        for (int i = 0; i < DIM; ++i) d[i] = h * y[i];
-    }
+    cm_affine<DIM>(d, m, s.x);
     q = s;
 #pragma unroll
     for (int r = 0; r < DIM; ++r) q.add(r, d[r]);

@@ -41,6 +41,7 @@ struct IntegrateArgs {
     double dt;
     int nTimeSteps;
     int nStepsODE;
+    double h_sub;         // dt / nStepsODE, set on the host (read from parameter space, not a register)
     int clamp;            // 1D zero-velocity boundary: clamp to [lo, hi]
     double clamp_lo, clamp_hi;
     unsigned long long *counters;  // [4] or nullptr: fast steps, fallback steps, sub-steps, points

@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
         const TileInfo ti = s_tile;
         if (ti.inst != loaded) {
             stage_tables<DIM, Real>(a.A + (size_t)ti.inst * tab, a.T + (size_t)ti.inst * tab, a.t.nC,
-                                    SCHEME == SCHEME_REF, sA, sT);
+                                    SCHEME == SCHEME_REF, a.h_sub, sA, sT);
             loaded = ti.inst;
             __syncthreads();
         }

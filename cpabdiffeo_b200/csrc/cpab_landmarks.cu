@@ -94,7 +94,8 @@ __global__ void __launch_bounds__(256) k_landmark_ll(LandmarkArgs a)
         const int64_t end = min(start + (int64_t)a.tile_pts, base + a.n_lm);
         if (inst != loaded) {
             __syncthreads();
-            stage_tables<DIM, Real>(a.A + (size_t)inst * tab, a.T + (size_t)inst * tab, a.t.nC, true, sA, sT);
+            stage_tables<DIM, Real>(a.A + (size_t)inst * tab, a.T + (size_t)inst * tab, a.t.nC, true,
+                                    a.h_sub, sA, sT);
             loaded = inst;
         }
         LandmarkSrc<DIM> src{a.src + (int64_t)inst * a.src_stride * DIM, base};

@@ -25,6 +25,7 @@ struct LandmarkArgs {
     int N, n_lm, tile_pts;
     double sigma, dt;
     int nTimeSteps, nStepsODE;
+    double h_sub;             // dt / nStepsODE, set on the host
     int clamp;                // the context's end-point clamp (1D zero boundary), as calc_T
     double clamp_lo, clamp_hi;
     const volatile int *cancel;

@@ -381,44 +381,36 @@ cudaError_t launch_remap_ssd(const RemapArgs &a, int map_prec, cudaStream_t s)
 
 // ------------------------------------------------------------ fused registration likelihood
 
-// Start points: the pixel centres ((col+0.5)/W, (row+0.5)/H) of instance
-// inst's image; the point index within the instance is row-major.
-struct PixelSrc {
-    int H, W;
-    int64_t base;  // first global index of the instance
+// Start and end points of the current tile's pixels live in shared memory,
+// one double2 slot per pixel.  A convergent pass writes the pixel centres
+// ((col+0.5)/W, (row+0.5)/H); the lane loop takes a point's start from its
+// slot and writes its end point back; a second convergent pass samples src
+// at the end points, compares with dst and sums the terms, thread t taking
+// pixels t, t + blockDim, ... of the tile (a fixed order, so results do not
+// depend on which warp integrated which pixel).  The pixel-index arithmetic
+// and the sampling stay out of the lane loop, whose register count sets the
+// CTAs per SM, and each warp samples 32 consecutive pixels together.
+struct SlotSrc2 {
+    const double2 *slot;
+    int64_t tile_start;
     template <typename Real>
     __device__ __forceinline__ void load(int64_t i, PState<2, Real> &st) const
     {
-        const int64_t j = i - base;
-        const int64_t r = j / W, c = j - r * W;
-        double p[2];
-        p[0] = ((double)c + 0.5) / (double)W;
-        p[1] = ((double)r + 0.5) / (double)H;
+        const double2 v = slot[i - tile_start];
+        const double p[2] = {v.x, v.y};
         st.set(p);
     }
 };
 
-// End points: sampled from src and scored against dst; nothing stored
-// unless `warped` is given.  Each pixel's term goes to its slot of the
-// tile's shared-memory array, so the tile sum can be taken in a fixed order
-// whichever warp finished the pixel.
-struct SsdSnk {
-    const float *src, *dst;
-    float *warped;
-    int H, W;
-    int64_t base, tile_start;
-    double k;
-    double *term;
+struct SlotSnk2 {
+    double2 *slot;
+    int64_t tile_start;
     template <typename Real>
     __device__ __forceinline__ void put(int64_t i, const PState<2, Real> &st)
     {
-        const int64_t j = i - base;
         double p[2];
         st.get(p);
-        const Real w = bilinear<Real>(src, H, W, p[0] * W - 0.5, p[1] * H - 0.5);
-        if (warped) warped[j] = (float)w;
-        const double e = (double)w - (double)__ldg(dst + j);
-        term[i - tile_start] = e * e * k;
+        slot[i - tile_start] = make_double2(p[0], p[1]);
     }
 };
 
@@ -429,8 +421,8 @@ __global__ void __launch_bounds__(256) k_register_ll(RegisterArgs a)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real *sA = reinterpret_cast<Real *>(smem_raw);
     Real *sT = sA + a.t.nC * NE;
-    // per-pixel terms of the current tile, after the tables (their size is a multiple of 8 bytes)
-    double *s_term = reinterpret_cast<double *>(sA + (1 + TableLayout<Real>::kTParts) * a.t.nC * NE);
+    // the tile's point slots, after the tables (48 or 96 bytes per cell: 16-byte aligned)
+    double2 *s_pos = reinterpret_cast<double2 *>(sA + (1 + TableLayout<Real>::kTParts) * a.t.nC * NE);
     __shared__ unsigned long long s_claim;
     const int tab = a.t.nC * NE;
     const Real h = (Real)(a.dt / (double)a.nStepsODE);
@@ -442,28 +434,40 @@ __global__ void __launch_bounds__(256) k_register_ll(RegisterArgs a)
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         if ((((tile - blockIdx.x) / gridDim.x) & 7) == 0 && cta_cancelled(a.cancel, a.counters)) break;
         const int inst = (int)(tile / tpi);
-        const int64_t k = tile - (int64_t)inst * tpi;
+        const int64_t kt = tile - (int64_t)inst * tpi;
         const int64_t base = (int64_t)inst * npx;
-        const int64_t start = base + k * a.tile_px;
-        const int64_t end = min(start + (int64_t)a.tile_px, base + npx);
+        const int64_t j0 = kt * a.tile_px;  // first pixel of the tile in its image
+        const int64_t start = base + j0;
+        const int n = (int)(min(start + (int64_t)a.tile_px, base + npx) - start);
         if (inst != loaded) {
             __syncthreads();
-            stage_tables<DIM, Real>(a.A + (size_t)inst * tab, a.T + (size_t)inst * tab, a.t.nC, true, sA, sT);
+            stage_tables<DIM, Real>(a.A + (size_t)inst * tab, a.T + (size_t)inst * tab, a.t.nC, true,
+                                    a.h_sub, sA, sT);
             loaded = inst;
-            __syncthreads();
         }
-        PixelSrc src{a.H, a.W, base};
-        SsdSnk snk{a.src + base, a.dst + base, a.warped ? a.warped + base : nullptr, a.H, a.W, base, start,
-                   -0.5 / (a.sigma * a.sigma), s_term};
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const int64_t q = j0 + j, r = q / a.W, c = q - r * a.W;
+            s_pos[j] = make_double2(((double)c + 0.5) / (double)a.W, ((double)r + 0.5) / (double)a.H);
+        }
         if (threadIdx.x == 0) s_claim = 0ull;
         __syncthreads();
         // all warps share the tile through the claim counter
-        integrate_range<DIM, TESS, Real, SCHEME_REF>(a.t, a.nTimeSteps, a.nStepsODE, sA, sT, start, end, h, src,
-                                                     snk, c_fast, c_fb, c_sub, c_pts, nullptr, 0, &s_claim);
+        const SlotSrc2 src{s_pos, start};
+        SlotSnk2 snk{s_pos, start};
+        integrate_range<DIM, TESS, Real, SCHEME_REF>(a.t, a.nTimeSteps, a.nStepsODE, sA, sT, start, start + n, h,
+                                                     src, snk, c_fast, c_fb, c_sub, c_pts, nullptr, 0, &s_claim);
         __syncthreads();
-        // fixed-order sum of the tile's terms: thread t takes slots t, t + blockDim, ...
+        const float *img = a.src + base, *ref = a.dst + base;
+        float *warped = a.warped ? a.warped + base : nullptr;
+        const double k = -0.5 / (a.sigma * a.sigma);
         double acc = 0.0;
-        for (int j = threadIdx.x; j < (int)(end - start); j += blockDim.x) acc += s_term[j];
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const double2 p = s_pos[j];
+            const Real w = bilinear<Real>(img, a.H, a.W, p.x * a.W - 0.5, p.y * a.H - 0.5);
+            if (warped) warped[j0 + j] = (float)w;
+            const double e = (double)w - (double)__ldg(ref + j0 + j);
+            acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(e, e), k));
+        }
         finish_tile(acc, tile, inst, (int)tpi, (int64_t)inst * tpi, a.partials, a.tickets, a.ll);
     }
     if (a.counters) {
@@ -480,11 +484,15 @@ __global__ void __launch_bounds__(256) k_register_ll(RegisterArgs a)
     }
 }
 
+size_t register_smem_bytes(int nC, int tile_px, int prec)
+{
+    return (size_t)nC * 6 * (prec == PREC_F64 ? 2 * 8 : 2 * 4) + (size_t)tile_px * sizeof(double2);
+}
+
 template <int TESS, typename Real>
 static cudaError_t launch_register_t(const RegisterArgs &a, const LaunchCfg &cfg, cudaStream_t s)
 {
-    size_t smem = (size_t)(1 + TableLayout<Real>::kTParts) * a.t.nC * 6 * sizeof(Real) +
-                  (size_t)a.tile_px * sizeof(double);
+    const size_t smem = register_smem_bytes(a.t.nC, a.tile_px, sizeof(Real) == 8 ? PREC_F64 : PREC_F32);
     auto kern = k_register_ll<TESS, Real>;
     if (smem > kSmemOptInAbove) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -37,10 +37,13 @@ struct RegisterArgs {
     int N, H, W, tile_px;
     double sigma, dt;
     int nTimeSteps, nStepsODE;
+    double h_sub;             // dt / nStepsODE, set on the host
     const volatile int *cancel;  // the context's cancel flag (device memory), polled between tiles, or nullptr
 };
 
 cudaError_t launch_remap_ssd(const RemapArgs &a, int map_prec, cudaStream_t s);
+// Dynamic shared memory of k_register_ll: the tables and one double2 point slot per tile pixel.
+size_t register_smem_bytes(int nC, int tile_px, int prec);
 cudaError_t launch_register_ll(const RegisterArgs &a, int prec, const LaunchCfg &cfg, cudaStream_t s);
 
 }  // namespace cpab

@@ -136,43 +136,38 @@ __global__ void __launch_bounds__(256) k_remap3d_ssd(Remap3dArgs a)
     }
 }
 
-// Start points: voxel centres of the unit cube, index j = (r * W + c) * D + k.
-struct VoxelSrc {
-    int H, W, D;
-    int64_t base;
+// Start and end points of the current tile's voxels live in shared memory,
+// three doubles per voxel: a convergent pass writes the voxel centres
+// ((col+0.5)/W, (row+0.5)/H, (dep+0.5)/D) of voxels j = (row * W + col) * D
+// + dep, the lane loop takes a point's start from its slot and writes its
+// end point back, and a second convergent pass samples src there, compares
+// with dst and sums the terms in a fixed order (thread t: voxels t,
+// t + blockDim, ...).  Index arithmetic and sampling stay out of the lane
+// loop, whose register count sets the CTAs per SM.
+struct SlotSrc3 {
+    const double *slot;
+    int64_t tile_start;
     template <typename Real>
     __device__ __forceinline__ void load(int64_t i, PState<3, Real> &st) const
     {
-        const int64_t j = i - base;
-        const int64_t rc = j / D, k = j - rc * D;
-        const int64_t r = rc / W, c = rc - r * W;
-        double p[3];
-        p[0] = ((double)c + 0.5) / (double)W;
-        p[1] = ((double)r + 0.5) / (double)H;
-        p[2] = ((double)k + 0.5) / (double)D;
+        const double *v = slot + 3 * (i - tile_start);
+        const double p[3] = {v[0], v[1], v[2]};
         st.set(p);
     }
 };
 
-// End points: sampled from src, compared with dst, the term into the tile's
-// shared-memory slot (summed in a fixed order by the CTA).
-struct Ssd3Snk {
-    const float *src, *dst;
-    float *warped;
-    int H, W, D;
-    int64_t base, tile_start;
-    double k;
-    double *term;
+struct SlotSnk3 {
+    double *slot;
+    int64_t tile_start;
     template <typename Real>
     __device__ __forceinline__ void put(int64_t i, const PState<3, Real> &st)
     {
-        const int64_t j = i - base;
         double p[3];
         st.get(p);
-        const Real w = trilinear<Real>(src, H, W, D, p[0] * W - 0.5, p[1] * H - 0.5, p[2] * D - 0.5);
-        if (warped) warped[j] = (float)w;
-        const double e = (double)w - (double)__ldg(dst + j);
-        term[i - tile_start] = e * e * k;
+        double *v = slot + 3 * (i - tile_start);
+        v[0] = p[0];
+        v[1] = p[1];
+        v[2] = p[2];
     }
 };
 
@@ -183,7 +178,7 @@ __global__ void __launch_bounds__(256) k_register3d_ll(Register3dArgs a)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real *sA = reinterpret_cast<Real *>(smem_raw);
     Real *sT = sA + a.t.nC * NE;
-    double *s_term = reinterpret_cast<double *>(sA + (1 + TableLayout<Real>::kTParts) * a.t.nC * NE);
+    double *s_pos = reinterpret_cast<double *>(sA + (1 + TableLayout<Real>::kTParts) * a.t.nC * NE);
     __shared__ unsigned long long s_claim;
     const int tab = a.t.nC * NE;
     const Real h = (Real)(a.dt / (double)a.nStepsODE);
@@ -197,23 +192,41 @@ __global__ void __launch_bounds__(256) k_register3d_ll(Register3dArgs a)
         const int inst = (int)(tile / tpi);
         const int64_t kt = tile - (int64_t)inst * tpi;
         const int64_t base = (int64_t)inst * nvx;
-        const int64_t start = base + kt * a.tile_px;
-        const int64_t end = min(start + (int64_t)a.tile_px, base + nvx);
+        const int64_t j0 = kt * a.tile_px;  // first voxel of the tile in its volume
+        const int64_t start = base + j0;
+        const int n = (int)(min(start + (int64_t)a.tile_px, base + nvx) - start);
         if (inst != loaded) {
             __syncthreads();
-            stage_tables<DIM, Real>(a.A + (size_t)inst * tab, a.T + (size_t)inst * tab, a.t.nC, true, sA, sT);
+            stage_tables<DIM, Real>(a.A + (size_t)inst * tab, a.T + (size_t)inst * tab, a.t.nC, true,
+                                    a.h_sub, sA, sT);
             loaded = inst;
         }
-        VoxelSrc src{a.H, a.W, a.D, base};
-        Ssd3Snk snk{a.src + base, a.dst + base, a.warped ? a.warped + base : nullptr, a.H, a.W, a.D, base, start,
-                    -0.5 / (a.sigma * a.sigma), s_term};
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const int64_t q = j0 + j, rc = q / a.D, dep = q - rc * a.D;
+            const int64_t r = rc / a.W, c = rc - r * a.W;
+            double *v = s_pos + 3 * j;
+            v[0] = ((double)c + 0.5) / (double)a.W;
+            v[1] = ((double)r + 0.5) / (double)a.H;
+            v[2] = ((double)dep + 0.5) / (double)a.D;
+        }
         if (threadIdx.x == 0) s_claim = 0ull;
         __syncthreads();
-        integrate_range<DIM, TESS, Real, SCHEME_REF>(a.t, a.nTimeSteps, a.nStepsODE, sA, sT, start, end, h, src,
-                                                     snk, c_fast, c_fb, c_sub, c_pts, nullptr, 0, &s_claim);
+        const SlotSrc3 src{s_pos, start};
+        SlotSnk3 snk{s_pos, start};
+        integrate_range<DIM, TESS, Real, SCHEME_REF>(a.t, a.nTimeSteps, a.nStepsODE, sA, sT, start, start + n, h,
+                                                     src, snk, c_fast, c_fb, c_sub, c_pts, nullptr, 0, &s_claim);
         __syncthreads();
+        const float *img = a.src + base, *ref = a.dst + base;
+        float *warped = a.warped ? a.warped + base : nullptr;
+        const double k = -0.5 / (a.sigma * a.sigma);
         double acc = 0.0;
-        for (int j = threadIdx.x; j < (int)(end - start); j += blockDim.x) acc += s_term[j];
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const double *v = s_pos + 3 * j;
+            const Real w = trilinear<Real>(img, a.H, a.W, a.D, v[0] * a.W - 0.5, v[1] * a.H - 0.5, v[2] * a.D - 0.5);
+            if (warped) warped[j0 + j] = (float)w;
+            const double e = (double)w - (double)__ldg(ref + j0 + j);
+            acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(e, e), k));
+        }
         finish_tile(acc, tile, inst, (int)tpi, (int64_t)inst * tpi, a.partials, a.tickets, a.ll);
     }
     if (a.counters) {
@@ -252,7 +265,7 @@ cudaError_t launch_register3d_t(const Register3dArgs &a, const LaunchCfg &cfg, c
 size_t register3d_smem_bytes(int nC, int tile_px, int prec)
 {
     const size_t tables = prec == PREC_F64 ? (size_t)nC * 12 * 2 * 8 : (size_t)nC * 12 * 2 * 4;
-    return tables + (size_t)tile_px * sizeof(double);
+    return tables + (size_t)tile_px * 3 * sizeof(double);  // three doubles per voxel slot
 }
 
 cudaError_t launch_remap3d_ssd(const Remap3dArgs &a, int map_prec, cudaStream_t s)

@@ -37,6 +37,7 @@ struct Register3dArgs {
     int N, H, W, D, tile_px;
     double sigma, dt;
     int nTimeSteps, nStepsODE;
+    double h_sub;             // dt / nStepsODE, set on the host
     const volatile int *cancel;
 };
 
