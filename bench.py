@@ -399,21 +399,28 @@ def other_configs(torch, dev) -> dict:
     x3 = torch.as_tensor(np.tile(grid, (8, 1)), device=dev)
     with torch.no_grad():
         y3 = transform(torch.as_tensor(pr3.sample(8, rng), device=dev), x3, sp3, **p)
-    t = th3.clone().requires_grad_(True)
-    for _ in range(2):
+
+    def fwd_adjoint_ms(scheme):
+        t = th3.clone().requires_grad_(True)
+        for _ in range(2):
+            t.grad = None
+            (0.5 * ((transform(t, x3, sp3, scheme=scheme, **p) - y3) ** 2).sum()).backward()
+        a, b = ev(), ev()
+        a.record()
         t.grad = None
-        (0.5 * ((transform(t, x3, sp3, **p) - y3) ** 2).sum()).backward()
-    a, b = ev(), ev()
-    a.record()
-    t.grad = None
-    (0.5 * ((transform(t, x3, sp3, **p) - y3) ** 2).sum()).backward()
-    b.record()
-    b.synchronize()
+        (0.5 * ((transform(t, x3, sp3, scheme=scheme, **p) - y3) ** 2).sum()).backward()
+        b.record()
+        b.synchronize()
+        return a.elapsed_time(b)
+
     n3 = x3.shape[0]
+    ms_ref, ms_simple = fwd_adjoint_ms("ref"), fwd_adjoint_ms("simple")
     out["c2_3d_fwd_adjoint_f64"] = {"theta": 8, "points_per_theta": 64 ** 3, "d": sp3.d,
-                                    "ms_fwd_plus_adjoint": a.elapsed_time(b),
-                                    "points_per_s": n3 / (a.elapsed_time(b) * 1e-3),
-                                    "scheme": "midpoint (calc_T_simple) forward, discrete adjoint"}
+                                    "ms_fwd_plus_adjoint": ms_ref,
+                                    "points_per_s": n3 / (ms_ref * 1e-3),
+                                    "scheme": "calc_T (closed-form steps + sub-step fallback) forward, adjoint along "
+                                              "the forward's branches, expm Frechet adjoint per cell",
+                                    "midpoint_scheme_ms_fwd_plus_adjoint": ms_simple}
 
     # batched MCMC registration: 256 chains x 256^2, FP32, steps captured in a CUDA graph
     sp2 = CpaSpace([0, 0], [1, 1], (4, 4), tess="I", device=dev, precision=torch.float32)

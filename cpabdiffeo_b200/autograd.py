@@ -4,10 +4,16 @@ kernel (cpab_grad_theta).
     y = transform(theta, pts, space, dt=..., nTimeSteps=..., nStepsODEsolver=...)
     loss = 0.5 * ((y - target) ** 2).sum();  loss.backward()   # theta.grad
 
-The forward is the midpoint scheme (calc_T_simple); the backward re-runs it
-with checkpoints every `ck` time steps and propagates dLoss/dT(x) through
-every sub-step (the exact gradient of the discrete map).  theta is [N, d]
-(N transforms), pts [N*n, dim] float64 (n points per transform).
+scheme="ref" (default): the forward is calc_T, the reference scheme
+(closed-form steps T = expm(dt A), nStepsODE midpoint sub-steps where a step
+leaves its cell); the backward (cpab_grad_theta_ref) re-runs it with
+checkpoints every `ck` time steps and propagates dLoss/dT(x) back through
+every step along the branch the forward took, mapping the per-cell
+dLoss/dT to dLoss/dA through the adjoint Frechet derivative of expm.
+scheme="simple": the forward is calc_T_simple (nTimeSteps * nStepsODE
+midpoint sub-steps) and the backward (cpab_grad_theta) goes through every
+sub-step.  Either is the exact gradient of the discrete map.  theta is
+[N, d] (N transforms), pts [N*n, dim] float64 (n points per transform).
 """
 from __future__ import annotations
 
@@ -35,23 +41,23 @@ def checkpoint_stride(space: CpaSpace, N: int, n: int, nT: int, budget_bytes: in
 
 class _Transform(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, theta, pts, space, sign, dt, nT, nODE, ck, need_pts_grad):
+    def forward(ctx, theta, pts, space, sign, dt, nT, nODE, ck, need_pts_grad, ref):
         N = theta.shape[0]
         n = pts.shape[0] // N
         sA, Tr = space.tables_from_theta(theta.detach(), dt, sign)
         out = torch.empty_like(pts)
         c = space._ctx
         c.check(c.lib.cpab_calc_T_batched(c.h, _lib.ptr(sA), _lib.ptr(Tr), _lib.ptr(pts), _lib.ptr(out), N, None, n,
-                                          None, 0, _lib.CPAB_F64, _lib.SCHEME_SIMPLE, dt, nT, nODE, None,
-                                          _lib.stream_ptr()))
-        ctx.save_for_backward(pts, sA)
+                                          None, 0, _lib.CPAB_F64, _lib.SCHEME_REF if ref else _lib.SCHEME_SIMPLE,
+                                          dt, nT, nODE, None, _lib.stream_ptr()))
+        ctx.save_for_backward(pts, sA, Tr)
         ctx.space, ctx.sign, ctx.dt, ctx.nT, ctx.nODE, ctx.ck = space, sign, dt, nT, nODE, ck
-        ctx.need_pts_grad = need_pts_grad
+        ctx.need_pts_grad, ctx.ref = need_pts_grad, ref
         return out
 
     @staticmethod
     def backward(ctx, grad_out):
-        pts, sA = ctx.saved_tensors
+        pts, sA, Tr = ctx.saved_tensors
         sp: CpaSpace = ctx.space
         N = sA.shape[0]
         n = pts.shape[0] // N
@@ -60,17 +66,29 @@ class _Transform(torch.autograd.Function):
         gA = torch.empty((N, sp.D), dtype=torch.float64, device=pts.device)
         gpts = torch.empty_like(pts) if ctx.need_pts_grad else None
         c = sp._ctx
-        wsb = int(c.lib.cpab_grad_workspace_bytes(c.h, N, n, ctx.nT, ctx.ck))
-        ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=pts.device)
-        c.check(c.lib.cpab_grad_theta(c.h, _lib.ptr(sp.B), sp.d, _lib.ptr(sA), N, _lib.ptr(pts), n, _lib.ptr(g),
-                                      ctx.dt, ctx.nT, ctx.nODE, ctx.sign, ctx.ck, None, _lib.ptr(gpts), _lib.ptr(gA),
-                                      _lib.ptr(dtheta), _lib.ptr(ws), ws.numel(), _lib.stream_ptr()))
-        return dtheta, gpts, None, None, None, None, None, None, None
+        if ctx.ref:
+            wsb = int(c.lib.cpab_grad_ref_workspace_bytes(c.h, N, n, ctx.nT, ctx.ck))
+            ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=pts.device)
+            c.check(c.lib.cpab_grad_theta_ref(c.h, _lib.ptr(sp.B), sp.d, _lib.ptr(sA), _lib.ptr(Tr), N, _lib.ptr(pts),
+                                              n, _lib.ptr(g), ctx.dt, ctx.nT, ctx.nODE, ctx.sign, ctx.ck, None,
+                                              _lib.ptr(gpts), _lib.ptr(gA), _lib.ptr(dtheta), _lib.ptr(ws),
+                                              ws.numel(), _lib.stream_ptr()))
+        else:
+            wsb = int(c.lib.cpab_grad_workspace_bytes(c.h, N, n, ctx.nT, ctx.ck))
+            ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=pts.device)
+            c.check(c.lib.cpab_grad_theta(c.h, _lib.ptr(sp.B), sp.d, _lib.ptr(sA), N, _lib.ptr(pts), n, _lib.ptr(g),
+                                          ctx.dt, ctx.nT, ctx.nODE, ctx.sign, ctx.ck, None, _lib.ptr(gpts),
+                                          _lib.ptr(gA), _lib.ptr(dtheta), _lib.ptr(ws), ws.numel(),
+                                          _lib.stream_ptr()))
+        return dtheta, gpts, None, None, None, None, None, None, None, None
 
 
 def transform(theta: torch.Tensor, pts: torch.Tensor, space: CpaSpace, mysign: int = 1, ck: int | None = None,
-              memory_budget_bytes: int = 8 << 30, **params_flow_int) -> torch.Tensor:
-    """T_theta(pts) (or T^-1 with mysign=-1) through the midpoint scheme, differentiable in theta and pts."""
+              memory_budget_bytes: int = 8 << 30, scheme: str = "ref", **params_flow_int) -> torch.Tensor:
+    """T_theta(pts) (or T^-1 with mysign=-1), differentiable in theta and pts, through the reference
+    scheme (calc_T, scheme="ref") or the midpoint scheme (calc_T_simple, scheme="simple")."""
+    if scheme not in ("ref", "simple"):
+        raise ValueError('scheme must be "ref" or "simple"')
     dt, nT, nODE = _flow(space, params_flow_int)
     theta = theta.reshape(-1, space.d)
     if theta.dtype != torch.float64 or pts.dtype != torch.float64:
@@ -81,4 +99,4 @@ def transform(theta: torch.Tensor, pts: torch.Tensor, space: CpaSpace, mysign: i
     if ck is None:
         ck = checkpoint_stride(space, N, pts.shape[0] // N, nT, memory_budget_bytes)
     return _Transform.apply(theta, pts.contiguous(), space, int(mysign), dt, nT, nODE, int(ck),
-                            bool(pts.requires_grad))
+                            bool(pts.requires_grad), scheme == "ref")

@@ -558,16 +558,28 @@ size_t cpab_grad_workspace_bytes(const cpab_ctx *ctx, int N, int64_t n_per_inst,
     return align256((size_t)nck * (size_t)N * (size_t)n_per_inst * ctx->t.dim * sizeof(double));
 }
 
-int cpab_grad_theta(cpab_ctx *ctx, const double *B, int d, const double *signedA, int N, const double *pts,
-                    int64_t n_per_inst, const double *grad_out, double dt, int nTimeSteps, int nStepsODE, int sign,
-                    int ck, double *out, double *grad_pts, double *gA, double *dtheta, void *workspace,
-                    size_t workspace_bytes, void *stream)
+size_t cpab_grad_ref_workspace_bytes(const cpab_ctx *ctx, int N, int64_t n_per_inst, int nTimeSteps, int ck)
+{
+    if (!ctx || N < 0 || n_per_inst < 0 || nTimeSteps < 1 || ck < 1) return 0;
+    return cpab_grad_workspace_bytes(ctx, N, n_per_inst, nTimeSteps, ck) +
+           align256((size_t)N * ctx->t.nC * cell_len(ctx) * sizeof(double));
+}
+
+}  // extern "C"
+
+// Shared body of cpab_grad_theta (ref == false: midpoint scheme) and
+// cpab_grad_theta_ref (reference scheme, needs Trels).
+static int grad_impl(cpab_ctx *ctx, const double *B, int d, const double *signedA, const double *Trels, bool ref,
+                     int N, const double *pts, int64_t n_per_inst, const double *grad_out, double dt, int nTimeSteps,
+                     int nStepsODE, int sign, int ck, double *out, double *grad_pts, double *gA, double *dtheta,
+                     void *workspace, size_t workspace_bytes, void *stream)
 {
     if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
     if (N < 0 || n_per_inst < 0) return fail(ctx, CPAB_BAD_SHAPE, "N and n_per_inst must be >= 0");
     if (N > 65535) return fail(ctx, CPAB_BAD_SHAPE, "at most 65535 instances per call (got %d)", N);
     if (N == 0) return CPAB_OK;
     if (!signedA || !gA) return fail(ctx, CPAB_BAD_ARG, "signedA/gA is NULL");
+    if (ref && !Trels) return fail(ctx, CPAB_BAD_ARG, "Trels is NULL");
     if (dtheta && (!B || d < 1)) return fail(ctx, CPAB_BAD_ARG, "dtheta needs the basis B and d >= 1");
     if (n_per_inst > 0 && (!pts || !grad_out)) return fail(ctx, CPAB_BAD_ARG, "pts/grad_out is NULL");
     if (nTimeSteps < 1 || nStepsODE < 1) return fail(ctx, CPAB_BAD_ARG, "nTimeSteps and nStepsODE must be >= 1");
@@ -575,12 +587,14 @@ int cpab_grad_theta(cpab_ctx *ctx, const double *B, int d, const double *signedA
     if (ck < 1) return fail(ctx, CPAB_BAD_ARG, "checkpoint stride must be >= 1");
     if (sign != 1 && sign != -1) return fail(ctx, CPAB_BAD_ARG, "sign must be +1 or -1");
     if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
-    CPAB_CHECK_ALIGN(ctx, {B, 8, "B"}, {signedA, 8, "signedA"}, {pts, 8, "pts"}, {grad_out, 8, "grad_out"},
-                     {out, 8, "out"}, {grad_pts, 8, "grad_pts"}, {gA, 8, "gA"}, {dtheta, 8, "dtheta"},
-                     {workspace, 8, "workspace"});
-    if ((size_t)2 * ctx->t.nC * cell_len(ctx) * 8 > (size_t)max_smem_optin())
+    CPAB_CHECK_ALIGN(ctx, {B, 8, "B"}, {signedA, 8, "signedA"}, {Trels, 8, "Trels"}, {pts, 8, "pts"},
+                     {grad_out, 8, "grad_out"}, {out, 8, "out"}, {grad_pts, 8, "grad_pts"}, {gA, 8, "gA"},
+                     {dtheta, 8, "dtheta"}, {workspace, 8, "workspace"});
+    // tables (reference scheme: also the closed-form steps and both gradient sums) in shared memory
+    if ((size_t)(ref ? 4 : 2) * ctx->t.nC * cell_len(ctx) * 8 > (size_t)max_smem_optin())
         return fail(ctx, CPAB_UNSUPPORTED, "cell tables exceed shared memory");
-    const size_t need = cpab_grad_workspace_bytes(ctx, N, n_per_inst, nTimeSteps, ck);
+    const size_t ck_bytes = cpab_grad_workspace_bytes(ctx, N, n_per_inst, nTimeSteps, ck);
+    const size_t need = ref ? cpab_grad_ref_workspace_bytes(ctx, N, n_per_inst, nTimeSteps, ck) : ck_bytes;
     if (n_per_inst > 0 && (!workspace || workspace_bytes < need))
         return fail(ctx, CPAB_NO_MEMORY, "workspace of %zu bytes needed", need);
     cudaStream_t s = (cudaStream_t)stream;
@@ -592,6 +606,7 @@ int cpab_grad_theta(cpab_ctx *ctx, const double *B, int d, const double *signedA
         memset(&a, 0, sizeof(a));
         a.t = ctx->t;
         a.A = signedA;
+        a.T = Trels;
         a.pts = pts;
         a.grad_out = grad_out;
         a.out = out;
@@ -604,7 +619,14 @@ int cpab_grad_theta(cpab_ctx *ctx, const double *B, int d, const double *signedA
         a.nTimeSteps = nTimeSteps;
         a.nStepsODE = nStepsODE;
         a.ck = ck;
-        e = launch_grad_simple(a, s);
+        if (ref) {
+            a.gT = reinterpret_cast<double *>(static_cast<char *>(workspace) + ck_bytes);
+            e = cudaMemsetAsync(a.gT, 0, (size_t)N * DA * sizeof(double), s);
+            if (e != cudaSuccess) return cuda_status(ctx, e, "gT reset");
+            e = launch_grad_ref(a, s);
+        } else {
+            e = launch_grad_simple(a, s);
+        }
         if (e != cudaSuccess) return cuda_status(ctx, e, "grad launch");
     }
     if (dtheta) {
@@ -612,6 +634,26 @@ int cpab_grad_theta(cpab_ctx *ctx, const double *B, int d, const double *signedA
         if (e != cudaSuccess) return cuda_status(ctx, e, "B^T launch");
     }
     return CPAB_OK;
+}
+
+extern "C" {
+
+int cpab_grad_theta(cpab_ctx *ctx, const double *B, int d, const double *signedA, int N, const double *pts,
+                    int64_t n_per_inst, const double *grad_out, double dt, int nTimeSteps, int nStepsODE, int sign,
+                    int ck, double *out, double *grad_pts, double *gA, double *dtheta, void *workspace,
+                    size_t workspace_bytes, void *stream)
+{
+    return grad_impl(ctx, B, d, signedA, nullptr, false, N, pts, n_per_inst, grad_out, dt, nTimeSteps, nStepsODE,
+                     sign, ck, out, grad_pts, gA, dtheta, workspace, workspace_bytes, stream);
+}
+
+int cpab_grad_theta_ref(cpab_ctx *ctx, const double *B, int d, const double *signedA, const double *Trels, int N,
+                        const double *pts, int64_t n_per_inst, const double *grad_out, double dt, int nTimeSteps,
+                        int nStepsODE, int sign, int ck, double *out, double *grad_pts, double *gA, double *dtheta,
+                        void *workspace, size_t workspace_bytes, void *stream)
+{
+    return grad_impl(ctx, B, d, signedA, Trels, true, N, pts, n_per_inst, grad_out, dt, nTimeSteps, nStepsODE, sign,
+                     ck, out, grad_pts, gA, dtheta, workspace, workspace_bytes, stream);
 }
 
 }  // extern "C"

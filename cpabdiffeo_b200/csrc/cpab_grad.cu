@@ -18,6 +18,19 @@
 // recomputed from the previous checkpoint (ck = 1 stores all, ck = nT only
 // the input).  Inside a time step the sub-steps are replayed in groups of
 // kGroup from kGroup start points held in a small per-thread buffer.
+//
+// k_grad_ref: the same for the reference scheme (calc_T, calc_2Dto2D.cu:
+// 348-408): a time step is either the closed-form step q = T_c [p; 1] with
+// T_c = expm(dt A_c), kept when q stays in cell c, or nStepsODE sub-steps as
+// above.  Backwards through a kept step
+//     dT_c += g [p; 1]^T,   g = T_lin^T g,
+// and through a fallback step the sub-step adjoint.  The per-cell sums dT_c
+// become dLoss/dA_c once per instance and cell (k_frechet_adjoint):
+//     dA_c += dt L(X^T, dT_c),  X = dt [A_c; 0],
+// L the Frechet derivative of expm, read off the top-right block of
+// expm([[X^T, G], [0, X^T]]).  This is the exact gradient of the discrete
+// map along the branch the forward took (kept / fallback, cells); where a
+// step changes branch the map itself is discontinuous.
 #include "cpab_integrate.cuh"
 #include "cpab_grad.h"
 #include "cpab_launch.h"
@@ -36,10 +49,97 @@ __device__ __forceinline__ void substeps(const Tess &t, const double *sA, double
     }
 }
 
+// Per-thread accumulator of one cell's dLoss/d(matrix) entries, added to the
+// CTA's shared sums when the cell changes (c = -1: flush).
+template <int NE>
+__device__ __forceinline__ void acc_switch(double *sG, double *acc, int &acc_cell, int c)
+{
+    if (c == acc_cell) return;
+    if (acc_cell >= 0) {
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
+            atomicAdd(sG + acc_cell * NE + e, acc[e]);
+            acc[e] = 0.0;
+        }
+    }
+    acc_cell = c;
+}
+
+// Backwards through the nODE sub-steps of one time step that starts at q
+// (q is consumed): g = dLoss/d(end of the step) on entry, dLoss/d(start) on
+// return; dLoss/dA of the cells used is accumulated (acc / acc_cell / sG).
+template <int DIM, int TESS>
+__device__ __forceinline__ void adjoint_substeps(const Tess &t, const double *sA, double *sG, double *q, double *g,
+                                                 double h, int nODE, double *acc, int &acc_cell)
+{
+    constexpr int NE = DIM * (DIM + 1), NH = DIM + 1;
+    const int ngroups = (nODE + kGroup - 1) / kGroup;
+    double buf1[kGroup][DIM], buf2[kGroup][DIM];
+    // group starts
+    for (int k = 0; k < nODE; ++k) {
+        if (k % kGroup == 0) {
+#pragma unroll
+            for (int i = 0; i < DIM; ++i) buf1[k / kGroup][i] = q[i];
+        }
+        int c = exact_cell<DIM, TESS>(t, q);
+        exact_midpoint<DIM>(q, sA + c * NE, h);
+    }
+    for (int gr = ngroups - 1; gr >= 0; --gr) {
+        const int k0 = gr * kGroup, k1 = min(nODE, k0 + kGroup);
+        double r[DIM];
+#pragma unroll
+        for (int i = 0; i < DIM; ++i) r[i] = buf1[gr][i];
+        for (int k = k0; k < k1; ++k) {
+#pragma unroll
+            for (int i = 0; i < DIM; ++i) buf2[k - k0][i] = r[i];
+            int c = exact_cell<DIM, TESS>(t, r);
+            exact_midpoint<DIM>(r, sA + c * NE, h);
+        }
+        for (int k = k1 - 1; k >= k0; --k) {
+            double pk[DIM];
+#pragma unroll
+            for (int i = 0; i < DIM; ++i) pk[i] = buf2[k - k0][i];
+            const int c = exact_cell<DIM, TESS>(t, pk);
+            const double *M = sA + c * NE;
+            acc_switch<NE>(sG, acc, acc_cell, c);
+            // recompute v and pm of the forward sub-step
+            double v[DIM], pm[DIM];
+            exact_affine<DIM>(v, M, pk);
+#pragma unroll
+            for (int i = 0; i < DIM; ++i) pm[i] = pk[i] + h * v[i] / 2.;
+            double av[DIM], dpm[DIM], b[DIM];
+#pragma unroll
+            for (int i = 0; i < DIM; ++i) av[i] = h * g[i];
+#pragma unroll
+            for (int jj = 0; jj < DIM; ++jj) {
+                double s2 = 0.0;
+#pragma unroll
+                for (int i = 0; i < DIM; ++i) s2 += M[i * NH + jj] * av[i];
+                dpm[jj] = s2;
+            }
+#pragma unroll
+            for (int i = 0; i < DIM; ++i) b[i] = 0.5 * h * dpm[i];
+#pragma unroll
+            for (int i = 0; i < DIM; ++i) {
+#pragma unroll
+                for (int jj = 0; jj < DIM; ++jj) acc[i * NH + jj] += av[i] * pm[jj] + b[i] * pk[jj];
+                acc[i * NH + DIM] += av[i] + b[i];
+            }
+#pragma unroll
+            for (int jj = 0; jj < DIM; ++jj) {
+                double s2 = 0.0;
+#pragma unroll
+                for (int i = 0; i < DIM; ++i) s2 += M[i * NH + jj] * b[i];
+                g[jj] += dpm[jj] + s2;
+            }
+        }
+    }
+}
+
 template <int DIM, int TESS>
 __global__ void __launch_bounds__(128) k_grad_simple(GradArgs a)
 {
-    constexpr int NE = DIM * (DIM + 1), NH = DIM + 1;
+    constexpr int NE = DIM * (DIM + 1);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *sA = reinterpret_cast<double *>(smem_raw);
     double *sG = sA + a.t.nC * NE;
@@ -52,7 +152,6 @@ __global__ void __launch_bounds__(128) k_grad_simple(GradArgs a)
     __syncthreads();
     const double h = XDIV(a.dt, (double)a.nStepsODE);
     const int nT = a.nTimeSteps, nODE = a.nStepsODE, ck = a.ck;
-    const int ngroups = (nODE + kGroup - 1) / kGroup;
     const int64_t n = a.n_per_inst;
     const int64_t total = n * a.N;
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
@@ -71,91 +170,202 @@ __global__ void __launch_bounds__(128) k_grad_simple(GradArgs a)
 #pragma unroll
         for (int e = 0; e < NE; ++e) acc[e] = 0.0;
         int acc_cell = -1;
-        double buf1[kGroup][DIM], buf2[kGroup][DIM];
         for (int s = nT - 1; s >= 0; --s) {
             // start of time step s
             double q[DIM];
             load_pt<DIM, double>(a.ckpt, (int64_t)(s / ck) * total + gi, q);
             substeps<DIM, TESS>(a.t, sA, q, h, s % ck * nODE);
-            // group starts
-            for (int k = 0; k < nODE; ++k) {
-                if (k % kGroup == 0) {
-#pragma unroll
-                    for (int i = 0; i < DIM; ++i) buf1[k / kGroup][i] = q[i];
-                }
-                int c = exact_cell<DIM, TESS>(a.t, q);
-                exact_midpoint<DIM>(q, sA + c * NE, h);
-            }
-            for (int gr = ngroups - 1; gr >= 0; --gr) {
-                const int k0 = gr * kGroup, k1 = min(nODE, k0 + kGroup);
-                double r[DIM];
-#pragma unroll
-                for (int i = 0; i < DIM; ++i) r[i] = buf1[gr][i];
-                for (int k = k0; k < k1; ++k) {
-#pragma unroll
-                    for (int i = 0; i < DIM; ++i) buf2[k - k0][i] = r[i];
-                    int c = exact_cell<DIM, TESS>(a.t, r);
-                    exact_midpoint<DIM>(r, sA + c * NE, h);
-                }
-                for (int k = k1 - 1; k >= k0; --k) {
-                    double pk[DIM];
-#pragma unroll
-                    for (int i = 0; i < DIM; ++i) pk[i] = buf2[k - k0][i];
-                    const int c = exact_cell<DIM, TESS>(a.t, pk);
-                    const double *M = sA + c * NE;
-                    if (c != acc_cell) {
-                        if (acc_cell >= 0) {
-#pragma unroll
-                            for (int e = 0; e < NE; ++e) {
-                                atomicAdd(sG + acc_cell * NE + e, acc[e]);
-                                acc[e] = 0.0;
-                            }
-                        }
-                        acc_cell = c;
-                    }
-                    // recompute v and pm of the forward sub-step
-                    double v[DIM], pm[DIM];
-                    exact_affine<DIM>(v, M, pk);
-#pragma unroll
-                    for (int i = 0; i < DIM; ++i) pm[i] = pk[i] + h * v[i] / 2.;
-                    double av[DIM], dpm[DIM], b[DIM];
-#pragma unroll
-                    for (int i = 0; i < DIM; ++i) av[i] = h * g[i];
-#pragma unroll
-                    for (int jj = 0; jj < DIM; ++jj) {
-                        double s2 = 0.0;
-#pragma unroll
-                        for (int i = 0; i < DIM; ++i) s2 += M[i * NH + jj] * av[i];
-                        dpm[jj] = s2;
-                    }
-#pragma unroll
-                    for (int i = 0; i < DIM; ++i) b[i] = 0.5 * h * dpm[i];
-#pragma unroll
-                    for (int i = 0; i < DIM; ++i) {
-#pragma unroll
-                        for (int jj = 0; jj < DIM; ++jj) acc[i * NH + jj] += av[i] * pm[jj] + b[i] * pk[jj];
-                        acc[i * NH + DIM] += av[i] + b[i];
-                    }
-#pragma unroll
-                    for (int jj = 0; jj < DIM; ++jj) {
-                        double s2 = 0.0;
-#pragma unroll
-                        for (int i = 0; i < DIM; ++i) s2 += M[i * NH + jj] * b[i];
-                        g[jj] += dpm[jj] + s2;
-                    }
-                }
-            }
+            adjoint_substeps<DIM, TESS>(a.t, sA, sG, q, g, h, nODE, acc, acc_cell);
         }
-        if (acc_cell >= 0) {
-#pragma unroll
-            for (int e = 0; e < NE; ++e) atomicAdd(sG + acc_cell * NE + e, acc[e]);
-        }
+        acc_switch<NE>(sG, acc, acc_cell, -1);
         if (a.grad_in) store_pt<DIM, double>(a.grad_in, gi, g);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < tab; i += blockDim.x) {
         double v = sG[i];
         if (v != 0.0) atomicAdd(a.gA + (size_t)inst * tab + i, v);
+    }
+}
+
+// One time step of the reference scheme from p (calc_T, the FP64 arithmetic
+// of k_integrate): the closed-form step when its end point stays in the
+// cell, else nODE sub-steps.  Returns whether the closed-form step was kept.
+template <int DIM, int TESS>
+__device__ __forceinline__ bool ref_step(const Tess &t, const double *sA, const double *sT, double *p, double h,
+                                         int nODE)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    const int c = exact_cell<DIM, TESS>(t, p);
+    double q[DIM];
+    exact_affine<DIM>(q, sT + c * NE, p);
+    if (exact_cell<DIM, TESS>(t, q) == c) {
+#pragma unroll
+        for (int i = 0; i < DIM; ++i) p[i] = q[i];
+        return true;
+    }
+    substeps<DIM, TESS>(t, sA, p, h, nODE);
+    return false;
+}
+
+template <int DIM, int TESS>
+__global__ void __launch_bounds__(128) k_grad_ref(GradArgs a)
+{
+    constexpr int NE = DIM * (DIM + 1), NH = DIM + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tab = a.t.nC * NE;
+    double *sA = reinterpret_cast<double *>(smem_raw);
+    double *sT = sA + tab;
+    double *sGA = sT + tab;   // dLoss/dA from sub-steps
+    double *sGT = sGA + tab;  // dLoss/dT from closed-form steps
+    const int inst = blockIdx.y;
+    for (int i = threadIdx.x; i < tab; i += blockDim.x) {
+        sA[i] = a.A[(size_t)inst * tab + i];
+        sT[i] = a.T[(size_t)inst * tab + i];
+        sGA[i] = 0.0;
+        sGT[i] = 0.0;
+    }
+    __syncthreads();
+    const double h = XDIV(a.dt, (double)a.nStepsODE);
+    const int nT = a.nTimeSteps, nODE = a.nStepsODE, ck = a.ck;
+    const int64_t n = a.n_per_inst;
+    const int64_t total = n * a.N;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t gi = (int64_t)inst * n + j;
+        double p[DIM];
+        load_pt<DIM, double>(a.pts, gi, p);
+        for (int s = 0; s < nT; ++s) {
+            if (s % ck == 0) store_pt<DIM, double>(a.ckpt, (int64_t)(s / ck) * total + gi, p);
+            ref_step<DIM, TESS>(a.t, sA, sT, p, h, nODE);
+        }
+        if (a.out) store_pt<DIM, double>(a.out, gi, p);
+        double g[DIM];
+        load_pt<DIM, double>(a.grad_out, gi, g);
+        double accA[NE], accT[NE];
+#pragma unroll
+        for (int e = 0; e < NE; ++e) accA[e] = accT[e] = 0.0;
+        int cellA = -1, cellT = -1;
+        for (int s = nT - 1; s >= 0; --s) {
+            double q[DIM];
+            load_pt<DIM, double>(a.ckpt, (int64_t)(s / ck) * total + gi, q);
+            for (int r = 0; r < s % ck; ++r) ref_step<DIM, TESS>(a.t, sA, sT, q, h, nODE);
+            // time step s from q, along the forward's branch
+            const int c = exact_cell<DIM, TESS>(a.t, q);
+            const double *T = sT + c * NE;
+            double y[DIM];
+            exact_affine<DIM>(y, T, q);
+            if (exact_cell<DIM, TESS>(a.t, y) == c) {
+                acc_switch<NE>(sGT, accT, cellT, c);
+#pragma unroll
+                for (int i = 0; i < DIM; ++i) {
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) accT[i * NH + k] += g[i] * q[k];
+                    accT[i * NH + DIM] += g[i];
+                }
+                double gn[DIM];
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) {
+                    double s2 = 0.0;
+#pragma unroll
+                    for (int i = 0; i < DIM; ++i) s2 += T[i * NH + k] * g[i];
+                    gn[k] = s2;
+                }
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) g[k] = gn[k];
+            } else {
+                adjoint_substeps<DIM, TESS>(a.t, sA, sGA, q, g, h, nODE, accA, cellA);
+            }
+        }
+        acc_switch<NE>(sGA, accA, cellA, -1);
+        acc_switch<NE>(sGT, accT, cellT, -1);
+        if (a.grad_in) store_pt<DIM, double>(a.grad_in, gi, g);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < tab; i += blockDim.x) {
+        const double va = sGA[i], vt = sGT[i];
+        if (va != 0.0) atomicAdd(a.gA + (size_t)inst * tab + i, va);
+        if (vt != 0.0) atomicAdd(a.gT + (size_t)inst * tab + i, vt);
+    }
+}
+
+// E = expm(Z) for a small K x K matrix: scaling and squaring (Moler & Van
+// Loan, "Nineteen dubious ways to compute the exponential of a matrix",
+// method 3) with the degree-18 Taylor polynomial of Z / 2^s,
+// ||Z / 2^s||_1 <= 1/2 (truncation below 1e-22 relative).  Z is scaled in
+// place.
+template <int K>
+__device__ void expm_small(double (&Z)[K][K], double (&E)[K][K])
+{
+    double nrm = 0.0;
+    for (int j = 0; j < K; ++j) {
+        double cs = 0.0;
+        for (int i = 0; i < K; ++i) cs += fabs(Z[i][j]);
+        nrm = fmax(nrm, cs);
+    }
+    int sq = 0;
+    while (nrm > 0.5 && sq < 60) {
+        nrm *= 0.5;
+        ++sq;
+    }
+    const double sc = ldexp(1.0, -sq);
+    double Tm[K][K], W[K][K];
+    for (int i = 0; i < K; ++i)
+        for (int j = 0; j < K; ++j) {
+            Z[i][j] *= sc;
+            Tm[i][j] = E[i][j] = (i == j) ? 1.0 : 0.0;
+        }
+    for (int k = 1; k <= 18; ++k) {
+        const double inv = 1.0 / (double)k;
+        for (int i = 0; i < K; ++i)
+            for (int j = 0; j < K; ++j) {
+                double s2 = 0.0;
+                for (int m = 0; m < K; ++m) s2 += Tm[i][m] * Z[m][j];
+                W[i][j] = s2 * inv;
+            }
+        for (int i = 0; i < K; ++i)
+            for (int j = 0; j < K; ++j) {
+                Tm[i][j] = W[i][j];
+                E[i][j] += W[i][j];
+            }
+    }
+    for (int r = 0; r < sq; ++r) {
+        for (int i = 0; i < K; ++i)
+            for (int j = 0; j < K; ++j) {
+                double s2 = 0.0;
+                for (int m = 0; m < K; ++m) s2 += E[i][m] * E[m][j];
+                W[i][j] = s2;
+            }
+        for (int i = 0; i < K; ++i)
+            for (int j = 0; j < K; ++j) E[i][j] = W[i][j];
+    }
+}
+
+// gA[c] += dt L(X^T, G_c) for every (instance, cell) c, X = dt [A_c; 0]
+// (homogeneous, last row zero) and G_c = [gT_c; 0].  L is linear in G, so G
+// is scaled to max |entry| 1 before the exponential and the block scaled
+// back, which keeps the squaring count set by X.
+template <int DIM>
+__global__ void k_frechet_adjoint(const double *A, const double *gT, double *gA, int total, double dt)
+{
+    constexpr int M = DIM + 1, K = 2 * M, NE = DIM * M;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+        const double *a = A + (size_t)idx * NE;
+        const double *g = gT + (size_t)idx * NE;
+        double gs = 0.0;
+        for (int e = 0; e < NE; ++e) gs = fmax(gs, fabs(g[e]));
+        if (!(gs > 0.0)) continue;  // no closed-form step in this cell
+        double Z[K][K], E[K][K];
+        for (int i = 0; i < K; ++i)
+            for (int j = 0; j < K; ++j) Z[i][j] = 0.0;
+        for (int i = 0; i < DIM; ++i)
+            for (int j = 0; j < M; ++j) {
+                const double x = dt * a[i * M + j];  // X[i][j]
+                Z[j][i] = x;                         // X^T, top left
+                Z[M + j][M + i] = x;                 // X^T, bottom right
+                Z[i][M + j] = g[i * M + j] / gs;     // G, top right
+            }
+        expm_small<K>(Z, E);
+        for (int i = 0; i < DIM; ++i)
+            for (int j = 0; j < M; ++j) gA[(size_t)idx * NE + i * M + j] += dt * gs * E[i][M + j];
     }
 }
 
@@ -189,6 +399,37 @@ static cudaError_t launch_grad_t(const GradArgs &a, cudaStream_t s)
     dim3 grid((unsigned)bx, (unsigned)a.N);
     kern<<<grid, 128, smem, s>>>(a);
     return cudaGetLastError();
+}
+
+template <int DIM, int TESS>
+static cudaError_t launch_grad_ref_t(const GradArgs &a, cudaStream_t s)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    size_t smem = (size_t)4 * a.t.nC * NE * sizeof(double);
+    auto kern = k_grad_ref<DIM, TESS>;
+    if (smem > kSmemOptInAbove) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    int64_t bx = (a.n_per_inst + 127) / 128;
+    int64_t cap = (int64_t)num_sms() * 8 / (a.N > 0 ? a.N : 1) + 1;
+    if (bx > cap) bx = cap;
+    if (bx < 1) bx = 1;
+    dim3 grid((unsigned)bx, (unsigned)a.N);
+    kern<<<grid, 128, smem, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int total = a.N * a.t.nC;
+    k_frechet_adjoint<DIM><<<(total + 63) / 64, 64, 0, s>>>(a.A, a.gT, a.gA, total, a.dt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grad_ref(const GradArgs &a, cudaStream_t s)
+{
+    const int dim = a.t.dim, tess = a.t.tess;
+    if (dim == 1) return launch_grad_ref_t<1, 2>(a, s);
+    if (dim == 2) return tess == 1 ? launch_grad_ref_t<2, 1>(a, s) : launch_grad_ref_t<2, 2>(a, s);
+    return tess == 1 ? launch_grad_ref_t<3, 1>(a, s) : launch_grad_ref_t<3, 2>(a, s);
 }
 
 cudaError_t launch_grad_simple(const GradArgs &a, cudaStream_t s)

@@ -11,11 +11,13 @@ namespace cpab {
 struct GradArgs {
     Tess t;
     const double *A;         // [N, nC, ne] signed matrices of the forward map
+    const double *T;         // [N, nC, ne] their closed-form steps expm(dt A) (reference scheme)
     const double *pts;       // [N * n, DIM] start points
     const double *grad_out;  // [N * n, DIM] dLoss/dT(x)
     double *out;             // [N * n, DIM] T(x) or nullptr
     double *grad_in;         // [N * n, DIM] dLoss/dx or nullptr
     double *gA;              // [N, nC, ne] dLoss/d(signed A), accumulated (zero on entry)
+    double *gT;              // [N, nC, ne] dLoss/dT scratch, zero on entry (reference scheme)
     double *ckpt;            // [ceil(nT/ck), N * n, DIM] scratch
     int N;
     int64_t n_per_inst;
@@ -24,6 +26,7 @@ struct GradArgs {
 };
 
 cudaError_t launch_grad_simple(const GradArgs &a, cudaStream_t s);
+cudaError_t launch_grad_ref(const GradArgs &a, cudaStream_t s);
 cudaError_t launch_bt_times(const double *B, const double *G, double *out, int DA, int d, int N, double scale,
                             cudaStream_t s);
 

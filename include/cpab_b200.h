@@ -370,6 +370,27 @@ int cpab_grad_theta(cpab_ctx *ctx, const double *B, int d, const double *signedA
                     int ck, double *out, double *grad_pts, double *gA, double *dtheta, void *workspace,
                     size_t workspace_bytes, void *stream);
 
+/* Scratch bytes of cpab_grad_theta_ref: checkpoints every ck time steps plus
+ * the per-cell dLoss/dTrels sums [N, nC, ne]. */
+size_t cpab_grad_ref_workspace_bytes(const cpab_ctx *ctx, int N, int64_t n_per_inst, int nTimeSteps, int ck);
+
+/* Gradient of a scalar loss of T(x) through the reference scheme (calc_T:
+ * per time step the closed-form step with Trels = expm(dt * signedA) when its
+ * end point stays in the cell, else nStepsODE midpoint sub-steps;
+ * cpab/gpu/calc_2Dto2D.cu:348-408, cpab/cpaNd/_CpaSpace.py:626-667, whose
+ * sensitivity code, calc_grad_theta :669-686, is never bound).  Same
+ * arguments and outputs as cpab_grad_theta plus Trels [N, nC, ne] from the
+ * same signedA and dt (cpab_theta_to_trels).  The forward run again here is
+ * calc_T's FP64 arithmetic (out: T(x), bit for bit); the adjoint follows the
+ * forward's branch at every step (closed-form step or fallback, and every
+ * sub-step's cell) and maps the per-cell dLoss/dTrels to dLoss/dA through the
+ * adjoint Frechet derivative of expm.  Workspace:
+ * cpab_grad_ref_workspace_bytes.  nStepsODE <= 256. */
+int cpab_grad_theta_ref(cpab_ctx *ctx, const double *B, int d, const double *signedA, const double *Trels, int N,
+                        const double *pts, int64_t n_per_inst, const double *grad_out, double dt, int nTimeSteps,
+                        int nStepsODE, int sign, int ck, double *out, double *grad_pts, double *gA, double *dtheta,
+                        void *workspace, size_t workspace_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
