@@ -590,8 +590,8 @@ static int grad_impl(cpab_ctx *ctx, const double *B, int d, const double *signed
     CPAB_CHECK_ALIGN(ctx, {B, 8, "B"}, {signedA, 8, "signedA"}, {Trels, 8, "Trels"}, {pts, 8, "pts"},
                      {grad_out, 8, "grad_out"}, {out, 8, "out"}, {grad_pts, 8, "grad_pts"}, {gA, 8, "gA"},
                      {dtheta, 8, "dtheta"}, {workspace, 8, "workspace"});
-    // tables (reference scheme: also the closed-form steps and both gradient sums) in shared memory
-    if ((size_t)(ref ? 4 : 2) * ctx->t.nC * cell_len(ctx) * 8 > (size_t)max_smem_optin())
+    // tables (reference scheme: the closed-form steps too) in shared memory
+    if ((size_t)2 * ctx->t.nC * cell_len(ctx) * 8 > (size_t)max_smem_optin())
         return fail(ctx, CPAB_UNSUPPORTED, "cell tables exceed shared memory");
     const size_t ck_bytes = cpab_grad_workspace_bytes(ctx, N, n_per_inst, nTimeSteps, ck);
     const size_t need = ref ? cpab_grad_ref_workspace_bytes(ctx, N, n_per_inst, nTimeSteps, ck) : ck_bytes;

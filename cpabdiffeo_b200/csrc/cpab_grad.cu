@@ -207,22 +207,27 @@ __device__ __forceinline__ bool ref_step(const Tess &t, const double *sA, const 
     return false;
 }
 
-template <int DIM, int TESS>
+// SACC: the gradient sums in shared memory, added to gA / gT at the end;
+// else (large tables) the per-thread accumulators go straight to gA / gT, so
+// that shared memory holds the tables only and more CTAs fit on an SM.
+template <int DIM, int TESS, bool SACC>
 __global__ void __launch_bounds__(128) k_grad_ref(GradArgs a)
 {
     constexpr int NE = DIM * (DIM + 1), NH = DIM + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int tab = a.t.nC * NE;
+    const int inst = blockIdx.y;
     double *sA = reinterpret_cast<double *>(smem_raw);
     double *sT = sA + tab;
-    double *sGA = sT + tab;   // dLoss/dA from sub-steps
-    double *sGT = sGA + tab;  // dLoss/dT from closed-form steps
-    const int inst = blockIdx.y;
+    double *sGA = SACC ? sT + tab : a.gA + (size_t)inst * tab;   // dLoss/dA from sub-steps
+    double *sGT = SACC ? sGA + tab : a.gT + (size_t)inst * tab;  // dLoss/dT from closed-form steps
     for (int i = threadIdx.x; i < tab; i += blockDim.x) {
         sA[i] = a.A[(size_t)inst * tab + i];
         sT[i] = a.T[(size_t)inst * tab + i];
-        sGA[i] = 0.0;
-        sGT[i] = 0.0;
+        if (SACC) {
+            sGA[i] = 0.0;
+            sGT[i] = 0.0;
+        }
     }
     __syncthreads();
     const double h = XDIV(a.dt, (double)a.nStepsODE);
@@ -279,6 +284,7 @@ __global__ void __launch_bounds__(128) k_grad_ref(GradArgs a)
         acc_switch<NE>(sGT, accT, cellT, -1);
         if (a.grad_in) store_pt<DIM, double>(a.grad_in, gi, g);
     }
+    if (!SACC) return;
     __syncthreads();
     for (int i = threadIdx.x; i < tab; i += blockDim.x) {
         const double va = sGA[i], vt = sGT[i];
@@ -405,8 +411,10 @@ template <int DIM, int TESS>
 static cudaError_t launch_grad_ref_t(const GradArgs &a, cudaStream_t s)
 {
     constexpr int NE = DIM * (DIM + 1);
-    size_t smem = (size_t)4 * a.t.nC * NE * sizeof(double);
-    auto kern = k_grad_ref<DIM, TESS>;
+    // gradient sums in shared memory only while all four arrays stay within 48 KB
+    const bool sacc = (size_t)4 * a.t.nC * NE * sizeof(double) <= 48 * 1024;
+    size_t smem = (size_t)(sacc ? 4 : 2) * a.t.nC * NE * sizeof(double);
+    auto kern = sacc ? k_grad_ref<DIM, TESS, true> : k_grad_ref<DIM, TESS, false>;
     if (smem > kSmemOptInAbove) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;

@@ -165,12 +165,16 @@ def _ref_forward(O, t, sA, Tr, x, dt, nT, nODE, branches=None):
 
 
 def _tables_np(sp, theta, dt):
+    ne = sp.dim * (sp.dim + 1)
     sA, Tr = sp.tables_from_theta(theta, dt, 1)
-    return sA[0].cpu().numpy(), Tr[0].cpu().numpy()
+    return sA[0].cpu().numpy().reshape(-1, ne), Tr[0].cpu().numpy().reshape(-1, ne)
 
 
+# (3, (4, 4, 4), "I"): 320 cells, whose gradient sums exceed the kernel's shared-memory budget and go
+# straight to global memory
 @pytest.mark.parametrize("dim,nCs,tess,ls,var", [(1, (20,), "II", 0.1, 1.0), (2, (4, 4), "I", 0.1, 1.0),
-                                                 (2, (3, 3), "II", 0.1, 1.0), (3, (2, 2, 2), "I", 0.15, 0.5)])
+                                                 (2, (3, 3), "II", 0.1, 1.0), (3, (2, 2, 2), "I", 0.15, 0.5),
+                                                 (3, (4, 4, 4), "I", 0.15, 0.5)])
 def test_ref_grad_vs_frozen_branch_fd(oracle_mod, dim, nCs, tess, ls, var):
     O = oracle_mod
     p = dict(dt=0.05, nTimeSteps=20, nStepsODEsolver=10)
@@ -201,11 +205,13 @@ def test_ref_grad_vs_frozen_branch_fd(oracle_mod, dim, nCs, tess, ls, var):
         return 0.5 * ((o - yn) ** 2).sum() + (o * wn).sum()
 
     h = 1e-6
-    fd = np.empty_like(g)
-    for j in range(sp.d):
+    comps = np.arange(sp.d) if sp.d <= 80 else np.random.default_rng(0).choice(sp.d, 60, replace=False)
+    fd = np.empty(len(comps))
+    for m, j in enumerate(comps):
         e = torch.zeros_like(th)
         e[0, j] = h
-        fd[j] = (L(th + e) - L(th - e)) / (2 * h)
+        fd[m] = (L(th + e) - L(th - e)) / (2 * h)
+    g = g[comps]
     err = np.abs(g - fd).max() / np.abs(fd).max()
     print(f"dim {dim} tess {tess}: d={sp.d} kept {kept_frac:.3f} max|fd|={np.abs(fd).max():.3e} rel err {err:.2e}")
     assert err < 1e-6
