@@ -95,3 +95,15 @@ def test_memory_budget_admission_drains():
     assert peak <= 200_000 + 2 * 8000 * 4 + (1 << 16)
     lat = srv.latencies()
     assert (lat > 0).all()
+
+
+def test_load_runner_warms_every_shape_then_serves_all():
+    """run_load serves one small request per shape untimed, forgets it, then
+    replays the seeded arrivals; every timed request completes."""
+    from cpabdiffeo_b200.serving_load import make_requests, run_load
+    reqs = make_requests(40.0, 0.3, seed=8, max_points=2e4, reg_steps=12, max_side=96)
+    r = run_load(reqs, device=torch.device(DEV), time_limit_s=60.0)
+    shapes = {(q.dim, tuple(q.nCs), q.tess) for _, q in reqs if isinstance(q, TransformRequest)}
+    has_reg = any(isinstance(q, RegistrationRequest) for _, q in reqs)
+    assert r["warm_up_requests"] == len(shapes) + int(has_reg)
+    assert r["requests_done"] == r["requests_submitted"] == len(reqs)
