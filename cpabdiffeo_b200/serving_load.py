@@ -59,12 +59,17 @@ def make_requests(rate_hz: float, duration_s: float, seed: int = 4, max_points: 
 
 
 def warm_up(srv: CpabServer, requests) -> int:
-    """Serve, untimed, one small request of every transform shape in `requests`
-    and one short registration job (long enough to capture its CUDA graph),
-    then forget them: the spaces, the kernels of every variant (loaded on
-    first launch) and the graph path are ready before the timed arrivals.
+    """Serve, untimed, one small request of every transform shape in `requests`,
+    the largest transform payload in full, and one short registration job
+    (long enough to capture its CUDA graph), then forget them: the spaces,
+    the kernels of every variant (loaded on first launch), the pinned host
+    buffer pool and the graph path are ready before the timed arrivals.
     Returns the number of warm-up requests."""
     seen, warm = set(), []
+    big = max((r for _, r in requests if isinstance(r, TransformRequest)),
+              key=lambda r: np.asarray(r.pts).shape[0], default=None)
+    if big is not None:
+        warm.append(TransformRequest(big.dim, big.nCs, big.theta, big.pts, tess=big.tess, scheme=big.scheme))
     for _, r in requests:
         if isinstance(r, TransformRequest):
             key = (r.dim, tuple(r.nCs), r.tess, r.scheme)

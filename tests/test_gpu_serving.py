@@ -105,5 +105,5 @@ def test_load_runner_warms_every_shape_then_serves_all():
     r = run_load(reqs, device=torch.device(DEV), time_limit_s=60.0)
     shapes = {(q.dim, tuple(q.nCs), q.tess) for _, q in reqs if isinstance(q, TransformRequest)}
     has_reg = any(isinstance(q, RegistrationRequest) for _, q in reqs)
-    assert r["warm_up_requests"] == len(shapes) + int(has_reg)
+    assert r["warm_up_requests"] == len(shapes) + int(has_reg) + 1  # + the largest payload once
     assert r["requests_done"] == r["requests_submitted"] == len(reqs)
