@@ -79,8 +79,8 @@ SIGNATURES = {
     "cpab_grad_theta": (_i, [_vp, _vp, _i, _vp, _i, _vp, _i64, _vp, _d, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp,
                              _sz, _vp]),
     "cpab_grad_ref_workspace_bytes": (_sz, [_vp, _i, _i64, _i, _i]),
-    "cpab_grad_theta_ref": (_i, [_vp, _vp, _i, _vp, _vp, _i, _vp, _i64, _vp, _d, _i, _i, _i, _i, _vp, _vp, _vp, _vp,
-                                 _vp, _sz, _vp]),
+    "cpab_grad_theta_ref": (_i, [_vp, _vp, _i, _vp, _vp, _i, _vp, _i64, _vp, _i, _d, _i, _i, _i, _i, _vp, _vp, _vp,
+                                 _vp, _vp, _sz, _vp]),
 }
 NOALLOC_MAX_INSTANCES = 65536
 

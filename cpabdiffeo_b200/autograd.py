@@ -13,7 +13,9 @@ dLoss/dT to dLoss/dA through the adjoint Frechet derivative of expm.
 scheme="simple": the forward is calc_T_simple (nTimeSteps * nStepsODE
 midpoint sub-steps) and the backward (cpab_grad_theta) goes through every
 sub-step.  Either is the exact gradient of the discrete map.  theta is
-[N, d] (N transforms), pts [N*n, dim] float64 (n points per transform).
+[N, d] float64 (N transforms), pts [N*n, dim] (n points per transform)
+float64, or float32 with scheme="ref" (the FP32 calc_T and its adjoint; the
+gradient in theta comes back float64).
 """
 from __future__ import annotations
 
@@ -47,8 +49,9 @@ class _Transform(torch.autograd.Function):
         sA, Tr = space.tables_from_theta(theta.detach(), dt, sign)
         out = torch.empty_like(pts)
         c = space._ctx
+        prec = _lib.CPAB_F64 if pts.dtype == torch.float64 else _lib.CPAB_F32
         c.check(c.lib.cpab_calc_T_batched(c.h, _lib.ptr(sA), _lib.ptr(Tr), _lib.ptr(pts), _lib.ptr(out), N, None, n,
-                                          None, 0, _lib.CPAB_F64, _lib.SCHEME_REF if ref else _lib.SCHEME_SIMPLE,
+                                          None, 0, prec, _lib.SCHEME_REF if ref else _lib.SCHEME_SIMPLE,
                                           dt, nT, nODE, None, _lib.stream_ptr()))
         ctx.save_for_backward(pts, sA, Tr)
         ctx.space, ctx.sign, ctx.dt, ctx.nT, ctx.nODE, ctx.ck = space, sign, dt, nT, nODE, ck
@@ -61,7 +64,8 @@ class _Transform(torch.autograd.Function):
         sp: CpaSpace = ctx.space
         N = sA.shape[0]
         n = pts.shape[0] // N
-        g = grad_out.contiguous().to(torch.float64)
+        g = grad_out.contiguous().to(pts.dtype)
+        prec = _lib.CPAB_F64 if pts.dtype == torch.float64 else _lib.CPAB_F32
         dtheta = torch.empty((N, sp.d), dtype=torch.float64, device=pts.device)
         gA = torch.empty((N, sp.D), dtype=torch.float64, device=pts.device)
         gpts = torch.empty_like(pts) if ctx.need_pts_grad else None
@@ -70,7 +74,7 @@ class _Transform(torch.autograd.Function):
             wsb = int(c.lib.cpab_grad_ref_workspace_bytes(c.h, N, n, ctx.nT, ctx.ck))
             ws = torch.empty(max(wsb, 1), dtype=torch.uint8, device=pts.device)
             c.check(c.lib.cpab_grad_theta_ref(c.h, _lib.ptr(sp.B), sp.d, _lib.ptr(sA), _lib.ptr(Tr), N, _lib.ptr(pts),
-                                              n, _lib.ptr(g), ctx.dt, ctx.nT, ctx.nODE, ctx.sign, ctx.ck, None,
+                                              n, _lib.ptr(g), prec, ctx.dt, ctx.nT, ctx.nODE, ctx.sign, ctx.ck, None,
                                               _lib.ptr(gpts), _lib.ptr(gA), _lib.ptr(dtheta), _lib.ptr(ws),
                                               ws.numel(), _lib.stream_ptr()))
         else:
@@ -91,8 +95,10 @@ def transform(theta: torch.Tensor, pts: torch.Tensor, space: CpaSpace, mysign: i
         raise ValueError('scheme must be "ref" or "simple"')
     dt, nT, nODE = _flow(space, params_flow_int)
     theta = theta.reshape(-1, space.d)
-    if theta.dtype != torch.float64 or pts.dtype != torch.float64:
-        raise TypeError("the differentiable transform works in float64")
+    if theta.dtype != torch.float64:
+        raise TypeError("theta must be float64")
+    if pts.dtype != torch.float64 and not (pts.dtype == torch.float32 and scheme == "ref"):
+        raise TypeError("pts must be float64 (or float32 with scheme='ref')")
     N = theta.shape[0]
     if pts.shape[0] % N:
         raise ValueError("pts must hold the same number of points for every theta")

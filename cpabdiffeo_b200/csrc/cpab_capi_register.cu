@@ -561,18 +561,19 @@ size_t cpab_grad_workspace_bytes(const cpab_ctx *ctx, int N, int64_t n_per_inst,
 size_t cpab_grad_ref_workspace_bytes(const cpab_ctx *ctx, int N, int64_t n_per_inst, int nTimeSteps, int ck)
 {
     if (!ctx || N < 0 || n_per_inst < 0 || nTimeSteps < 1 || ck < 1) return 0;
+    // checkpoints (FP32: hi and lo per coordinate, the same bytes), then dLoss/dTrels and dLoss/d(sub-step map)
     return cpab_grad_workspace_bytes(ctx, N, n_per_inst, nTimeSteps, ck) +
-           align256((size_t)N * ctx->t.nC * cell_len(ctx) * sizeof(double));
+           2 * align256((size_t)N * ctx->t.nC * cell_len(ctx) * sizeof(double));
 }
 
 }  // extern "C"
 
-// Shared body of cpab_grad_theta (ref == false: midpoint scheme) and
-// cpab_grad_theta_ref (reference scheme, needs Trels).
+// Shared body of cpab_grad_theta (ref == false: midpoint scheme, FP64) and
+// cpab_grad_theta_ref (reference scheme, needs Trels; FP64 or FP32 points).
 static int grad_impl(cpab_ctx *ctx, const double *B, int d, const double *signedA, const double *Trels, bool ref,
-                     int N, const double *pts, int64_t n_per_inst, const double *grad_out, double dt, int nTimeSteps,
-                     int nStepsODE, int sign, int ck, double *out, double *grad_pts, double *gA, double *dtheta,
-                     void *workspace, size_t workspace_bytes, void *stream)
+                     int N, const void *pts, int64_t n_per_inst, const void *grad_out, int precision, double dt,
+                     int nTimeSteps, int nStepsODE, int sign, int ck, void *out, void *grad_pts, double *gA,
+                     double *dtheta, void *workspace, size_t workspace_bytes, void *stream)
 {
     if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
     if (N < 0 || n_per_inst < 0) return fail(ctx, CPAB_BAD_SHAPE, "N and n_per_inst must be >= 0");
@@ -587,8 +588,12 @@ static int grad_impl(cpab_ctx *ctx, const double *B, int d, const double *signed
     if (ck < 1) return fail(ctx, CPAB_BAD_ARG, "checkpoint stride must be >= 1");
     if (sign != 1 && sign != -1) return fail(ctx, CPAB_BAD_ARG, "sign must be +1 or -1");
     if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
-    CPAB_CHECK_ALIGN(ctx, {B, 8, "B"}, {signedA, 8, "signedA"}, {Trels, 8, "Trels"}, {pts, 8, "pts"},
-                     {grad_out, 8, "grad_out"}, {out, 8, "out"}, {grad_pts, 8, "grad_pts"}, {gA, 8, "gA"},
+    if (precision != CPAB_F64 && precision != CPAB_F32)
+        return fail(ctx, CPAB_BAD_DTYPE, "precision must be CPAB_F64 or CPAB_F32");
+    if (!ref && precision != CPAB_F64) return fail(ctx, CPAB_UNSUPPORTED, "the midpoint-scheme adjoint is FP64");
+    const unsigned pa = precision == CPAB_F64 ? 8u : 4u;
+    CPAB_CHECK_ALIGN(ctx, {B, 8, "B"}, {signedA, 8, "signedA"}, {Trels, 8, "Trels"}, {pts, pa, "pts"},
+                     {grad_out, pa, "grad_out"}, {out, pa, "out"}, {grad_pts, pa, "grad_pts"}, {gA, 8, "gA"},
                      {dtheta, 8, "dtheta"}, {workspace, 8, "workspace"});
     // tables (reference scheme: the closed-form steps too) in shared memory
     if ((size_t)2 * ctx->t.nC * cell_len(ctx) * 8 > (size_t)max_smem_optin())
@@ -607,10 +612,10 @@ static int grad_impl(cpab_ctx *ctx, const double *B, int d, const double *signed
         a.t = ctx->t;
         a.A = signedA;
         a.T = Trels;
-        a.pts = pts;
-        a.grad_out = grad_out;
-        a.out = out;
-        a.grad_in = grad_pts;
+        a.pts = static_cast<const double *>(pts);  // float data when precision is CPAB_F32
+        a.grad_out = static_cast<const double *>(grad_out);
+        a.out = static_cast<double *>(out);
+        a.grad_in = static_cast<double *>(grad_pts);
         a.gA = gA;
         a.ckpt = static_cast<double *>(workspace);
         a.N = N;
@@ -619,11 +624,14 @@ static int grad_impl(cpab_ctx *ctx, const double *B, int d, const double *signed
         a.nTimeSteps = nTimeSteps;
         a.nStepsODE = nStepsODE;
         a.ck = ck;
+        a.h_sub = dt / (double)nStepsODE;
         if (ref) {
+            const size_t sum_bytes = align256((size_t)N * DA * sizeof(double));
             a.gT = reinterpret_cast<double *>(static_cast<char *>(workspace) + ck_bytes);
-            e = cudaMemsetAsync(a.gT, 0, (size_t)N * DA * sizeof(double), s);
-            if (e != cudaSuccess) return cuda_status(ctx, e, "gT reset");
-            e = launch_grad_ref(a, s);
+            a.gS = reinterpret_cast<double *>(static_cast<char *>(workspace) + ck_bytes + sum_bytes);
+            e = cudaMemsetAsync(a.gT, 0, 2 * sum_bytes, s);
+            if (e != cudaSuccess) return cuda_status(ctx, e, "gradient sums reset");
+            e = precision == CPAB_F64 ? launch_grad_ref(a, s) : launch_grad_ref_f32(a, s);
         } else {
             e = launch_grad_simple(a, s);
         }
@@ -643,17 +651,17 @@ int cpab_grad_theta(cpab_ctx *ctx, const double *B, int d, const double *signedA
                     int ck, double *out, double *grad_pts, double *gA, double *dtheta, void *workspace,
                     size_t workspace_bytes, void *stream)
 {
-    return grad_impl(ctx, B, d, signedA, nullptr, false, N, pts, n_per_inst, grad_out, dt, nTimeSteps, nStepsODE,
-                     sign, ck, out, grad_pts, gA, dtheta, workspace, workspace_bytes, stream);
+    return grad_impl(ctx, B, d, signedA, nullptr, false, N, pts, n_per_inst, grad_out, CPAB_F64, dt, nTimeSteps,
+                     nStepsODE, sign, ck, out, grad_pts, gA, dtheta, workspace, workspace_bytes, stream);
 }
 
 int cpab_grad_theta_ref(cpab_ctx *ctx, const double *B, int d, const double *signedA, const double *Trels, int N,
-                        const double *pts, int64_t n_per_inst, const double *grad_out, double dt, int nTimeSteps,
-                        int nStepsODE, int sign, int ck, double *out, double *grad_pts, double *gA, double *dtheta,
-                        void *workspace, size_t workspace_bytes, void *stream)
+                        const void *pts, int64_t n_per_inst, const void *grad_out, int precision, double dt,
+                        int nTimeSteps, int nStepsODE, int sign, int ck, void *out, void *grad_pts, double *gA,
+                        double *dtheta, void *workspace, size_t workspace_bytes, void *stream)
 {
-    return grad_impl(ctx, B, d, signedA, Trels, true, N, pts, n_per_inst, grad_out, dt, nTimeSteps, nStepsODE, sign,
-                     ck, out, grad_pts, gA, dtheta, workspace, workspace_bytes, stream);
+    return grad_impl(ctx, B, d, signedA, Trels, true, N, pts, n_per_inst, grad_out, precision, dt, nTimeSteps,
+                     nStepsODE, sign, ck, out, grad_pts, gA, dtheta, workspace, workspace_bytes, stream);
 }
 
 }  // extern "C"

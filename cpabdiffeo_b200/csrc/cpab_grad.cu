@@ -375,6 +375,240 @@ __global__ void k_frechet_adjoint(const double *A, const double *gT, double *gA,
     }
 }
 
+// ------------------------------------------------------------ FP32 adjoint of calc_T
+//
+// The FP32 forward (k_integrate<float>, SCHEME_REF) keeps each coordinate as
+// a compensated pair hi + lo and moves it by x + M[x; 1] with the cell's
+// float T - I (closed-form step) or S - I (one midpoint sub-step, S the
+// sub-step's affine map).  k_grad_ref_f32 replays exactly that arithmetic
+// (checkpoints hold hi and lo) and goes backwards through
+//     x' = x + M_c [x; 1]:   dM_c += g [x; 1]^T,  g = g + M_lin^T g,
+// with dM summed per cell for T (gT) and for S (gS).  Per instance and cell,
+// dLoss/dA then follows in FP64 from gT through the expm Frechet adjoint and
+// from gS through the derivative of S - I = [hL + h^2/2 L^2 | hb + h^2/2 Lb]
+// (k_substep_map_adjoint).
+
+template <int NE>
+__device__ __forceinline__ void acc_switch_f(double *sG, float *acc, int &acc_cell, int c)
+{
+    if (c == acc_cell) return;
+    if (acc_cell >= 0) {
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
+            atomicAdd(sG + acc_cell * NE + e, (double)acc[e]);
+            acc[e] = 0.0f;
+        }
+    }
+    acc_cell = c;
+}
+
+// x' = x + M[x; 1] on the compensated state (the float advance() of the lane scheduler)
+template <int DIM>
+__device__ __forceinline__ void f32_map(PState<DIM, float> &st, const float *M)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    float m[NE], d[DIM];
+    load_cell<DIM>(M, m);
+    cm_affine<DIM>(d, m, st.x);
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) st.add(r, d[r]);
+}
+
+// One time step of calc_T in FP32 from st; returns whether the closed-form step was kept.
+template <int DIM, int TESS>
+__device__ __forceinline__ bool ref_step_f32(const Tess &t, const float *sS, const float *sT, PState<DIM, float> &st,
+                                             int nODE)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    const int c = fast_cell<DIM, TESS>(t, st.x);
+    PState<DIM, float> q = st;
+    f32_map<DIM>(q, sT + c * NE);
+    if (fast_cell<DIM, TESS>(t, q.x) == c) {
+        st = q;
+        return true;
+    }
+    for (int k = 0; k < nODE; ++k) f32_map<DIM>(st, sS + fast_cell<DIM, TESS>(t, st.x) * NE);
+    return false;
+}
+
+// Backwards through x' = x + M[x; 1] (M column-major float, cell c): accumulate
+// g [x; 1]^T into acc (row-major, as the FP64 tables) and set g += M_lin^T g.
+template <int DIM>
+__device__ __forceinline__ void f32_map_adjoint(const float *M, const float *x, float *g, float *acc)
+{
+    constexpr int NE = DIM * (DIM + 1), NH = DIM + 1;
+    float m[NE];
+    load_cell<DIM>(M, m);
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) {
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) acc[r * NH + k] = fmaf(g[r], x[k], acc[r * NH + k]);
+        acc[r * NH + DIM] += g[r];
+    }
+    float gn[DIM];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        float s2 = g[k];
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) s2 = fmaf(m[k * DIM + r], g[r], s2);
+        gn[k] = s2;
+    }
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) g[k] = gn[k];
+}
+
+// Backwards through the nODE sub-steps of a fallback step starting at st (consumed).
+template <int DIM, int TESS>
+__device__ __forceinline__ void adjoint_substeps_f32(const Tess &t, const float *sS, double *sGS,
+                                                     PState<DIM, float> &st, float *g, int nODE, float *acc,
+                                                     int &acc_cell)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    const int ngroups = (nODE + kGroup - 1) / kGroup;
+    float starts[kGroup][2 * DIM];  // hi, lo at each group's first sub-step
+    float xs[kGroup][DIM];
+    int cs[kGroup];
+    for (int k = 0; k < nODE; ++k) {
+        if (k % kGroup == 0) {
+#pragma unroll
+            for (int i = 0; i < DIM; ++i) {
+                starts[k / kGroup][i] = st.hi[i];
+                starts[k / kGroup][DIM + i] = st.lo[i];
+            }
+        }
+        f32_map<DIM>(st, sS + fast_cell<DIM, TESS>(t, st.x) * NE);
+    }
+    for (int gr = ngroups - 1; gr >= 0; --gr) {
+        const int k0 = gr * kGroup, k1 = min(nODE, k0 + kGroup);
+        PState<DIM, float> r;
+#pragma unroll
+        for (int i = 0; i < DIM; ++i) {
+            r.hi[i] = starts[gr][i];
+            r.lo[i] = starts[gr][DIM + i];
+            r.x[i] = r.hi[i] + r.lo[i];
+        }
+        for (int k = k0; k < k1; ++k) {
+            const int c = fast_cell<DIM, TESS>(t, r.x);
+#pragma unroll
+            for (int i = 0; i < DIM; ++i) xs[k - k0][i] = r.x[i];
+            cs[k - k0] = c;
+            f32_map<DIM>(r, sS + c * NE);
+        }
+        for (int k = k1 - 1; k >= k0; --k) {
+            const int c = cs[k - k0];
+            acc_switch_f<NE>(sGS, acc, acc_cell, c);
+            f32_map_adjoint<DIM>(sS + c * NE, xs[k - k0], g, acc);
+        }
+    }
+}
+
+template <int DIM, int TESS, bool SACC>
+__global__ void __launch_bounds__(128) k_grad_ref_f32(GradArgs a)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tab = a.t.nC * NE;
+    const int inst = blockIdx.y;
+    double *sums = reinterpret_cast<double *>(smem_raw);
+    double *sGS = SACC ? sums : a.gS + (size_t)inst * tab;        // dLoss/dS (sub-steps)
+    double *sGT = SACC ? sums + tab : a.gT + (size_t)inst * tab;  // dLoss/dT (closed-form steps)
+    float *sS = reinterpret_cast<float *>(sums + (SACC ? 2 * tab : 0));
+    float *sT = sS + tab;
+    stage_tables<DIM, float>(a.A + (size_t)inst * tab, a.T + (size_t)inst * tab, a.t.nC, true, a.h_sub, sS, sT);
+    if (SACC)
+        for (int i = threadIdx.x; i < 2 * tab; i += blockDim.x) sums[i] = 0.0;
+    __syncthreads();
+    const int nT = a.nTimeSteps, nODE = a.nStepsODE, ck = a.ck;
+    const int64_t n = a.n_per_inst;
+    const int64_t total = n * a.N;
+    float *ckpt = reinterpret_cast<float *>(a.ckpt);  // [ceil(nT/ck), N*n, 2*DIM]: hi, lo
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t gi = (int64_t)inst * n + j;
+        float p[DIM];
+        load_pt<DIM, float>(a.pts, gi, p);
+        PState<DIM, float> st;
+        st.set(p);
+        for (int s = 0; s < nT; ++s) {
+            if (s % ck == 0) {
+                float *c = ckpt + ((int64_t)(s / ck) * total + gi) * 2 * DIM;
+#pragma unroll
+                for (int i = 0; i < DIM; ++i) {
+                    c[i] = st.hi[i];
+                    c[DIM + i] = st.lo[i];
+                }
+            }
+            ref_step_f32<DIM, TESS>(a.t, sS, sT, st, nODE);
+        }
+        if (a.out) {
+            st.get(p);
+            store_pt<DIM, float>(a.out, gi, p);
+        }
+        float g[DIM];
+        load_pt<DIM, float>(a.grad_out, gi, g);
+        float accS[NE], accT[NE];
+#pragma unroll
+        for (int e = 0; e < NE; ++e) accS[e] = accT[e] = 0.0f;
+        int cellS = -1, cellT = -1;
+        for (int s = nT - 1; s >= 0; --s) {
+            PState<DIM, float> q;
+            const float *c = ckpt + ((int64_t)(s / ck) * total + gi) * 2 * DIM;
+#pragma unroll
+            for (int i = 0; i < DIM; ++i) {
+                q.hi[i] = c[i];
+                q.lo[i] = c[DIM + i];
+                q.x[i] = q.hi[i] + q.lo[i];
+            }
+            for (int r = 0; r < s % ck; ++r) ref_step_f32<DIM, TESS>(a.t, sS, sT, q, nODE);
+            // time step s from q, along the forward's branch
+            const int cc = fast_cell<DIM, TESS>(a.t, q.x);
+            PState<DIM, float> y = q;
+            f32_map<DIM>(y, sT + cc * NE);
+            if (fast_cell<DIM, TESS>(a.t, y.x) == cc) {
+                acc_switch_f<NE>(sGT, accT, cellT, cc);
+                f32_map_adjoint<DIM>(sT + cc * NE, q.x, g, accT);
+            } else {
+                adjoint_substeps_f32<DIM, TESS>(a.t, sS, sGS, q, g, nODE, accS, cellS);
+            }
+        }
+        acc_switch_f<NE>(sGS, accS, cellS, -1);
+        acc_switch_f<NE>(sGT, accT, cellT, -1);
+        if (a.grad_in) store_pt<DIM, float>(a.grad_in, gi, g);
+    }
+    if (!SACC) return;
+    __syncthreads();
+    for (int i = threadIdx.x; i < tab; i += blockDim.x) {
+        const double vs = sGS[i], vt = sGT[i];
+        if (vs != 0.0) atomicAdd(a.gS + (size_t)inst * tab + i, vs);
+        if (vt != 0.0) atomicAdd(a.gT + (size_t)inst * tab + i, vt);
+    }
+}
+
+// gA[c] += dLoss/dA through S - I = [hL + h^2/2 L^2 | hb + h^2/2 Lb] (A = [L | b]):
+//     dL = h G + h^2/2 (G L^T + L^T G + g b^T),   db = h g + h^2/2 L^T g,
+// G, g the linear and offset parts of gS[c].
+template <int DIM>
+__global__ void k_substep_map_adjoint(const double *A, const double *gS, double *gA, int total, double h)
+{
+    constexpr int M = DIM + 1, NE = DIM * M;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+        const double *a = A + (size_t)idx * NE;
+        const double *G = gS + (size_t)idx * NE;
+        double *o = gA + (size_t)idx * NE;
+        const double hh = 0.5 * h * h;
+        for (int i = 0; i < DIM; ++i) {
+            for (int j = 0; j < DIM; ++j) {
+                double s2 = 0.0;
+                for (int k = 0; k < DIM; ++k) s2 += G[i * M + k] * a[j * M + k] + a[k * M + i] * G[k * M + j];
+                s2 += G[i * M + DIM] * a[j * M + DIM];
+                o[i * M + j] += h * G[i * M + j] + hh * s2;
+            }
+            double s3 = 0.0;
+            for (int k = 0; k < DIM; ++k) s3 += a[k * M + i] * G[k * M + DIM];
+            o[i * M + DIM] += h * G[i * M + DIM] + hh * s3;
+        }
+    }
+}
+
 // out[n, j] = scale * sum_k B[k, j] * G[n, k]  (dLoss/dtheta = B^T dLoss/dA)
 __global__ void k_bt_times(const double *B, const double *G, double *out, int DA, int d, int N, double scale)
 {
@@ -430,6 +664,40 @@ static cudaError_t launch_grad_ref_t(const GradArgs &a, cudaStream_t s)
     const int total = a.N * a.t.nC;
     k_frechet_adjoint<DIM><<<(total + 63) / 64, 64, 0, s>>>(a.A, a.gT, a.gA, total, a.dt);
     return cudaGetLastError();
+}
+
+template <int DIM, int TESS>
+static cudaError_t launch_grad_ref_f32_t(const GradArgs &a, cudaStream_t s)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    const size_t tables = (size_t)2 * a.t.nC * NE * sizeof(float), sums = (size_t)2 * a.t.nC * NE * sizeof(double);
+    const bool sacc = tables + sums <= 48 * 1024;
+    const size_t smem = tables + (sacc ? sums : 0);
+    auto kern = sacc ? k_grad_ref_f32<DIM, TESS, true> : k_grad_ref_f32<DIM, TESS, false>;
+    if (smem > kSmemOptInAbove) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    int64_t bx = (a.n_per_inst + 127) / 128;
+    int64_t cap = (int64_t)num_sms() * 8 / (a.N > 0 ? a.N : 1) + 1;
+    if (bx > cap) bx = cap;
+    if (bx < 1) bx = 1;
+    dim3 grid((unsigned)bx, (unsigned)a.N);
+    kern<<<grid, 128, smem, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int total = a.N * a.t.nC;
+    k_frechet_adjoint<DIM><<<(total + 63) / 64, 64, 0, s>>>(a.A, a.gT, a.gA, total, a.dt);
+    k_substep_map_adjoint<DIM><<<(total + 127) / 128, 128, 0, s>>>(a.A, a.gS, a.gA, total, a.h_sub);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grad_ref_f32(const GradArgs &a, cudaStream_t s)
+{
+    const int dim = a.t.dim, tess = a.t.tess;
+    if (dim == 1) return launch_grad_ref_f32_t<1, 2>(a, s);
+    if (dim == 2) return tess == 1 ? launch_grad_ref_f32_t<2, 1>(a, s) : launch_grad_ref_f32_t<2, 2>(a, s);
+    return tess == 1 ? launch_grad_ref_f32_t<3, 1>(a, s) : launch_grad_ref_f32_t<3, 2>(a, s);
 }
 
 cudaError_t launch_grad_ref(const GradArgs &a, cudaStream_t s)

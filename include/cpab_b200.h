@@ -371,7 +371,7 @@ int cpab_grad_theta(cpab_ctx *ctx, const double *B, int d, const double *signedA
                     size_t workspace_bytes, void *stream);
 
 /* Scratch bytes of cpab_grad_theta_ref: checkpoints every ck time steps plus
- * the per-cell dLoss/dTrels sums [N, nC, ne]. */
+ * two per-cell sums [N, nC, ne] (dLoss/dTrels, dLoss/d(sub-step map)). */
 size_t cpab_grad_ref_workspace_bytes(const cpab_ctx *ctx, int N, int64_t n_per_inst, int nTimeSteps, int ck);
 
 /* Gradient of a scalar loss of T(x) through the reference scheme (calc_T:
@@ -380,16 +380,19 @@ size_t cpab_grad_ref_workspace_bytes(const cpab_ctx *ctx, int N, int64_t n_per_i
  * cpab/gpu/calc_2Dto2D.cu:348-408, cpab/cpaNd/_CpaSpace.py:626-667, whose
  * sensitivity code, calc_grad_theta :669-686, is never bound).  Same
  * arguments and outputs as cpab_grad_theta plus Trels [N, nC, ne] from the
- * same signedA and dt (cpab_theta_to_trels).  The forward run again here is
- * calc_T's FP64 arithmetic (out: T(x), bit for bit); the adjoint follows the
- * forward's branch at every step (closed-form step or fallback, and every
- * sub-step's cell) and maps the per-cell dLoss/dTrels to dLoss/dA through the
- * adjoint Frechet derivative of expm.  Workspace:
- * cpab_grad_ref_workspace_bytes.  nStepsODE <= 256. */
+ * same signedA and dt (cpab_theta_to_trels) and `precision`: pts, grad_out,
+ * out and grad_pts are float64 (CPAB_F64) or float32 (CPAB_F32); signedA,
+ * Trels, gA and dtheta are float64 either way.  The forward run again here is
+ * calc_T's arithmetic in that precision (out: T(x), bit for bit); the
+ * adjoint follows the forward's branch at every step (closed-form step or
+ * fallback, and every sub-step's cell) and maps the per-cell dLoss/dTrels to
+ * dLoss/dA through the adjoint Frechet derivative of expm (FP32: also the
+ * sub-steps' per-cell map).  Workspace: cpab_grad_ref_workspace_bytes.
+ * nStepsODE <= 256. */
 int cpab_grad_theta_ref(cpab_ctx *ctx, const double *B, int d, const double *signedA, const double *Trels, int N,
-                        const double *pts, int64_t n_per_inst, const double *grad_out, double dt, int nTimeSteps,
-                        int nStepsODE, int sign, int ck, double *out, double *grad_pts, double *gA, double *dtheta,
-                        void *workspace, size_t workspace_bytes, void *stream);
+                        const void *pts, int64_t n_per_inst, const void *grad_out, int precision, double dt,
+                        int nTimeSteps, int nStepsODE, int sign, int ck, void *out, void *grad_pts, double *gA,
+                        double *dtheta, void *workspace, size_t workspace_bytes, void *stream);
 
 #ifdef __cplusplus
 }

@@ -121,23 +121,27 @@ def test_grad_ref_validation_before_launch():
     assert lib.cpab_ctx_create(C.byref(h), 2, 1, nCs, incs) == 0
     N, n, nT, ck = 3, 100, 50, 5
     ws = lib.cpab_grad_ref_workspace_bytes(h, N, n, nT, ck)
-    # checkpoints (10 x 300 points x 2 doubles) + dLoss/dTrels (3 x 64 cells x 6 doubles), each 256-aligned
-    assert ws == 48128 + 9216
+    # checkpoints (10 x 300 points x 2 doubles) + dLoss/dTrels and dLoss/d(sub-step map)
+    # (3 x 64 cells x 6 doubles each), each 256-aligned
+    assert ws == 48128 + 2 * 9216
     assert lib.cpab_grad_workspace_bytes(h, N, n, nT, ck) == 48128
     base = 1 << 20
-    args = [h, base, 62, base, base, N, base, n, base, 0.02, nT, 100, 1, ck, None, None, base, base, base, ws, None]
+    args = [h, base, 62, base, base, N, base, n, base, 0, 0.02, nT, 100, 1, ck, None, None, base, base, base, ws, None]
     bad = list(args)
     bad[4] = None                                              # Trels NULL
     assert lib.cpab_grad_theta_ref(*bad) == 1
     assert b"Trels" in lib.cpab_last_error_string(h)
     bad = list(args)
-    bad[12] = 0                                                # sign 0
+    bad[13] = 0                                                # sign 0
     assert lib.cpab_grad_theta_ref(*bad) == 1
     bad = list(args)
-    bad[11] = 300                                              # more sub-steps than the adjoint replays
+    bad[12] = 300                                              # more sub-steps than the adjoint replays
     assert lib.cpab_grad_theta_ref(*bad) != 0
     small = list(args)
-    small[19] = ws - 8                                         # workspace too small
+    small[20] = ws - 8                                         # workspace too small
     assert lib.cpab_grad_theta_ref(*small) == 5
     assert b"workspace" in lib.cpab_last_error_string(h)
+    bad = list(args)
+    bad[9] = 7                                                 # unknown precision
+    assert lib.cpab_grad_theta_ref(*bad) == 3
     assert lib.cpab_ctx_destroy(h) == 0

@@ -256,3 +256,52 @@ def test_ref_batched_thetas_independent_and_inverse():
             t = one.clone().requires_grad_(True)
             (transform(t, x, sp, mysign=sign, **p) ** 2).sum().backward()
             torch.testing.assert_close(both.grad[i], t.grad[0], rtol=1e-12, atol=1e-12)
+
+
+# FP32 points (scheme="ref"): the FP32 calc_T and its adjoint.  The FP32 forward differs from the FP64 one by
+# ~1e-7 and may take the other branch at a step whose end point lies that close to a cell face, so its
+# gradient is compared with the FP64 adjoint's: 2e-3 relative to max|grad|.
+@pytest.mark.parametrize("dim,nCs,tess,ls,var", [(1, (20,), "II", 0.1, 1.0), (2, (4, 4), "I", 0.1, 1.0),
+                                                 (3, (2, 2, 2), "I", 0.15, 0.5), (3, (4, 4, 4), "I", 0.15, 0.5)])
+def test_ref_grad_f32_vs_f64(dim, nCs, tess, ls, var):
+    p = dict(dt=0.05, nTimeSteps=20, nStepsODEsolver=10)
+    sp, th, th2, x = _setup(dim, nCs, tess, 2000, 13, ls, var)
+    sp32 = CpaSpace([0.0] * dim, [1.0] * dim, nCs, tess=tess, device=DEV, precision=torch.float32)
+    x32 = x.float()
+    x64 = x32.double()
+    with torch.no_grad():
+        y = transform(th2, x64, sp, **p)
+    grads = {}
+    for name, s_, xx0 in (("f64", sp, x64), ("f32", sp32, x32)):
+        t = th.clone().requires_grad_(True)
+        xx = xx0.clone().requires_grad_(True)
+        out = transform(t, xx, s_, **p)
+        (0.5 * ((out.double() - y) ** 2).sum()).backward()
+        grads[name] = (t.grad[0].cpu().numpy(), xx.grad.double().cpu().numpy(), out.detach())
+    # the FP32 forward of the adjoint is calc_T in FP32, bit for bit
+    sA, Tr = sp32.tables_from_theta(th, p["dt"], 1)
+    ref = torch.empty_like(x32)
+    sp32.calc_T_batched((sA, Tr), x32, ref, scheme=_lib.SCHEME_REF, **p)
+    assert torch.equal(grads["f32"][2], ref)
+    g64, g32 = grads["f64"][0], grads["f32"][0]
+    err = np.abs(g32 - g64).max() / np.abs(g64).max()
+    errx = np.abs(grads["f32"][1] - grads["f64"][1]).max() / np.abs(grads["f64"][1]).max()
+    print(f"dim {dim} {nCs}: d={sp.d} FP32 vs FP64 gradient rel err {err:.2e} (points {errx:.2e})")
+    assert err < 2e-3 and errx < 2e-3
+
+
+def test_ref_grad_f32_ck_invariance():
+    p = dict(dt=0.02, nTimeSteps=12, nStepsODEsolver=30)
+    sp = CpaSpace([0.0, 0.0], [1.0, 1.0], (4, 4), tess="I", device=DEV, precision=torch.float32)
+    rng = np.random.default_rng(21)
+    th = torch.as_tensor(Prior.create(sp.geo, 0.1, 1.0).sample(2, rng), device=DEV)
+    x = torch.as_tensor(rng.uniform(0.05, 0.95, size=(2 * 1500, 2)).astype(np.float32), device=DEV)
+    grads = []
+    for ck in (1, 5, 12):
+        t = th.clone().requires_grad_(True)
+        xx = x.clone().requires_grad_(True)
+        transform(t, xx, sp, ck=ck, **p).pow(2).sum().backward()
+        grads.append((t.grad.clone(), xx.grad.clone()))
+    for gt, gx in grads[1:]:
+        assert torch.equal(gx, grads[0][1])
+        torch.testing.assert_close(gt, grads[0][0], rtol=1e-6, atol=0)
