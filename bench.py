@@ -421,6 +421,37 @@ def other_configs(torch, dev) -> dict:
                                     "scheme": "calc_T (closed-form steps + sub-step fallback) forward, adjoint along "
                                               "the forward's branches, expm Frechet adjoint per cell",
                                     "midpoint_scheme_ms_fwd_plus_adjoint": ms_simple}
+    del x3, y3
+
+    # the configuration's size in FP32: 64 theta x 128^3 grid points (134 M), forward + adjoint, checkpoints
+    # within 48 GB (every 4th time step; the others are recomputed)
+    sp32 = CpaSpace([0, 0, 0], [1, 1, 1], (4, 4, 4), tess="I", device=dev, precision=torch.float32)
+    th32 = torch.as_tensor(pr3.sample(64, rng), device=dev)
+    g = ((np.arange(128) + 0.5) / 128).astype(np.float32)
+    grid = torch.as_tensor(np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3), device=dev)
+    x32 = grid.repeat(64, 1)
+    with torch.no_grad():
+        y32 = transform(torch.as_tensor(pr3.sample(64, rng), device=dev), x32, sp32, **p)
+    budget = 48 << 30
+
+    def step32():
+        t = th32.clone().requires_grad_(True)
+        (0.5 * ((transform(t, x32, sp32, memory_budget_bytes=budget, **p) - y32).double() ** 2).sum()).backward()
+        return t.grad
+
+    step32()
+    a, b = ev(), ev()
+    a.record()
+    step32()
+    b.record()
+    b.synchronize()
+    ms32 = a.elapsed_time(b)
+    out["c2_3d_fwd_adjoint_f32_64theta_128cube"] = {
+        "theta": 64, "points_per_theta": 128 ** 3, "d": sp3.d, "ms_fwd_plus_adjoint": ms32,
+        "points_per_s": x32.shape[0] / (ms32 * 1e-3),
+        "scheme": "calc_T in FP32 (compensated state) forward, its adjoint; gradient FP64",
+        "checkpoint_budget_bytes": budget}
+    del x32, y32, grid
 
     # batched MCMC registration: 256 chains x 256^2, FP32, steps captured in a CUDA graph
     sp2 = CpaSpace([0, 0], [1, 1], (4, 4), tess="I", device=dev, precision=torch.float32)
