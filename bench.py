@@ -886,14 +886,15 @@ def main():
             if args.serve_seconds > 0:
                 try:
                     from cpabdiffeo_b200.serving_load import make_requests, run_load
+                    # the mix at 200 req/s (latency when the GPU keeps up) before the overload run
+                    reqs = make_requests(200.0, 2.0, seed=5)
+                    line["serving_200hz"] = dict(run_load(reqs, device=dev), arrival_rate_hz=200.0, arrivals_s=2.0)
                     reqs = make_requests(2000.0, args.serve_seconds, seed=4)
                     line["serving"] = dict(run_load(reqs, device=dev), arrival_rate_hz=2000.0,
                                            arrivals_s=args.serve_seconds,
                                            mix="1D/2D/3D, nC in {16,64,256,1024}, 1e3-4e6 pts, 10% 200-step "
                                                "registrations (side 64-1024)")
-                    # the same mix at a tenth of the rate: latency when the GPU keeps up
-                    reqs = make_requests(200.0, 2.0, seed=5)
-                    line["serving_200hz"] = dict(run_load(reqs, device=dev), arrival_rate_hz=200.0, arrivals_s=2.0)
+                    del reqs
                 except Exception as ex:
                     line["serving"] = {"error": repr(ex)}
         print(json.dumps(line), flush=True)

@@ -15,6 +15,7 @@ Metropolis steps); theta from the Gaussian prior.
 """
 from __future__ import annotations
 
+import gc
 import time
 
 import numpy as np
@@ -92,6 +93,7 @@ def run_load(requests, device=None, time_limit_s: float = 120.0) -> dict:
     srv = CpabServer(device=device)
     # spaces, kernels and graph capture warmed by one small request of each shape (not timed)
     n_warm = warm_up(srv, requests)
+    gc.collect()                                   # garbage of earlier work is not collected inside the window
     t0 = time.perf_counter()
     i = 0
     while i < len(requests) or not srv.idle():
