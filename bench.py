@@ -60,11 +60,13 @@ def parse():
                     help="instance groups of the host-buffer pipeline (copy in / integrate / copy out overlap)")
     ap.add_argument("--serve-seconds", type=float, default=0.5,
                     help="seconds of Poisson arrivals (2000 req/s) for the serving leg; 0 skips it")
-    ap.add_argument("--workload", default="batched_1d", choices=["batched_1d", "batched_2d_nc64", "remap_ssd"],
+    ap.add_argument("--workload", default="batched_1d",
+                    choices=["batched_1d", "batched_2d_nc64", "remap_ssd", "mcmc_c3"],
                     help="batched_1d: the headline (1D nC=100, 4096 theta, ragged); batched_2d_nc64: the reference "
                          "scheme in FP32 on 2D tess I 4x4 (nC=64), 4096 theta x 8192 points, for the "
                          "integration kernel's FP32 roofline; remap_ssd: remap + SSD of 256 pairs of 256x256 "
-                         "images through FP32 maps, for its HBM roofline")
+                         "images through FP32 maps, for its HBM roofline; mcmc_c3: 256-chain MCMC registration of "
+                         "256x256 FP32 image pairs, for the fused likelihood kernel's roofline")
     return ap.parse_args()
 
 
@@ -614,6 +616,77 @@ def remap_ssd_c3(torch, dev, theta, src, dst, reps: int = 10) -> dict:
             "l2": "256 MB buffer written before each timed call"}
 
 
+def bench_mcmc_c3(args, torch, dev) -> dict:
+    """Batched MCMC registration (the 256-chain configuration): 256 chains, each
+    its own 256x256 FP32 image pair (target = source warped by a prior draw plus
+    N(0, 0.02^2) noise), sigma 0.05, random-walk proposals 0.05 Sigma^1/2; a step
+    is one Metropolis step of every chain (propose, A = B theta and expm,
+    fused integration + remap + SSD, accept), 10 steps per CUDA graph."""
+    from scipy.ndimage import gaussian_filter
+
+    from cpabdiffeo_b200 import _lib
+    from cpabdiffeo_b200.cpa_space import CpaSpace
+    from cpabdiffeo_b200.mcmc import BatchedMetropolis
+    from cpabdiffeo_b200.registration import GaussianLogLikelihood
+    from cpabdiffeo_b200.space import Prior
+    rng = np.random.default_rng(2)
+    torch.manual_seed(2)
+    p = dict(dt=DT, nTimeSteps=NT, nStepsODEsolver=NODE)
+    sp = CpaSpace([0, 0], [1, 1], (4, 4), tess="I", device=dev, precision=torch.float32)
+    pr = Prior.create(sp.geo, 0.1, 1.0)
+    C, H = 256, 256
+    src = torch.as_tensor(np.stack([gaussian_filter(rng.uniform(0, 1, (H, H)).astype(np.float32), 8.0)
+                                    for _ in range(C)]), device=dev)
+    warped = torch.empty_like(src)
+    GaussianLogLikelihood(sp, src, src, 0.05, p).batch(torch.as_tensor(pr.sample(C, rng), device=dev), warped=warped)
+    dst = warped + 0.02 * torch.randn_like(warped)
+    ll = GaussianLogLikelihood(sp, src, dst, 0.05, p)
+    mh = BatchedMetropolis(ll, torch.zeros((C, sp.d), device=dev), np.sqrt(np.diag(pr.cov_cpa)), scale=0.05, seed=3)
+    steps = 10 * max(1, -(-args.steps // 10))
+    mh.run(10 * max(1, -(-args.warmup // 10)), graph_steps=10)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index or 0) as clk:
+        torch.cuda.nvtx.range_push("timed_mcmc")
+        s.record()
+        mh.run(steps, graph_steps=10)
+        e.record()
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+    ms = s.elapsed_time(e) / steps
+    # the fused likelihood kernel alone on the chains' current proposals, with its work counters
+    cnt = torch.zeros(_lib.CNT_N, dtype=torch.int64, device=dev)
+    ll.batch_tables((mh.sA, mh.Tr), ll=mh.ll_prop, counters=cnt)
+    ks, ke = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ks.record()
+    for _ in range(5):
+        ll.batch_tables((mh.sA, mh.Tr), ll=mh.ll_prop)
+    ke.record()
+    torch.cuda.synchronize()
+    kern_ms = ks.elapsed_time(ke) / 5
+    cnt_h = cnt.cpu().numpy()
+    flops = flops_ref_2d(cnt_h)
+    peaks = measured_peaks(torch)
+    achieved = flops / (kern_ms * 1e-3) / 1e12
+    return {"metric": METRIC, "value": C * H * H / (ms * 1e-3), "unit": "pixels/s", "n_gpus": 1,
+            "steps": steps, "warmup": 10 * max(1, -(-args.warmup // 10)), "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (smoothed noise images, targets warped by prior draws plus noise)",
+            "config": {"workload": "mcmc_registration_256chains_256x256_f32", "sigma": 0.05, "proposal_scale": 0.05,
+                       "graph_steps": 10, "l2": "images 128 MB (src+dst), each step reads all of them"},
+            "mh_steps_per_s_all_chains": C / (ms * 1e-3), "accept_pct_mean": float(mh.accept_ratio().mean()),
+            "gpu_launches": 4 * steps, "clocks": clk.summary(),
+            "work": {"kept_steps": int(cnt_h[0]), "fallback_steps": int(cnt_h[1]), "substeps": int(cnt_h[2]),
+                     "pixels": int(cnt_h[3])},
+            "roofline": {"bound": "fp32", "kernel": "k_register_ll<tess I, float>", "achieved": achieved,
+                         "peak": peaks["fp32_simt_tflops"], "unit": "TFLOP/s",
+                         "frac": achieved / peaks["fp32_simt_tflops"],
+                         "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off",
+                         "flop_model": "the integration's algorithmic FLOPs as for the 2D workload (sampling and SSD "
+                                       "not counted)",
+                         "kernel_ms": kern_ms, "algorithmic_flop_per_launch": flops, "traffic": None}}
+
+
 def bench_remap(args, torch, dev) -> dict:
     """remap + SSD of 256 image pairs 256x256 through precomputed FP32 maps."""
     from scipy.ndimage import gaussian_filter
@@ -657,7 +730,8 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if args.workload != "batched_1d":
-        line = bench_2d(args, torch, dev) if args.workload == "batched_2d_nc64" else bench_remap(args, torch, dev)
+        line = {"batched_2d_nc64": bench_2d, "remap_ssd": bench_remap, "mcmc_c3": bench_mcmc_c3}[args.workload](
+            args, torch, dev)
         if rank == 0:
             print(json.dumps(line), flush=True)
         return
