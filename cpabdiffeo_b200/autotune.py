@@ -1,8 +1,8 @@
 """Autotuner for the integration launch shape.
 
 Candidates: threads per CTA, points per CTA tile, cell-sort on/off.  Each is
-timed with CUDA events on a sample of the caller's batch (the first instances
-up to `sample_points` points), the fastest kept, and the choice cached per
+timed with CUDA events on a sample of the caller's batch (its first whole
+instances, up to `sample_points` points), the fastest kept, and the choice cached per
 (GPU name, dim, tessellation, cell count, precision, scheme) in memory and in
 a JSON file (CPAB_B200_CACHE directory).  Results never depend on the choice:
 every configuration runs each point through the same arithmetic.
@@ -85,7 +85,10 @@ def tune(space: CpaSpace, tables, pts: torch.Tensor, offsets: torch.Tensor | Non
         sub_off = offsets[:n_inst + 1]
         x = pts[:int(offs[n_inst])]
     else:
-        sub_tables, sub_off, x = tables, None, pts[:sample_points - sample_points % sA.shape[0]]
+        # whole instances (the batch's own points per instance), as many as the sample holds
+        n_per = pts.shape[0] // max(1, sA.shape[0])
+        n_inst = max(1, min(sA.shape[0], sample_points // max(1, n_per)))
+        sub_tables, sub_off, x = (sA[:n_inst], Tr[:n_inst]), None, pts[:n_inst * n_per]
     out = torch.empty_like(x)
     cand = [dict(block=b, tile_pts=t, cell_sort=s) for b, t, s in
             itertools.product(CANDIDATES["block"], CANDIDATES["tile_pts"], CANDIDATES["cell_sort"])]

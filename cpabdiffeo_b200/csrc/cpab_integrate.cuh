@@ -266,33 +266,40 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
         steps_left = nT;
         sub_left = (SCHEME == SCHEME_SIMPLE) ? nT * nODE : 0;
     }
+    // FP32: two units per lane between the warp's votes (a lane whose point
+    // finishes after the first idles for the second; points finish about once
+    // in a hundred units)
+    constexpr int kUnits = sizeof(Real) == 4 ? 2 : 1;
     while (__any_sync(FULL, active)) {
         bool fin = false;
-        if (active) {
-            const bool fast = (SCHEME == SCHEME_REF) && sub_left == 0;
-            PState<DIM, Real> q;
-            advance<DIM>(fast, st, sA + c * NE, sT + c * NE, nullptr, h, q);
-            const int cq = cell_of<DIM, TESS>(t, q);
-            if (fast && cq != c) {
-                // the end point left the cell: redo the step with nStepsODE sub-steps from p
-                sub_left = nODE;
-                ++c_fb;
-            } else {
-                st = q;
-                c = cq;
-                if (fast) {
-                    --steps_left;
-                    ++c_fast;
+#pragma unroll
+        for (int u = 0; u < kUnits; ++u) {
+            if (active && !fin) {
+                const bool fast = (SCHEME == SCHEME_REF) && sub_left == 0;
+                PState<DIM, Real> q;
+                advance<DIM>(fast, st, sA + c * NE, sT + c * NE, nullptr, h, q);
+                const int cq = cell_of<DIM, TESS>(t, q);
+                if (fast && cq != c) {
+                    // the end point left the cell: redo the step with nStepsODE sub-steps from p
+                    sub_left = nODE;
+                    ++c_fb;
                 } else {
-                    --sub_left;
-                    ++c_sub;
-                    if (SCHEME == SCHEME_REF && sub_left == 0) --steps_left;
+                    st = q;
+                    c = cq;
+                    if (fast) {
+                        --steps_left;
+                        ++c_fast;
+                    } else {
+                        --sub_left;
+                        ++c_sub;
+                        if (SCHEME == SCHEME_REF && sub_left == 0) --steps_left;
+                    }
                 }
-            }
-            fin = (SCHEME == SCHEME_SIMPLE) ? (sub_left == 0) : (steps_left == 0);
-            if (fin) {
-                snk.put(idx, st);
-                ++c_pts;
+                fin = (SCHEME == SCHEME_SIMPLE) ? (sub_left == 0) : (steps_left == 0);
+                if (fin) {
+                    snk.put(idx, st);
+                    ++c_pts;
+                }
             }
         }
         unsigned done = __ballot_sync(FULL, fin);
