@@ -1,6 +1,5 @@
 // cpab_capi.cu -- the extern "C" boundary declared in include/cpab_b200.h:
 // argument validation, status codes and error strings, launch dispatch.
-#include <algorithm>
 #include <cmath>
 #include <new>
 
@@ -264,20 +263,6 @@ static IntegrateArgs make_args(cpab_ctx *ctx, const double *signedA, const doubl
     return a;
 }
 
-// Points per tile of a uniform launch: the configured tile, or a smaller one
-// (a multiple of 32, at least 64) when the launch has too few points to give
-// every SM four tiles -- a single transform of a few hundred thousand points
-// would otherwise occupy fewer SMs than the GPU has.  Results do not depend
-// on the tiling.
-static int uniform_tile_pts(int64_t total, int tile_pts)
-{
-    const int64_t want = 4 * (int64_t)num_sms();
-    if (total >= want * tile_pts) return tile_pts;
-    int64_t t = (total + want - 1) / want;
-    t = (t + 31) / 32 * 32;
-    return (int)std::max<int64_t>(64, std::min<int64_t>(t, tile_pts));
-}
-
 static int run_integrate(cpab_ctx *ctx, IntegrateArgs &a, int precision, int scheme, int64_t uniform_tiles_total,
                          cudaStream_t s)
 {
@@ -303,7 +288,7 @@ int cpab_calc_T(cpab_ctx *ctx, const double *signedA, const double *Trels, const
     a.batch.n_uniform = nPts;
     a.batch.offsets = nullptr;
     a.batch.tile_prefix = nullptr;
-    a.batch.tile_pts = uniform_tile_pts(nPts, ctx->cfg.tile_pts);
+    a.batch.tile_pts = small_launch_tile(nPts, ctx->cfg.tile_pts);
     a.batch.tiles_per_inst = (nPts + a.batch.tile_pts - 1) / a.batch.tile_pts;
     return run_integrate(ctx, a, precision, scheme, a.batch.tiles_per_inst, (cudaStream_t)stream);
 }
@@ -346,7 +331,7 @@ int cpab_calc_T_batched(cpab_ctx *ctx, const double *signedA, const double *Trel
         a.batch.tile_prefix = prefix;
     } else {
         if (n_uniform == 0) return CPAB_OK;
-        a.batch.tile_pts = uniform_tile_pts((int64_t)N * n_uniform, ctx->cfg.tile_pts);
+        a.batch.tile_pts = small_launch_tile((int64_t)N * n_uniform, ctx->cfg.tile_pts);
         a.batch.n_uniform = n_uniform;
         a.batch.tiles_per_inst = (n_uniform + a.batch.tile_pts - 1) / a.batch.tile_pts;
         uniform_tiles = a.batch.tiles_per_inst * N;

@@ -22,6 +22,23 @@ struct LaunchCfg {
 constexpr size_t kSmemOptInAbove = 40 * 1024;
 
 int num_sms();
+
+// Points per tile of a uniform integration launch over `total` points: the
+// configured tile, or a smaller one (a multiple of 32, at least 64) when the
+// launch has too few points to give every SM four tiles -- one transform of a
+// few hundred thousand points would otherwise occupy fewer SMs than the GPU
+// has.  Per-point results do not depend on the tiling.  (The likelihood
+// kernels keep the configured tile: their sums follow the tiles, and a tile
+// that depended on the batch would break "the same alone and in a batch".)
+inline int small_launch_tile(int64_t total, int tile_pts)
+{
+    const int64_t want = 4 * (int64_t)num_sms();
+    if (total >= want * tile_pts) return tile_pts;
+    int64_t t = (total + want - 1) / want;
+    t = (t + 31) / 32 * 32;
+    if (t < 64) t = 64;
+    return (int)(t < tile_pts ? t : tile_pts);
+}
 int persistent_grid_impl(const void *kern, const LaunchCfg &cfg, size_t smem);
 template <typename K>
 inline int persistent_grid(K kern, const LaunchCfg &cfg, size_t smem)
