@@ -4,6 +4,7 @@
 
 #include "cpab_ctx.h"
 #include "cpab_landmarks.h"
+#include "cpab_reduce.cuh"
 #include "cpab_register.h"
 #include "cpab_register3d.h"
 
@@ -29,6 +30,16 @@ WsLayout ws_layout(int N, int64_t tiles_per_image)
 }
 
 int64_t tiles_of(int H, int W, int tile_px) { return ((int64_t)H * W + tile_px - 1) / tile_px; }
+
+// Tile of the fused likelihood kernels over `total` pixels (voxels): the
+// small-launch rule rounded up to whole 256-point sum chunks.  Their sums do
+// not depend on the tile (finish_tile_chunks), so the tile may follow the
+// launch size.
+int likelihood_tile(int64_t total, int tile_pts)
+{
+    const int t = small_launch_tile(total, tile_pts);
+    return (t + kSumChunk - 1) / kSumChunk * kSumChunk;
+}
 
 int check_images(cpab_ctx *ctx, int N, int H, int W)
 {
@@ -100,7 +111,7 @@ int cpab_remap_ssd(cpab_ctx *ctx, const void *map, int map_precision, const floa
 size_t cpab_register_workspace_bytes(const cpab_ctx *ctx, int N, int H, int W)
 {
     if (!ctx || N < 0 || H < 1 || W < 1) return 0;
-    return ws_layout(N, tiles_of(H, W, ctx->cfg.tile_pts)).total;
+    return ws_layout(N, tiles_of(H, W, kSumChunk)).total;  // one partial per 256-pixel chunk
 }
 
 int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, int N, const float *src,
@@ -121,12 +132,12 @@ int cpab_register_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, 
     if (!(sigma > 0)) return fail(ctx, CPAB_BAD_ARG, "sigma must be positive");
     if (nTimeSteps < 1 || nStepsODE < 1) return fail(ctx, CPAB_BAD_ARG, "nTimeSteps and nStepsODE must be >= 1");
     if (!std::isfinite(dt)) return fail(ctx, CPAB_BAD_ARG, "dt is not finite");
-    const int tile_px = ctx->cfg.tile_pts;
+    const int tile_px = likelihood_tile((int64_t)N * H * W, ctx->cfg.tile_pts);
     // cell tables plus one point slot per pixel of a tile
     if (register_smem_bytes(ctx->t.nC, tile_px, precision == CPAB_F64 ? PREC_F64 : PREC_F32) >
         (size_t)max_smem_optin())
         return fail(ctx, CPAB_UNSUPPORTED, "cell tables and tile scratch exceed shared memory");
-    const WsLayout L = ws_layout(N, tiles_of(H, W, tile_px));
+    const WsLayout L = ws_layout(N, tiles_of(H, W, kSumChunk));
     if (!workspace || workspace_bytes < L.total)
         return fail(ctx, CPAB_NO_MEMORY, "workspace of %zu bytes needed", L.total);
     RegisterArgs a;
@@ -233,7 +244,7 @@ int cpab_remap3d_ssd(cpab_ctx *ctx, const void *map, int map_precision, const fl
 size_t cpab_register3d_workspace_bytes(const cpab_ctx *ctx, int N, int H, int W, int D)
 {
     if (!ctx || N < 0 || H < 1 || W < 1 || D < 1) return 0;
-    return ws_layout(N, tiles_of3(H, W, D, ctx->cfg.tile_pts)).total;
+    return ws_layout(N, tiles_of3(H, W, D, kSumChunk)).total;  // one partial per 256-voxel chunk
 }
 
 int cpab_register3d_ll(cpab_ctx *ctx, const double *signedA, const double *Trels, int N, const float *src,
@@ -257,10 +268,10 @@ int cpab_register3d_ll(cpab_ctx *ctx, const double *signedA, const double *Trels
     CPAB_CHECK_ALIGN(ctx, {signedA, 8, "signedA"}, {Trels, 8, "Trels"}, {src, 4, "src"}, {dst, 4, "dst"},
                      {ll, 8, "ll"}, {warped, 4, "warped"}, {workspace, 8, "workspace"}, {counters, 8, "counters"});
     const int prec = precision == CPAB_F64 ? PREC_F64 : PREC_F32;
-    const int tile_px = ctx->cfg.tile_pts;
+    const int tile_px = likelihood_tile((int64_t)N * H * W * D, ctx->cfg.tile_pts);
     if (register3d_smem_bytes(ctx->t.nC, tile_px, prec) > (size_t)max_smem_optin())
         return fail(ctx, CPAB_UNSUPPORTED, "cell tables and tile scratch exceed shared memory");
-    const WsLayout L = ws_layout(N, tiles_of3(H, W, D, tile_px));
+    const WsLayout L = ws_layout(N, tiles_of3(H, W, D, kSumChunk));
     if (!workspace || workspace_bytes < L.total)
         return fail(ctx, CPAB_NO_MEMORY, "workspace of %zu bytes needed", L.total);
     Register3dArgs a;

@@ -14,10 +14,12 @@
 //                   calc_T_inv), sampled from src and compared with dst, without
 //                   writing the map.
 //
-// Sums are deterministic: each tile of pixels reduces in a fixed order
-// (lanes, then warps), writes its partial, and the last tile of an image to
-// finish (atomic ticket with fences) adds that image's partials in index
-// order.  A result is therefore the same alone and inside any batch.
+// Sums are deterministic.  k_remap_ssd: each tile of pixels reduces in a
+// fixed order (lanes, then warps) and writes its partial; a second launch
+// adds each image's partials in index order.  k_register_ll: fixed 256-pixel
+// chunks (cpab_reduce.cuh finish_tile_chunks), added per image in index
+// order by the last tile to finish, so the sum does not depend on the tile
+// size either.  A result is therefore the same alone and inside any batch.
 #include <cmath>
 
 #include <math_constants.h>
@@ -421,14 +423,17 @@ __global__ void __launch_bounds__(256) k_register_ll(RegisterArgs a)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Real *sA = reinterpret_cast<Real *>(smem_raw);
     Real *sT = sA + a.t.nC * NE;
-    // the tile's point slots, after the tables (48 or 96 bytes per cell: 16-byte aligned)
+    // the tile's point slots, after the tables (48 or 96 bytes per cell: 16-byte aligned), then the
+    // 32-point group sums of the likelihood
     double2 *s_pos = reinterpret_cast<double2 *>(sA + (1 + TableLayout<Real>::kTParts) * a.t.nC * NE);
+    double *s_grp = reinterpret_cast<double *>(s_pos + a.tile_px);
     __shared__ unsigned long long s_claim;
     const int tab = a.t.nC * NE;
     const Real h = (Real)(a.dt / (double)a.nStepsODE);
     const int64_t npx = (int64_t)a.H * a.W;
     const int64_t tpi = (npx + a.tile_px - 1) / a.tile_px;
     const int64_t ntiles = tpi * a.N;
+    const int cpi = (int)((npx + kSumChunk - 1) / kSumChunk);  // chunk partials per image
     unsigned long long c_fast = 0, c_fb = 0, c_sub = 0, c_pts = 0;
     int loaded = -1;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -436,7 +441,7 @@ __global__ void __launch_bounds__(256) k_register_ll(RegisterArgs a)
         const int inst = (int)(tile / tpi);
         const int64_t kt = tile - (int64_t)inst * tpi;
         const int64_t base = (int64_t)inst * npx;
-        const int64_t j0 = kt * a.tile_px;  // first pixel of the tile in its image
+        const int64_t j0 = kt * a.tile_px;  // first pixel of the tile in its image (a multiple of kSumChunk)
         const int64_t start = base + j0;
         const int n = (int)(min(start + (int64_t)a.tile_px, base + npx) - start);
         if (inst != loaded) {
@@ -460,15 +465,17 @@ __global__ void __launch_bounds__(256) k_register_ll(RegisterArgs a)
         const float *img = a.src + base, *ref = a.dst + base;
         float *warped = a.warped ? a.warped + base : nullptr;
         const double k = -0.5 / (a.sigma * a.sigma);
-        double acc = 0.0;
+        // each pixel's term replaces the x of its slot, then the chunk-ordered sum
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
             const double2 p = s_pos[j];
             const Real w = bilinear<Real>(img, a.H, a.W, p.x * a.W - 0.5, p.y * a.H - 0.5);
             if (warped) warped[j0 + j] = (float)w;
             const double e = (double)w - (double)__ldg(ref + j0 + j);
-            acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(e, e), k));
+            s_pos[j].x = __dmul_rn(__dmul_rn(e, e), k);
         }
-        finish_tile(acc, tile, inst, (int)tpi, (int64_t)inst * tpi, a.partials, a.tickets, a.ll);
+        __syncthreads();
+        finish_tile_chunks(n, [&](int j) { return s_pos[j].x; }, s_grp, (int64_t)inst * cpi + j0 / kSumChunk, inst,
+                           (int)tpi, cpi, a.partials, a.tickets, a.ll);
     }
     if (a.counters) {
         c_fast = warp_sum_u64(c_fast);
@@ -486,7 +493,8 @@ __global__ void __launch_bounds__(256) k_register_ll(RegisterArgs a)
 
 size_t register_smem_bytes(int nC, int tile_px, int prec)
 {
-    return (size_t)nC * 6 * (prec == PREC_F64 ? 2 * 8 : 2 * 4) + (size_t)tile_px * sizeof(double2);
+    return (size_t)nC * 6 * (prec == PREC_F64 ? 2 * 8 : 2 * 4) + (size_t)tile_px * sizeof(double2) +
+           (size_t)((tile_px + 31) / 32) * sizeof(double);
 }
 
 template <int TESS, typename Real>

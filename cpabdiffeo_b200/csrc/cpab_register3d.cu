@@ -179,12 +179,14 @@ __global__ void __launch_bounds__(256) k_register3d_ll(Register3dArgs a)
     Real *sA = reinterpret_cast<Real *>(smem_raw);
     Real *sT = sA + a.t.nC * NE;
     double *s_pos = reinterpret_cast<double *>(sA + (1 + TableLayout<Real>::kTParts) * a.t.nC * NE);
+    double *s_grp = s_pos + 3 * (size_t)a.tile_px;  // 32-voxel group sums of the likelihood
     __shared__ unsigned long long s_claim;
     const int tab = a.t.nC * NE;
     const Real h = (Real)(a.dt / (double)a.nStepsODE);
     const int64_t nvx = (int64_t)a.H * a.W * a.D;
     const int64_t tpi = (nvx + a.tile_px - 1) / a.tile_px;
     const int64_t ntiles = tpi * a.N;
+    const int cpi = (int)((nvx + kSumChunk - 1) / kSumChunk);  // chunk partials per volume
     unsigned long long c_fast = 0, c_fb = 0, c_sub = 0, c_pts = 0;
     int loaded = -1;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -219,15 +221,17 @@ __global__ void __launch_bounds__(256) k_register3d_ll(Register3dArgs a)
         const float *img = a.src + base, *ref = a.dst + base;
         float *warped = a.warped ? a.warped + base : nullptr;
         const double k = -0.5 / (a.sigma * a.sigma);
-        double acc = 0.0;
+        // each voxel's term replaces the first coordinate of its slot, then the chunk-ordered sum
         for (int j = threadIdx.x; j < n; j += blockDim.x) {
-            const double *v = s_pos + 3 * j;
+            double *v = s_pos + 3 * j;
             const Real w = trilinear<Real>(img, a.H, a.W, a.D, v[0] * a.W - 0.5, v[1] * a.H - 0.5, v[2] * a.D - 0.5);
             if (warped) warped[j0 + j] = (float)w;
             const double e = (double)w - (double)__ldg(ref + j0 + j);
-            acc = __dadd_rn(acc, __dmul_rn(__dmul_rn(e, e), k));
+            v[0] = __dmul_rn(__dmul_rn(e, e), k);
         }
-        finish_tile(acc, tile, inst, (int)tpi, (int64_t)inst * tpi, a.partials, a.tickets, a.ll);
+        __syncthreads();
+        finish_tile_chunks(n, [&](int j) { return s_pos[3 * j]; }, s_grp, (int64_t)inst * cpi + j0 / kSumChunk, inst,
+                           (int)tpi, cpi, a.partials, a.tickets, a.ll);
     }
     if (a.counters) {
         c_fast = warp_sum_u64(c_fast);
@@ -265,7 +269,8 @@ cudaError_t launch_register3d_t(const Register3dArgs &a, const LaunchCfg &cfg, c
 size_t register3d_smem_bytes(int nC, int tile_px, int prec)
 {
     const size_t tables = prec == PREC_F64 ? (size_t)nC * 12 * 2 * 8 : (size_t)nC * 12 * 2 * 4;
-    return tables + (size_t)tile_px * 3 * sizeof(double);  // three doubles per voxel slot
+    // three doubles per voxel slot, then the 32-voxel group sums
+    return tables + (size_t)tile_px * 3 * sizeof(double) + (size_t)((tile_px + 31) / 32) * sizeof(double);
 }
 
 cudaError_t launch_remap3d_ssd(const Remap3dArgs &a, int map_prec, cudaStream_t s)
