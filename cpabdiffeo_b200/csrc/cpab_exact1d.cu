@@ -81,7 +81,8 @@ __device__ __forceinline__ double cf_phi(const Exact1D &e, int c, double x, doub
 // hitting time depends on (cell, direction) only.  Those are evaluated once
 // per instance with the same function (cf_crossing) into shared memory, one
 // record per (cell k, direction dir) at index 2 k + dir:
-//   te[.] = {hitting time, entry point},  cn[.] = {cell of the entry point, next cell}
+//   te[.] = {hitting time, entry point},
+//   cn[.] = {cell of the entry point, index of the next record or -1}
 // (dir 0: entered from the left, 1: from the right), so a step of the walk
 // is one 16-byte and one 8-byte load.  The results are those of evaluating
 // cf_crossing at every visit.
@@ -89,6 +90,10 @@ struct Transit {
     double2 *te;
     int2 *cn;
 };
+
+// Transit record entered when moving from cell c into cell n (from the left
+// when moving right): 2 n + dir, or -1 when there is no next cell.
+__device__ __forceinline__ int record_of(int n, int c) { return n < 0 ? -1 : 2 * n + (n > c ? 0 : 1); }
 
 __device__ void build_transit(const Exact1D &e, Transit tr)
 {
@@ -101,8 +106,8 @@ __device__ void build_transit(const Exact1D &e, Transit tr)
         const double t1 = cf_crossing(e, x1, c1, n1);
         tr.te[2 * k] = make_double2(t0, x0);
         tr.te[2 * k + 1] = make_double2(t1, x1);
-        tr.cn[2 * k] = make_int2(c0, n0);
-        tr.cn[2 * k + 1] = make_int2(c1, n1);
+        tr.cn[2 * k] = make_int2(c0, record_of(n0, c0));
+        tr.cn[2 * k + 1] = make_int2(c1, record_of(n1, c1));
     }
 }
 
@@ -125,17 +130,18 @@ __device__ bool cf_point(const Exact1D &e, const Transit &tr, double x, double t
     // first visit: general position
     int c = cf_cell(e, x_old), cn;
     double tc = cf_crossing(e, x_old, c, cn);
+    // the record of the next cell (entered at its nudged vertex, from the left when moving right)
+    int idx = record_of(cn, c);
     bool ok = true;
     // walk the transit table (cheap, divergent); the final exponential runs
     // after the loop so that all lanes of a warp evaluate it together
     for (int counter = 0;;) {
         ++visits;
         // stop when the remaining time ends inside this cell, when no further
-        // crossing exists (cn < 0), and on NaN (comparisons with NaN are false)
-        if (!(tc < t_rem) || cn < 0 || cn >= e.nC) break;
+        // crossing exists (idx -1, or any index outside the table), and on NaN
+        // (comparisons with NaN are false)
+        if (!(tc < t_rem) || (unsigned)idx >= (unsigned)(2 * e.nC)) break;
         t_rem -= tc;
-        // enter cell cn at the nudged vertex: from the left when moving right
-        const int idx = 2 * cn + (cn > c ? 0 : 1);
         const double2 te = tr.te[idx];
         if (++counter >= cap) {
             // the point would have been left at the crossing it just made
@@ -147,7 +153,7 @@ __device__ bool cf_point(const Exact1D &e, const Transit &tr, double x, double t
         x_old = te.y;
         tc = te.x;
         c = nn.x;
-        cn = nn.y;
+        idx = nn.y;
     }
     out = ok ? fmin(1.0, fmax(0.0, cf_phi(e, c, x_old, t_rem))) : x_old;
     return ok;
