@@ -222,11 +222,11 @@ def measured_peaks(torch) -> dict:
 
 # DRAM bytes per launch measured with ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum, one captured launch of the timed region):
-#  * k_exact1d on the 2048-theta case (42.7 M points): 299.7 MB, 7.01 B/point,
+#  * k_exact1d on the 2048-theta case (42.7 M points): 300.4 MB, 7.03 B/point,
 #    scaled to a launch by the points it processes;
 #  * k_integrate on the 2D 4096 x 8192-point workload: 587.9 MB per launch;
 #  * k_remap_ssd_bulk on 256 pairs of 256^2 images: 273.4 MB per launch.
-TRAFFIC_EXACT1D_BYTES_PER_POINT = 299.69e6 / 42737756
+TRAFFIC_EXACT1D_BYTES_PER_POINT = 300.43e6 / 42737756
 TRAFFIC_2D_BYTES_PER_LAUNCH = 587.94e6
 TRAFFIC_REMAP_BYTES_PER_LAUNCH = 273.43e6
 
