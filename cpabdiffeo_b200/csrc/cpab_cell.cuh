@@ -19,7 +19,7 @@
 //    division, or an exact product when inc is a power of two.
 //
 //  * fast (float): the same tessellation geometry in single precision with
-//    fused multiply-adds, for the FP32 mode whose results are judged by a
+//    fused multiply-adds, for the FP32 mode, whose results are held to a
 //    tolerance against the double-precision oracle.
 //
 // Everything is __host__ __device__ so the exact family can be checked

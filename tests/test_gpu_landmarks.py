@@ -4,7 +4,7 @@ reference's calc_T scheme), then sums -0.5 |T(src) - dst|^2 / sigma^2.
 
 Tolerances: transformed landmarks bit-exact in FP64 (same tables, same
 scheme); log-likelihoods 1e-12 relative in FP64 (the sum order differs),
-1e-6 relative in FP32 (north_star bar)."""
+1e-6 relative in FP32 (the FP32 likelihood tolerance)."""
 import numpy as np
 import pytest
 import torch
