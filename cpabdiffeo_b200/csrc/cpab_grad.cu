@@ -457,48 +457,29 @@ __device__ __forceinline__ void f32_map_adjoint(const float *M, const float *x, 
     for (int k = 0; k < DIM; ++k) g[k] = gn[k];
 }
 
-// Backwards through the nODE sub-steps of a fallback step starting at st (consumed).
+// Backwards through the nODE sub-steps of a fallback step starting at st
+// (consumed): one forward pass keeps every sub-step's point and cell in a
+// per-thread array (nODE <= 256, at most 4 KB of local memory, touched only
+// by fallback steps), then the adjoint runs down it.
 template <int DIM, int TESS>
 __device__ __forceinline__ void adjoint_substeps_f32(const Tess &t, const float *sS, double *sGS,
                                                      PState<DIM, float> &st, float *g, int nODE, float *acc,
                                                      int &acc_cell)
 {
     constexpr int NE = DIM * (DIM + 1);
-    const int ngroups = (nODE + kGroup - 1) / kGroup;
-    float starts[kGroup][2 * DIM];  // hi, lo at each group's first sub-step
-    float xs[kGroup][DIM];
-    int cs[kGroup];
+    float xs[256][DIM];
+    int cs[256];
     for (int k = 0; k < nODE; ++k) {
-        if (k % kGroup == 0) {
+        const int c = fast_cell<DIM, TESS>(t, st.x);
 #pragma unroll
-            for (int i = 0; i < DIM; ++i) {
-                starts[k / kGroup][i] = st.hi[i];
-                starts[k / kGroup][DIM + i] = st.lo[i];
-            }
-        }
-        f32_map<DIM>(st, sS + fast_cell<DIM, TESS>(t, st.x) * NE);
+        for (int i = 0; i < DIM; ++i) xs[k][i] = st.x[i];
+        cs[k] = c;
+        f32_map<DIM>(st, sS + c * NE);
     }
-    for (int gr = ngroups - 1; gr >= 0; --gr) {
-        const int k0 = gr * kGroup, k1 = min(nODE, k0 + kGroup);
-        PState<DIM, float> r;
-#pragma unroll
-        for (int i = 0; i < DIM; ++i) {
-            r.hi[i] = starts[gr][i];
-            r.lo[i] = starts[gr][DIM + i];
-            r.x[i] = r.hi[i] + r.lo[i];
-        }
-        for (int k = k0; k < k1; ++k) {
-            const int c = fast_cell<DIM, TESS>(t, r.x);
-#pragma unroll
-            for (int i = 0; i < DIM; ++i) xs[k - k0][i] = r.x[i];
-            cs[k - k0] = c;
-            f32_map<DIM>(r, sS + c * NE);
-        }
-        for (int k = k1 - 1; k >= k0; --k) {
-            const int c = cs[k - k0];
-            acc_switch_f<NE>(sGS, acc, acc_cell, c);
-            f32_map_adjoint<DIM>(sS + c * NE, xs[k - k0], g, acc);
-        }
+    for (int k = nODE - 1; k >= 0; --k) {
+        const int c = cs[k];
+        acc_switch_f<NE>(sGS, acc, acc_cell, c);
+        f32_map_adjoint<DIM>(sS + c * NE, xs[k], g, acc);
     }
 }
 
