@@ -16,8 +16,8 @@
 // Memory: positions at the start of every `ck`-th time step are kept in
 // scratch ([ceil(nT/ck), nPts, D] float64); the start of any other step is
 // recomputed from the previous checkpoint (ck = 1 stores all, ck = nT only
-// the input).  Inside a time step the sub-steps are replayed in groups of
-// kGroup from kGroup start points held in a small per-thread buffer.
+// the input).  Inside a time step the sub-steps are replayed once, keeping
+// every sub-step's start point and cell in a per-thread array.
 //
 // k_grad_ref: the same for the reference scheme (calc_T, calc_2Dto2D.cu:
 // 348-408): a time step is either the closed-form step q = T_c [p; 1] with
@@ -37,7 +37,7 @@
 
 namespace cpab {
 
-constexpr int kGroup = 16;   // sub-steps per replay group; nStepsODE <= kGroup * kGroup
+constexpr int kMaxSubsteps = 256;  // sub-steps per time step the adjoint keeps (cpab_grad_theta* check)
 
 template <int DIM, int TESS>
 __device__ __forceinline__ void substeps(const Tess &t, const double *sA, double *p, double h, int n)
@@ -68,70 +68,59 @@ __device__ __forceinline__ void acc_switch(double *sG, double *acc, int &acc_cel
 // Backwards through the nODE sub-steps of one time step that starts at q
 // (q is consumed): g = dLoss/d(end of the step) on entry, dLoss/d(start) on
 // return; dLoss/dA of the cells used is accumulated (acc / acc_cell / sG).
+// One forward pass keeps every sub-step's start point and cell in a
+// per-thread array (nODE <= 256: at most 7 KB of local memory), then the
+// adjoint runs down it.
 template <int DIM, int TESS>
 __device__ __forceinline__ void adjoint_substeps(const Tess &t, const double *sA, double *sG, double *q, double *g,
                                                  double h, int nODE, double *acc, int &acc_cell)
 {
     constexpr int NE = DIM * (DIM + 1), NH = DIM + 1;
-    const int ngroups = (nODE + kGroup - 1) / kGroup;
-    double buf1[kGroup][DIM], buf2[kGroup][DIM];
-    // group starts
+    double xs[kMaxSubsteps][DIM];
+    int cs[kMaxSubsteps];
     for (int k = 0; k < nODE; ++k) {
-        if (k % kGroup == 0) {
+        const int c = exact_cell<DIM, TESS>(t, q);
 #pragma unroll
-            for (int i = 0; i < DIM; ++i) buf1[k / kGroup][i] = q[i];
-        }
-        int c = exact_cell<DIM, TESS>(t, q);
+        for (int i = 0; i < DIM; ++i) xs[k][i] = q[i];
+        cs[k] = c;
         exact_midpoint<DIM>(q, sA + c * NE, h);
     }
-    for (int gr = ngroups - 1; gr >= 0; --gr) {
-        const int k0 = gr * kGroup, k1 = min(nODE, k0 + kGroup);
-        double r[DIM];
+    for (int k = nODE - 1; k >= 0; --k) {
+        double pk[DIM];
 #pragma unroll
-        for (int i = 0; i < DIM; ++i) r[i] = buf1[gr][i];
-        for (int k = k0; k < k1; ++k) {
+        for (int i = 0; i < DIM; ++i) pk[i] = xs[k][i];
+        const int c = cs[k];
+        const double *M = sA + c * NE;
+        acc_switch<NE>(sG, acc, acc_cell, c);
+        // recompute v and pm of the forward sub-step
+        double v[DIM], pm[DIM];
+        exact_affine<DIM>(v, M, pk);
 #pragma unroll
-            for (int i = 0; i < DIM; ++i) buf2[k - k0][i] = r[i];
-            int c = exact_cell<DIM, TESS>(t, r);
-            exact_midpoint<DIM>(r, sA + c * NE, h);
+        for (int i = 0; i < DIM; ++i) pm[i] = pk[i] + h * v[i] / 2.;
+        double av[DIM], dpm[DIM], b[DIM];
+#pragma unroll
+        for (int i = 0; i < DIM; ++i) av[i] = h * g[i];
+#pragma unroll
+        for (int jj = 0; jj < DIM; ++jj) {
+            double s2 = 0.0;
+#pragma unroll
+            for (int i = 0; i < DIM; ++i) s2 += M[i * NH + jj] * av[i];
+            dpm[jj] = s2;
         }
-        for (int k = k1 - 1; k >= k0; --k) {
-            double pk[DIM];
 #pragma unroll
-            for (int i = 0; i < DIM; ++i) pk[i] = buf2[k - k0][i];
-            const int c = exact_cell<DIM, TESS>(t, pk);
-            const double *M = sA + c * NE;
-            acc_switch<NE>(sG, acc, acc_cell, c);
-            // recompute v and pm of the forward sub-step
-            double v[DIM], pm[DIM];
-            exact_affine<DIM>(v, M, pk);
+        for (int i = 0; i < DIM; ++i) b[i] = 0.5 * h * dpm[i];
 #pragma unroll
-            for (int i = 0; i < DIM; ++i) pm[i] = pk[i] + h * v[i] / 2.;
-            double av[DIM], dpm[DIM], b[DIM];
+        for (int i = 0; i < DIM; ++i) {
 #pragma unroll
-            for (int i = 0; i < DIM; ++i) av[i] = h * g[i];
+            for (int jj = 0; jj < DIM; ++jj) acc[i * NH + jj] += av[i] * pm[jj] + b[i] * pk[jj];
+            acc[i * NH + DIM] += av[i] + b[i];
+        }
 #pragma unroll
-            for (int jj = 0; jj < DIM; ++jj) {
-                double s2 = 0.0;
+        for (int jj = 0; jj < DIM; ++jj) {
+            double s2 = 0.0;
 #pragma unroll
-                for (int i = 0; i < DIM; ++i) s2 += M[i * NH + jj] * av[i];
-                dpm[jj] = s2;
-            }
-#pragma unroll
-            for (int i = 0; i < DIM; ++i) b[i] = 0.5 * h * dpm[i];
-#pragma unroll
-            for (int i = 0; i < DIM; ++i) {
-#pragma unroll
-                for (int jj = 0; jj < DIM; ++jj) acc[i * NH + jj] += av[i] * pm[jj] + b[i] * pk[jj];
-                acc[i * NH + DIM] += av[i] + b[i];
-            }
-#pragma unroll
-            for (int jj = 0; jj < DIM; ++jj) {
-                double s2 = 0.0;
-#pragma unroll
-                for (int i = 0; i < DIM; ++i) s2 += M[i * NH + jj] * b[i];
-                g[jj] += dpm[jj] + s2;
-            }
+            for (int i = 0; i < DIM; ++i) s2 += M[i * NH + jj] * b[i];
+            g[jj] += dpm[jj] + s2;
         }
     }
 }
@@ -467,8 +456,8 @@ __device__ __forceinline__ void adjoint_substeps_f32(const Tess &t, const float 
                                                      int &acc_cell)
 {
     constexpr int NE = DIM * (DIM + 1);
-    float xs[256][DIM];
-    int cs[256];
+    float xs[kMaxSubsteps][DIM];
+    int cs[kMaxSubsteps];
     for (int k = 0; k < nODE; ++k) {
         const int c = fast_cell<DIM, TESS>(t, st.x);
 #pragma unroll
