@@ -13,7 +13,9 @@ Requests of mixed dimension, tessellation and size arrive at any time
   4. advances every running registration job by a slice of MCMC steps on a
      low-priority stream, one slice in flight per job, so registration slices
      and transform batches overlap and transform batches (high-priority
-     streams) are not queued behind long registrations.
+     streams) are not queued behind long registrations (priority orders
+     kernels: a transform batch may wait for the one likelihood launch in
+     flight, not for a job's remaining steps).
 State kept resident on the GPU: the basis of each space, every job's theta,
 log-likelihood and chain state.  Results do not depend on what else was in
 the batch: the transform kernels are per point, the likelihood reduction has
