@@ -324,7 +324,7 @@ class CpaSpace:
         return out
 
     def calc_T_batched_host(self, theta, pts_host: torch.Tensor, out_host: torch.Tensor, offsets_host,
-                            mysign: int = 1, scheme: int = _lib.SCHEME_REF, chunks: int = 8,
+                            mysign: int = 1, scheme: int = _lib.SCHEME_REF, chunks: int = 16,
                             **params_flow_int) -> torch.cuda.Event:
         """calc_T_batched for inputs and outputs in (pinned) HOST memory.
 
