@@ -66,6 +66,21 @@ def apply(space: CpaSpace, cfg: dict) -> None:
     space.set_launch(block=int(cfg["block"]), tile_pts=int(cfg["tile_pts"]), cell_sort=bool(cfg["cell_sort"]))
 
 
+def sample_extent(n_inst_total: int, n_pts_total: int, offsets, sample_points: int) -> tuple[int, int]:
+    """(instances, points) of the tuning sample: the batch's first whole
+    instances with their own points.  Ragged (offsets: host int64 [N+1]): the
+    instances up to the one whose points reach `sample_points`, and the next
+    one; N equal slices (offsets None): as many whole instances as fit in
+    `sample_points`.  At least one instance either way."""
+    if offsets is not None:
+        n_inst = int(np.searchsorted(offsets, sample_points)) + 1
+        n_inst = max(1, min(n_inst, len(offsets) - 1))
+        return n_inst, int(offsets[n_inst])
+    n_per = n_pts_total // max(1, n_inst_total)
+    n_inst = max(1, min(n_inst_total, sample_points // max(1, n_per)))
+    return n_inst, n_inst * n_per
+
+
 def tune(space: CpaSpace, tables, pts: torch.Tensor, offsets: torch.Tensor | None, scheme: int,
          sample_points: int = 4_000_000, reps: int = 3, use_cache: bool = True, **params_flow_int) -> dict:
     """Pick and apply the fastest launch shape for this batch; returns it (with its time)."""
@@ -77,18 +92,10 @@ def tune(space: CpaSpace, tables, pts: torch.Tensor, offsets: torch.Tensor | Non
             apply(space, hit)
             return hit
     sA, Tr = tables
-    if offsets is not None:
-        offs = offsets.cpu().numpy()
-        n_inst = int(np.searchsorted(offs, sample_points)) + 1
-        n_inst = max(1, min(n_inst, len(offs) - 1))
-        sub_tables = (sA[:n_inst], Tr[:n_inst])
-        sub_off = offsets[:n_inst + 1]
-        x = pts[:int(offs[n_inst])]
-    else:
-        # whole instances (the batch's own points per instance), as many as the sample holds
-        n_per = pts.shape[0] // max(1, sA.shape[0])
-        n_inst = max(1, min(sA.shape[0], sample_points // max(1, n_per)))
-        sub_tables, sub_off, x = (sA[:n_inst], Tr[:n_inst]), None, pts[:n_inst * n_per]
+    offs = offsets.cpu().numpy() if offsets is not None else None
+    n_inst, n_pts = sample_extent(sA.shape[0], pts.shape[0], offs, sample_points)
+    sub_tables, x = (sA[:n_inst], Tr[:n_inst]), pts[:n_pts]
+    sub_off = offsets[:n_inst + 1] if offsets is not None else None
     out = torch.empty_like(x)
     cand = [dict(block=b, tile_pts=t, cell_sort=s) for b, t, s in
             itertools.product(CANDIDATES["block"], CANDIDATES["tile_pts"], CANDIDATES["cell_sort"])]
