@@ -366,7 +366,8 @@ int cpab_calc_trajectory(cpab_ctx *ctx, const double *signedA, const double *Tre
 // latency-critical loop that must not pay for cudaMalloc's implicit
 // synchronisation.  For them the tile bookkeeping of a ragged batch lives in
 // this fixed array, compiled into the library.  Every GPU that loads the
-// library holds it (CPAB_NOALLOC_MAX_INSTANCES + 1 int64, 512 KiB) until the
+// library holds it (CPAB_NOALLOC_MAX_INSTANCES + 1 int64 rounded up to 256
+// bytes, about 512 KiB) until the
 // process exits.  All calls share it and it keeps the last call's contents;
 // each call rewrites every entry it reads, so nothing needs clearing, but two
 // calls whose work overlaps on the GPU (different streams, or different host
@@ -376,7 +377,11 @@ int cpab_calc_trajectory(cpab_ctx *ctx, const double *signedA, const double *Tre
 // current, on the first call made on it.
 #include <mutex>
 
-static __device__ __align__(256) int64_t g_noalloc_tile_prefix[CPAB_NOALLOC_MAX_INSTANCES + 1];
+// Sized as cpab_batched_workspace_bytes(CPAB_NOALLOC_MAX_INSTANCES): (MAX + 1)
+// int64 entries rounded up to 256 bytes, so a ragged call at exactly the
+// maximum passes the workspace-size check of cpab_calc_T_batched.
+constexpr size_t kNoallocScratchBytes = ((size_t)(CPAB_NOALLOC_MAX_INSTANCES + 1) * sizeof(int64_t) + 255) & ~(size_t)255;
+static __device__ __align__(256) int64_t g_noalloc_tile_prefix[kNoallocScratchBytes / sizeof(int64_t)];
 
 namespace {
 constexpr int kNoallocMaxDevices = 64;

@@ -66,6 +66,39 @@ def test_noalloc_matches_workspace_entry_point_twice(dim, nCs, tess, dtype):
     assert torch.equal(got2, want2)
 
 
+def test_noalloc_at_the_maximum_and_uniform():
+    """A ragged call at exactly NOALLOC_MAX_INSTANCES (most instances empty)
+    and a uniform call (offsets NULL, which needs no scratch) both equal the
+    workspace entry point."""
+    sp = CpaSpace([0.0], [1.0], (100,), device=DEV, precision=torch.float32)
+    rng = np.random.default_rng(7)
+    n = _lib.NOALLOC_MAX_INSTANCES
+    theta = Prior.create(sp.geo, 0.1, 1.0).sample(n, rng)
+    tables = sp.tables_from_theta(torch.as_tensor(theta, device=DEV), DT, 1)
+    sizes = np.zeros(n, dtype=np.int64)
+    busy = rng.choice(n, size=64, replace=False)
+    sizes[busy] = rng.integers(1, 700, size=busy.size)
+    sizes[-1] = 5                                   # the last instance is not empty
+    offs = torch.as_tensor(np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64), device=DEV)
+    x = torch.as_tensor(rng.uniform(0, 1, size=(int(sizes.sum()), 1)), dtype=torch.float32, device=DEV)
+    got = _noalloc(sp, tables, offs, x, _lib.CPAB_F32)
+    want = _with_workspace(sp, tables, offs, x, _lib.CPAB_F32)
+    torch.cuda.synchronize()
+    assert torch.equal(got, want)
+
+    sA, Tr = (t[:9].contiguous() for t in tables)
+    xu = torch.as_tensor(rng.uniform(0, 1, size=(9 * 333, 1)), dtype=torch.float32, device=DEV)
+    out = torch.full_like(xu, float("nan"))
+    c = sp._ctx
+    c.check(c.lib.cpab_calc_T_batched_noalloc(c.h, _lib.ptr(sA), _lib.ptr(Tr), _lib.ptr(xu), _lib.ptr(out), 9,
+                                              None, 333, _lib.CPAB_F32, _lib.SCHEME_REF, DT, NT, NODE, None,
+                                              _lib.stream_ptr()))
+    want_u = torch.empty_like(xu)
+    sp.calc_T_batched((sA, Tr), xu, want_u, dt=DT, nTimeSteps=NT, nStepsODEsolver=NODE)
+    torch.cuda.synchronize()
+    assert torch.equal(out, want_u)
+
+
 def test_noalloc_rejects_too_many_instances():
     sp = CpaSpace([0.0], [1.0], (100,), device=DEV, precision=torch.float32)
     c = sp._ctx
