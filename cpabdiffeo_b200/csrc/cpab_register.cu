@@ -213,12 +213,17 @@ __global__ void __launch_bounds__(256) k_remap_ssd(RemapArgs a)
 // cp.async.bulk, so the only loads the threads wait on are the source taps.
 // Same per-pixel arithmetic and per-thread order as the plain path, hence
 // the same results.  A stage whose copy does not complete within the wait
-// bound makes that image's ll NaN and leaves its warped tile unwritten.
+// bound makes that tile's partial (hence its image's ll) NaN and leaves its
+// warped tile unwritten; the CTA then issues no further copies, marks its
+// remaining tiles NaN without waiting, and before exiting waits once more
+// (bounded) for the copies it has in flight -- a copy still outstanding after
+// that second bound may land in the CTA's shared memory after it exits.
 template <typename MapT, bool FCOORD>
 __global__ void __launch_bounds__(256, 4) k_remap_ssd_bulk(RemapArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ int s_dead;  // a wait of this CTA gave up
     const int TP = a.tile_px;
     // stage s: map at s_map0 + s * 2 TP, dst at s_dst0 + s * TP
     MapT *const s_map0 = reinterpret_cast<MapT *>(smem_raw);
@@ -232,9 +237,12 @@ __global__ void __launch_bounds__(256, 4) k_remap_ssd_bulk(RemapArgs a)
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
         mbar_fence_init();
+        s_dead = 0;
     }
     __syncthreads();
+    int issued0 = 0, issued1 = 0;  // copies thread 0 issued per stage (one phase each)
     auto issue = [&](int64_t tile, int stage) {
+        if (stage) ++issued1; else ++issued0;
         const int inst = (int)(tile / tpi);
         const int64_t start = (tile - (int64_t)inst * tpi) * TP;
         const int n = (int)min((int64_t)TP, npx - start);
@@ -249,9 +257,12 @@ __global__ void __launch_bounds__(256, 4) k_remap_ssd_bulk(RemapArgs a)
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
         const int stage = it & 1;
         const uint32_t parity = (uint32_t)(it >> 1) & 1u;
+        // s_dead was last written before the previous tile's closing barrier
+        const bool dead = s_dead != 0;
         // the other stage was released by the previous iteration's closing barrier
-        if (threadIdx.x == 0 && tile + gridDim.x < ntiles) issue(tile + gridDim.x, stage ^ 1);
-        const bool ok = mbar_wait(&s_bar[stage], parity);
+        if (threadIdx.x == 0 && !dead && tile + gridDim.x < ntiles) issue(tile + gridDim.x, stage ^ 1);
+        const bool ok = !dead && mbar_wait(&s_bar[stage], parity);
+        if (!ok && !dead) s_dead = 1;
         const int inst = (int)(tile / tpi);
         const int64_t start = (tile - (int64_t)inst * tpi) * TP;
         const int n = (int)min((int64_t)TP, npx - start);
@@ -311,7 +322,13 @@ __global__ void __launch_bounds__(256, 4) k_remap_ssd_bulk(RemapArgs a)
         else
             __syncthreads();
     }
-    // every copy this CTA issued was waited for above (the last issue targets the last tile)
+    // Without a give-up every copy this CTA issued was waited for above (the
+    // last issue targets its last tile).  After one, wait (bounded) for the
+    // last phase issued to each stage before the shared memory is released.
+    if (threadIdx.x == 0 && s_dead) {
+        if (issued0) mbar_wait(&s_bar[0], (uint32_t)(issued0 - 1) & 1u);
+        if (issued1) mbar_wait(&s_bar[1], (uint32_t)(issued1 - 1) & 1u);
+    }
 }
 
 template <typename MapT, bool FCOORD>

@@ -35,9 +35,21 @@ class OracleTess(C.Structure):
                 ("inc_x", C.c_double), ("inc_y", C.c_double), ("inc_z", C.c_double)]
 
 
+def ref_root() -> Path | None:
+    """The cpabDiffeo checkout to compile oracle/_ref from: $CPAB_REF_ROOT, else
+    the checkout mounted at /root/reference in the build container; None when
+    neither exists (the GPU box uses the prebuilt oracle/_ref)."""
+    for cand in (os.environ.get("CPAB_REF_ROOT"), "/root/reference"):
+        if cand and (Path(cand) / "cpab" / "gpu" / "calc_2Dto2D.cu").exists():
+            return Path(cand)
+    return None
+
+
 def build(quiet: bool = True) -> None:
     """Run the oracle Makefile (liboracle.so; _ref only if the reference exists)."""
-    r = subprocess.run(["make", "-C", str(HERE)], capture_output=True, text=True)
+    root = ref_root()
+    args = ["make", "-C", str(HERE)] + ([f"REF_ROOT={root}"] if root else [])
+    r = subprocess.run(args, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
     if not quiet:
