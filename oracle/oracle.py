@@ -170,6 +170,33 @@ def closed_form_1d(sA, nC: int, pts, t_total: float):
     return out, int(nf)
 
 
+def cell_facets(t: OracleTess, cells) -> tuple[np.ndarray, np.ndarray]:
+    """Facets of every cell (cpab_oracle_exact.c): ([nC, nF, dim+1] rows
+    (outward unit normal, -offset), [nC, nF] neighbour cell or -1)."""
+    cells = _c64(cells)
+    nC, nV, nh = cells.shape
+    nF = nh if (nV == nh and t.dim > 1) else 2 * t.dim
+    F = np.empty((nC, nF, nh))
+    nb = np.empty((nC, nF), dtype=np.int32)
+    got = lib().oracle_cell_facets(C.byref(t), _d(cells), C.c_int(nV), _d(F), nb.ctypes.data_as(_ip))
+    assert got == nF
+    return F, nb
+
+
+def calc_T_exact(t: OracleTess, Trels, sA, facets, nbr, pts, dt, nT, nODE):
+    """EXACT scheme (hitting times; cpab_oracle_exact.c). Returns (out, counters[4]):
+    steps kept, steps with an exit, facet crossings, fallbacks."""
+    pts = _c64(pts)
+    out = np.empty_like(pts)
+    cnt = np.zeros(4, dtype=np.int64)
+    F = _c64(facets)
+    nb = np.ascontiguousarray(nbr, dtype=np.int32)
+    lib().oracle_calc_T_exact(C.byref(t), _d(_c64(Trels)), _d(_c64(sA)), _d(F), nb.ctypes.data_as(_ip),
+                              C.c_int(F.shape[1]), _d(pts), _d(out), C.c_int64(pts.shape[0]), C.c_double(dt),
+                              C.c_int(nT), C.c_int(nODE), cnt.ctypes.data_as(C.POINTER(C.c_int64)))
+    return out, cnt
+
+
 def clamp_1d(x, lo=0.0, hi=1.0):
     """threshold_krnl (cpab/cpaNd/_CpaSpace.py:35-43)."""
     y = np.array(x, dtype=np.float64, copy=True)
