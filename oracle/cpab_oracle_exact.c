@@ -11,36 +11,36 @@
  * expm(dt A_c) while a step's end stays in the start cell and otherwise
  * re-integrates the step with nStepsODE explicit-midpoint sub-steps
  * (calc_2Dto2D.cu:167-197).  The EXACT scheme keeps the closed-form step
- * and the same keep test, and replaces the midpoint fallback by the flow
- * itself:
+ * and its keep test, and re-integrates a step that leaves its cell with
+ * nStepsODE sub-steps of the exact flow, S_c = expm(h A_c), h = dt/nStepsODE:
  *
- *   inside cell c the flow is x(t) = expm(t A_c)[p; 1]; the time at which it
- *   leaves the cell through an interior facet k (outward unit normal n_k,
- *   offset h_k: n_k . x <= h_k inside) is the first root of
- *   g_k(t) = n_k . x(t) - h_k.  The remaining time s of the step is
- *   sampled at s/4, s/2, 3s/4 and s; the first sample outside an interior
- *   facet brackets the exit, a safeguarded Newton iteration
- *   (g_k' = n_k . v_c(x(t))) finds the root of every violated facet, and
- *   the earliest one is the exit time tau.  The point moves to x(tau), the
- *   cell becomes the facet's neighbour, s -= tau, and the step continues.
- *   Facets on the domain boundary never exit (the velocity's normal
- *   component vanishes there).
+ *   a sub-step whose end stays in the cell is kept; one whose end leaves it
+ *   brackets the exit.  Inside cell c the flow is x(t) = expm(t A_c)[p; 1];
+ *   it leaves through an interior facet k (outward unit normal n_k, offset
+ *   h_k: n_k . x <= h_k inside) at the first root of
+ *   g_k(t) = n_k . x(t) - h_k.  For every interior facet the sub-step's end
+ *   violates, a safeguarded Newton iteration (g_k' = n_k . v_c(x(t))) finds
+ *   the root in [0, h]; the earliest is the exit time tau.  The point moves
+ *   to x(tau), the cell becomes the facet's neighbour, and the rest of the
+ *   sub-step (h - tau) is the neighbour's flow, exiting again if its end
+ *   leaves that cell.  Facets on the domain boundary never exit (the
+ *   velocity's normal component vanishes there).
  *
- * x(t) is evaluated as the action of the exponential on [p; 1] by its
+ * x(t) for arbitrary t is the action of the exponential on [p; 1] by its
  * Taylor series, x(t) = p + sum_k w_k with w_1 = t (L p + b),
  * w_k = (t / k) L w_{k-1} (A = [L | b]), until the terms fall below the
- * rounding of the sum -- t never exceeds dt here.
+ * rounding of the sum (t <= h).
  *
- * Fallback (the nStepsODE fallback): when a step needs more than
- * 4 nC + 16 crossings (a point trapped on an edge or corner by rounding)
- * or a root comes out NaN, the rest of that step is integrated with the
- * reference's midpoint sub-steps of length dt / nStepsODE.
+ * Fallback: when no interior facet explains a sub-step's exit (a point on
+ * the domain boundary) or more than 4 nC + 16 crossings occur in one
+ * sub-step, the sub-step's end point is kept, as in the reference scheme.
  *
  * Counters: [0] closed-form steps kept, [1] steps with an exit,
  * [2] facet crossings, [3] fallbacks.
  */
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 typedef struct {
@@ -52,7 +52,6 @@ typedef struct {
 
 int oracle_cell_idx(const oracle_tess *t, const double *p);
 
-#define EX_NB 4            /* bracketing samples per remaining step */
 #define EX_MAX_NEWTON 100
 #define EX_MAX_TAYLOR 60
 
@@ -192,15 +191,6 @@ static inline double facet_dg(int dim, const double *F, const double *A, const d
     return d;
 }
 
-/* Inside cell c as far as its interior facets go (index of the first
- * violated interior facet, or -1). */
-static int first_violated(int dim, const double *Fc, const int *nb, int nF, const double *x)
-{
-    for (int k = 0; k < nF; ++k)
-        if (nb[k] >= 0 && facet_g(dim, Fc + k * (dim + 1), x) > 0) return k;
-    return -1;
-}
-
 /* Root of g(t) = n . x(t) - h in [lo, hi], g(lo) <= 0 < g(hi). */
 static double facet_root(int dim, const double *A, const double *F, const double *p, double lo, double hi,
                          double glo, double ghi)
@@ -232,31 +222,94 @@ static inline void affine3(int dim, const double *A, const double *x, double *y)
     }
 }
 
-/* The reference's midpoint sub-steps (solveODE, calc_2Dto2D.cu:167-197) for
- * the remaining time s of a step, in sub-steps of about h. */
-static void midpoint_rest(const oracle_tess *t, const double *As, double *p, double s, double h)
+/* S = expm(h A) of a cell's affine matrix (homogeneous, bottom row 0), as
+ * the DIM x (DIM+1) top block, by its Taylor series. */
+static void expm_sub(int dim, const double *A, double h, double *S)
 {
-    const int dim = t->dim, ne = dim * (dim + 1);
-    int n = (int)ceil(s / h - 1e-9);
-    if (n < 1) n = 1;
-    const double hs = s / n;
-    double v[3], pm[3];
-    for (int k = 0; k < n; ++k) {
-        const int c = oracle_cell_idx(t, p);
-        affine3(dim, As + (size_t)c * ne, p, v);
-        for (int i = 0; i < dim; ++i) pm[i] = p[i] + hs * v[i] / 2.;
-        affine3(dim, As + (size_t)c * ne, pm, v);
-        for (int i = 0; i < dim; ++i) p[i] += v[i] * hs;
+    const int nh = dim + 1;
+    double P[12], Q[12];
+    for (int i = 0; i < dim * nh; ++i) {
+        P[i] = h * A[i];
+        S[i] = P[i];
+    }
+    for (int k = 2; k <= EX_MAX_TAYLOR; ++k) {
+        double big = 0;
+        for (int i = 0; i < dim; ++i)
+            for (int j = 0; j < nh; ++j) {
+                double v = 0;
+                for (int m = 0; m < dim; ++m) v += h * A[i * nh + m] * P[m * nh + j];
+                Q[i * nh + j] = v / k;
+            }
+        for (int i = 0; i < dim * nh; ++i) {
+            P[i] = Q[i];
+            S[i] += P[i];
+            big = fmax(big, fabs(P[i]));
+        }
+        if (big <= 1e-18) break;
+    }
+    for (int i = 0; i < dim; ++i) S[i * nh + i] += 1.0;
+}
+
+/* The exact flow over one sub-step of length h from p in cell c whose end
+ * point (q, from the cell's sub-step map) left the cell: exit times through
+ * interior facets, the neighbour across the exited facet, the rest of the
+ * sub-step there (again exiting if its end leaves that cell).  p becomes the
+ * point at the sub-step's end; returns its cell. */
+static int exact_substep_crossing(const oracle_tess *t, const double *As, const double *facets, const int *nbr,
+                                  int nF, int c, double *p, const double *q, double h, int cap, int64_t *cnt)
+{
+    const int dim = t->dim, nh = dim + 1, ne = dim * nh;
+    double y[3];
+    double s = h;
+    memcpy(y, q, sizeof(double) * dim);
+    for (int crossings = 0;; ) {
+        if (oracle_cell_idx(t, y) == c) {
+            memcpy(p, y, sizeof(double) * dim);
+            return c;
+        }
+        const double *A = As + (size_t)c * ne;
+        const double *Fc = facets + (size_t)c * nF * nh;
+        const int *nb = nbr + c * nF;
+        double tau = s;
+        int kbest = -1;
+        for (int k = 0; k < nF; ++k) {
+            if (nb[k] < 0) continue;
+            const double *F = Fc + k * nh;
+            const double ghi = facet_g(dim, F, y);
+            if (!(ghi > 0)) continue;
+            const double glo = facet_g(dim, F, p);
+            const double r = (glo >= 0) ? 0.0 : facet_root(dim, A, F, p, 0.0, s, glo, ghi);
+            if (kbest < 0 || r < tau) {
+                tau = r;
+                kbest = k;
+            }
+        }
+        if (kbest < 0 || !(tau == tau) || ++crossings > cap) {
+            /* no interior facet explains the exit (or too many crossings):
+             * keep the sub-step's end point, as the reference scheme does */
+            memcpy(p, y, sizeof(double) * dim);
+            ++cnt[3];
+            return oracle_cell_idx(t, p);
+        }
+        double z[3];
+        expmv(dim, A, p, tau, z);
+        memcpy(p, z, sizeof(double) * dim);
+        s -= tau;
+        c = nb[kbest];
+        ++cnt[2];
+        if (!(s > 0)) return c;
+        expmv(dim, As + (size_t)c * ne, p, s, y);
     }
 }
 
-static void exact_point(const oracle_tess *t, const double *Trels, const double *As, const double *facets,
-                        const int *nbr, int nF, double *p, double dt, int nT, int nODE, int64_t *cnt)
+static void exact_point(const oracle_tess *t, const double *Trels, const double *As, const double *Ss,
+                        const double *facets, const int *nbr, int nF, double *p, double dt, int nT, int nODE,
+                        int64_t *cnt)
 {
     const int dim = t->dim, nh = dim + 1, ne = dim * nh;
     const int cap = 4 * n_cells(t) + 16;
     const double h = dt / (double)nODE;
-    double q[3], y[3], ys[EX_NB + 1][3];
+    double q[3];
     for (int step = 0; step < nT; ++step) {
         int c = oracle_cell_idx(t, p);
         affine3(dim, Trels + (size_t)c * ne, p, q);
@@ -266,57 +319,15 @@ static void exact_point(const oracle_tess *t, const double *Trels, const double 
             continue;
         }
         ++cnt[1];
-        double s = dt;
-        int crossings = 0;
-        for (;;) {
-            const double *A = As + (size_t)c * ne;
-            const double *Fc = facets + (size_t)c * nF * nh;
-            const int *nb = nbr + c * nF;
-            /* samples of the remaining time: the first one outside brackets the exit */
-            double lo = 0.0, hi = s;
-            int j_out = -1;
-            memcpy(ys[0], p, sizeof(double) * dim);
-            for (int j = 1; j <= EX_NB; ++j) {
-                const double tj = (j == EX_NB) ? s : s * j / EX_NB;
-                expmv(dim, A, p, tj, ys[j]);
-                if (first_violated(dim, Fc, nb, nF, ys[j]) >= 0) {
-                    j_out = j;
-                    hi = tj;
-                    break;
-                }
-                lo = tj;
+        /* the step again in nStepsODE sub-steps of the exact flow; a sub-step
+         * whose end leaves its cell is resolved at the exit times */
+        for (int k = 0; k < nODE; ++k) {
+            affine3(dim, Ss + (size_t)c * ne, p, q);
+            if (oracle_cell_idx(t, q) == c) {
+                memcpy(p, q, sizeof(double) * dim);
+                continue;
             }
-            if (j_out < 0) {  /* stays in c for the rest of the step */
-                memcpy(p, ys[EX_NB], sizeof(double) * dim);
-                break;
-            }
-            double tau = hi;
-            int kbest = -1;
-            for (int k = 0; k < nF; ++k) {
-                if (nb[k] < 0) continue;
-                const double *F = Fc + k * nh;
-                const double ghi = facet_g(dim, F, ys[j_out]);
-                if (!(ghi > 0)) continue;
-                double glo = facet_g(dim, F, ys[j_out - 1]);
-                double r;
-                if (glo >= 0) r = lo;  /* already on (or past) the facet at lo */
-                else r = facet_root(dim, A, F, p, lo, hi, glo, ghi);
-                if (kbest < 0 || r < tau) {
-                    tau = r;
-                    kbest = k;
-                }
-            }
-            if (kbest < 0 || !(tau == tau) || ++crossings > cap) {
-                midpoint_rest(t, As, p, s, h);
-                ++cnt[3];
-                break;
-            }
-            expmv(dim, A, p, tau, y);
-            memcpy(p, y, sizeof(double) * dim);
-            s -= tau;
-            c = nb[kbest];
-            ++cnt[2];
-            if (!(s > 0)) break;
+            c = exact_substep_crossing(t, As, facets, nbr, nF, c, p, q, h, cap, cnt);
         }
     }
 }
@@ -327,17 +338,21 @@ void oracle_calc_T_exact(const oracle_tess *t, const double *Trels, const double
                          const int *nbr, int nF, const double *pts, double *out, int64_t n, double dt,
                          int nTimeSteps, int nStepsODE, int64_t *counters)
 {
-    const int dim = t->dim;
+    const int dim = t->dim, ne = dim * (dim + 1), nC = n_cells(t);
+    double *Ss = (double *)malloc(sizeof(double) * (size_t)nC * ne);
+    if (!Ss) return;
+    for (int c = 0; c < nC; ++c) expm_sub(dim, As + (size_t)c * ne, dt / (double)nStepsODE, Ss + (size_t)c * ne);
     int64_t c0 = 0, c1 = 0, c2 = 0, c3 = 0;
     #pragma omp parallel for schedule(dynamic, 64) reduction(+:c0, c1, c2, c3)
     for (int64_t i = 0; i < n; ++i) {
         double p[3];
         int64_t cnt[4] = {0, 0, 0, 0};
         for (int k = 0; k < dim; ++k) p[k] = pts[i * dim + k];
-        exact_point(t, Trels, As, facets, nbr, nF, p, dt, nTimeSteps, nStepsODE, cnt);
+        exact_point(t, Trels, As, Ss, facets, nbr, nF, p, dt, nTimeSteps, nStepsODE, cnt);
         for (int k = 0; k < dim; ++k) out[i * dim + k] = p[k];
         c0 += cnt[0]; c1 += cnt[1]; c2 += cnt[2]; c3 += cnt[3];
     }
+    free(Ss);
     if (counters) {
         counters[0] += c0; counters[1] += c1; counters[2] += c2; counters[3] += c3;
     }
