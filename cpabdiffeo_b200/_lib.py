@@ -19,7 +19,8 @@ STATUS_NAMES = {
 }
 CPAB_F64, CPAB_F32 = 0, 1
 SCHEME_REF, SCHEME_SIMPLE, SCHEME_EXACT = 0, 1, 2
-CNT_FAST, CNT_FALLBACK, CNT_SUBSTEPS, CNT_POINTS, CNT_FAILED, CNT_NAN, CNT_CANCELLED, CNT_N = 0, 1, 2, 3, 4, 5, 6, 7
+CNT_FAST, CNT_FALLBACK, CNT_SUBSTEPS, CNT_POINTS, CNT_FAILED, CNT_NAN, CNT_CANCELLED, CNT_CROSSINGS, CNT_N = (
+    0, 1, 2, 3, 4, 5, 6, 7, 8)
 
 
 class CpabLibraryError(RuntimeError):
@@ -37,6 +38,7 @@ _vp, _i, _i64, _d, _sz = C.c_void_p, C.c_int, C.c_int64, C.c_double, C.c_size_t
 SIGNATURES = {
     "cpab_ctx_create": (_i, [C.POINTER(_vp), _i, _i, C.POINTER(_i), C.POINTER(_d)]),
     "cpab_ctx_destroy": (_i, [_vp]),
+    "cpab_tess_facets": (_i, [_i, _i, C.POINTER(_i), C.POINTER(_d), _vp, _vp, C.POINTER(_i)]),
     "cpab_last_error_string": (C.c_char_p, [_vp]),
     "cpab_ctx_num_cells": (_i, [_vp]),
     "cpab_ctx_cell_len": (_i, [_vp]),
@@ -46,6 +48,7 @@ SIGNATURES = {
     "cpab_cancel_requested": (_i, [_vp]),
     "cpab_set_launch": (_i, [_vp, _i, _i, _i]),
     "cpab_set_cell_sort": (_i, [_vp, _i]),
+    "cpab_set_max_ctas": (_i, [_vp, _i]),
     "cpab_expm": (_i, [_vp, _vp, _i, _d, _i, _vp, _vp, _vp]),
     "cpab_theta_to_trels": (_i, [_vp, _vp, _i, _vp, _i, _d, _i, _vp, _vp, _vp, _vp]),
     "cpab_calc_cell_idx": (_i, [_vp, _vp, _vp, _i64, _vp]),

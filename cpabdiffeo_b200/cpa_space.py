@@ -243,10 +243,11 @@ class CpaSpace:
         return self._calc_T(pat, pts, mysign, out, scheme=_lib.SCHEME_SIMPLE, **params_flow_int)
 
     def calc_T_exact(self, pat=None, pts=None, mysign=1, out=None, **params_flow_int):
-        """Closed-form 1D flow across cells for time dt*nTimeSteps
-        (cpab/cpa1d/calcs/ClosedFormInt.py:64-165)."""
-        if self.dim != 1:
-            raise NotImplementedError("the exact scheme is built for 1D spaces")
+        """The flow for time dt*nTimeSteps with cell-boundary hitting times:
+        in 1D the closed form (cpab/cpa1d/calcs/ClosedFormInt.py:64-165); in
+        2D/3D the reference's closed-form steps, with a step that leaves its
+        cell re-integrated in nStepsODE sub-steps of the exact flow whose
+        exits are resolved at the facet hitting times."""
         return self._calc_T(pat, pts, mysign, out, scheme=_lib.SCHEME_EXACT, **params_flow_int)
 
     def calc_trajectory(self, pat=None, pts=None, mysign=1, **params_flow_int) -> torch.Tensor:
@@ -267,14 +268,23 @@ class CpaSpace:
         return traj
 
     # ------------------------------------------------------------------ batches
-    def tables_from_theta(self, theta: torch.Tensor, dt: float, mysign: int = 1, A_out: torch.Tensor | None = None):
-        """signed A and Trel for a batch theta [N, d] (one fused launch)."""
+    def tables_from_theta(self, theta: torch.Tensor, dt: float, mysign: int = 1, A_out: torch.Tensor | None = None,
+                          out: tuple | None = None):
+        """signed A and Trel for a batch theta [N, d] (one fused launch);
+        written into out = (sA, Tr) ([N, D] float64 CUDA) when given."""
         th = theta.to(device=self.device, dtype=torch.float64).contiguous()
         if th.ndim != 2 or th.shape[1] != self.d:
             raise ValueError(th.shape)
         N = th.shape[0]
-        sA = torch.empty((N, self.D), dtype=torch.float64, device=self.device)
-        Tr = torch.empty_like(sA)
+        if out is None:
+            sA = torch.empty((N, self.D), dtype=torch.float64, device=self.device)
+            Tr = torch.empty_like(sA)
+        else:
+            sA, Tr = out
+            for t in (sA, Tr):
+                if t.shape != (N, self.D) or t.dtype != torch.float64 or not t.is_contiguous() or \
+                        t.device != self.device:
+                    raise ValueError("out must be two contiguous float64 [N, D] tensors on the space's device")
         c = self._ctx
         c.check(c.lib.cpab_theta_to_trels(c.h, _lib.ptr(self.B), self.d, _lib.ptr(th), N, float(dt), int(mysign),
                                           _lib.ptr(A_out), _lib.ptr(sA), _lib.ptr(Tr), _lib.stream_ptr()))
@@ -323,15 +333,31 @@ class CpaSpace:
                                           scheme, dt, nT, nODE, _lib.ptr(counters), _lib.stream_ptr()))
         return out
 
+    def capture_batched(self, n_theta: int, pts: torch.Tensor, out: torch.Tensor,
+                        offsets: torch.Tensor | None = None, mysign: int = 1, scheme: int = _lib.SCHEME_REF,
+                        counters: torch.Tensor | None = None, **params_flow_int) -> "BatchedStep":
+        """One batched step -- theta [n_theta, d] -> A = B theta -> expm ->
+        integration of every instance's points -- captured in a CUDA graph
+        (replaces the reference's per-call launch path, cpab/gpu/Calcs.py:454-624,
+        for a batch whose shapes repeat).  pts, out, offsets and counters are
+        the graph's fixed buffers: refill them in place between replays."""
+        return BatchedStep(self, n_theta, pts, out, offsets, mysign, scheme, counters, **params_flow_int)
+
     def calc_T_batched_host(self, theta, pts_host: torch.Tensor, out_host: torch.Tensor, offsets_host,
                             mysign: int = 1, scheme: int = _lib.SCHEME_REF, chunks: int = 16,
                             **params_flow_int) -> torch.cuda.Event:
         """calc_T_batched for inputs and outputs in (pinned) HOST memory.
 
-        The batch is cut into `chunks` contiguous groups of instances with about
-        equal point counts; group k+1 is copied in while group k is integrated
-        and group k-1 is copied out (three streams, three device buffers, so
-        no stage waits for a buffer while the other two are busy).
+        The batch is cut into `chunks` contiguous groups of instances; group
+        k+1 is copied in while group k is integrated and group k-1 is copied
+        out (three streams, three device buffers).  The first two and last two
+        groups carry 1/4 and 1/2 of an inner group's points, so the copy-in
+        before the first integration and the copy-out after the last one --
+        the stretches where the host link carries one direction only -- are
+        short.  The device buffers belong to the space and are reused by the
+        next call once their previous contents are copied out (events); every
+        tensor used on a side stream is recorded on it, so freeing or growing
+        a buffer never hands memory in use to another allocation.
         theta: [N, d] (host or device); offsets_host: int64 [N+1] (host).
         Returns an event recorded on the current stream once out_host is
         complete; the current stream waits for it."""
@@ -342,38 +368,46 @@ class CpaSpace:
         cur = torch.cuda.current_stream(dev)
         if not hasattr(self, "_pipe_streams"):
             self._pipe_streams = [torch.cuda.Stream(device=dev) for _ in range(3)]
+            self._pipe_pool = []
         s_in, s_cmp, s_out = self._pipe_streams
         th = torch.as_tensor(theta, dtype=torch.float64)
         th = th.pin_memory().to(dev, non_blocking=True) if th.device.type == "cpu" else th.to(dev)
         tables = self.tables_from_theta(th, dt, mysign)
+        for t in tables:
+            t.record_stream(s_cmp)
         ev_tables = torch.cuda.Event()
         ev_tables.record(cur)
         total = int(offs[-1])
         chunks = max(1, min(int(chunks), N))
-        # instance boundaries with about total/chunks points each
-        cuts = np.searchsorted(offs, np.linspace(0, total, chunks + 1)[1:-1])
-        bounds = np.unique(np.concatenate([[0], cuts, [N]]))
-        groups = [(int(a), int(b)) for a, b in zip(bounds[:-1], bounds[1:]) if b > a]
+        groups = _pipeline_groups(offs, chunks)
         maxpts = max(int(offs[b] - offs[a]) for a, b in groups)
         dim = self.dim
         dt_ = pts_host.dtype
-        bufs = []
         nbuf = min(3, len(groups))
-        for _ in range(nbuf):
-            bufs.append(dict(x=torch.empty((maxpts, dim), dtype=dt_, device=dev),
-                             o=torch.empty((maxpts, dim), dtype=dt_, device=dev),
-                             off=torch.empty(len(offs), dtype=torch.int64, device=dev),
-                             ws=torch.empty(int(self._ctx.lib.cpab_batched_workspace_bytes(N)) + 256,
-                                            dtype=torch.uint8, device=dev),
-                             ev_free=None))
+        ws_need = int(self._ctx.lib.cpab_batched_workspace_bytes(N)) + 256
+        pool = self._pipe_pool
+        for i in range(nbuf):
+            buf = pool[i] if i < len(pool) else None
+            if buf is None or buf["x"].dtype != dt_ or buf["x"].shape[0] < maxpts or buf["x"].shape[1] != dim or \
+                    buf["off"].numel() < len(offs) or buf["ws"].numel() < ws_need:
+                # the old buffers were recorded on the streams that used them: freeing is safe
+                buf = dict(x=torch.empty((maxpts, dim), dtype=dt_, device=dev),
+                           o=torch.empty((maxpts, dim), dtype=dt_, device=dev),
+                           off=torch.empty(len(offs), dtype=torch.int64, device=dev),
+                           ws=torch.empty(ws_need, dtype=torch.uint8, device=dev),
+                           ev_free=buf["ev_free"] if buf is not None else None)
+                if i < len(pool):
+                    pool[i] = buf
+                else:
+                    pool.append(buf)
         off_pin = torch.empty((len(groups), len(offs)), dtype=torch.int64).pin_memory()
         ev_last = None
         for k, (a, b) in enumerate(groups):
-            buf = bufs[k % nbuf]
+            buf = pool[k % nbuf]
             o0, o1 = int(offs[a]), int(offs[b])
             n = o1 - o0
             off_pin[k, :b - a + 1] = torch.from_numpy(offs[a:b + 1] - o0)
-            if buf["ev_free"] is not None:
+            if buf["ev_free"] is not None:          # its previous group (this call or the last) is copied out
                 s_in.wait_event(buf["ev_free"])
             with torch.cuda.stream(s_in):
                 buf["x"][:n].copy_(pts_host[o0:o1], non_blocking=True)
@@ -392,11 +426,12 @@ class CpaSpace:
                 out_host[o0:o1].copy_(buf["o"][:n], non_blocking=True)
                 ev_o = torch.cuda.Event()
                 ev_o.record(s_out)
+            for key, st in (("x", s_in), ("off", s_in), ("x", s_cmp), ("o", s_cmp), ("off", s_cmp), ("ws", s_cmp),
+                            ("o", s_out)):
+                buf[key].record_stream(st)
             buf["ev_free"] = ev_o
             ev_last = ev_o
         cur.wait_event(ev_last)
-        # keep the device buffers alive until the copies are done
-        self._pipe_keep = (bufs, tables, th, off_pin)
         done = torch.cuda.Event()
         done.record(cur)
         return done
@@ -410,11 +445,85 @@ class CpaSpace:
         c = self._ctx
         c.check(c.lib.cpab_clear_cancel(c.h))
 
-    def set_launch(self, block: int = 0, ctas_per_sm: int = 0, tile_pts: int = 0, cell_sort: bool | None = None) -> None:
+    def set_launch(self, block: int = 0, ctas_per_sm: int = 0, tile_pts: int = 0, cell_sort: bool | None = None,
+                   max_ctas: int | None = None) -> None:
         c = self._ctx
         c.check(c.lib.cpab_set_launch(c.h, block, ctas_per_sm, tile_pts))
         if cell_sort is not None:
             c.check(c.lib.cpab_set_cell_sort(c.h, int(bool(cell_sort))))
+        if max_ctas is not None:
+            c.check(c.lib.cpab_set_max_ctas(c.h, int(max_ctas)))
 
     def __repr__(self) -> str:
         return self.geo.subspace_string
+
+
+def _pipeline_groups(offs: np.ndarray, chunks: int) -> list[tuple[int, int]]:
+    """Contiguous instance groups [a, b) for the host-buffer pipeline: point
+    counts in the proportions 1/4, 1/2, 1, ..., 1, 1/2, 1/4 (equal when there
+    are fewer than six groups), cut at instance boundaries; empty groups are
+    dropped."""
+    N = offs.size - 1
+    total = int(offs[-1])
+    w = np.ones(chunks)
+    if chunks >= 6:
+        w[[0, -1]] = 0.25
+        w[[1, -2]] = 0.5
+    frac = np.cumsum(w)[:-1] / w.sum()
+    cuts = np.searchsorted(offs, frac * total)
+    bounds = np.unique(np.concatenate([[0], cuts, [N]]))
+    return [(int(a), int(b)) for a, b in zip(bounds[:-1], bounds[1:]) if b > a]
+
+
+class BatchedStep:
+    """A batched transform step replayed from a CUDA graph.
+
+    The graph holds the three launches of a step -- the fused
+    theta -> A -> expm prologue, the ragged batch's tile prefix and the
+    persistent integration kernel -- on fixed buffers: `theta` (owned here,
+    [n_theta, d] float64), the caller's `pts`, `out`, `offsets` and
+    `counters`, and an owned workspace and table pair.  Construction runs the
+    step once eagerly (kernel attributes, launch shapes) and captures it on a
+    side stream; `__call__` replays it on the current stream.  The launch
+    shape (CpaSpace.set_launch / the autotuner) is fixed at capture."""
+
+    def __init__(self, space: CpaSpace, n_theta: int, pts: torch.Tensor, out: torch.Tensor,
+                 offsets: torch.Tensor | None, mysign: int, scheme: int, counters: torch.Tensor | None,
+                 **params_flow_int):
+        self.space = space
+        dev = space.device
+        self.dt, self.nT, self.nODE = space._flow(params_flow_int)
+        self.params = dict(dt=self.dt, nTimeSteps=self.nT, nStepsODEsolver=self.nODE)
+        self.mysign, self.scheme = int(mysign), int(scheme)
+        self.pts, self.out, self.offsets, self.counters = pts, out, offsets, counters
+        self.theta = torch.zeros((n_theta, space.d), dtype=torch.float64, device=dev)
+        self.tables = (torch.empty((n_theta, space.D), dtype=torch.float64, device=dev),
+                       torch.empty((n_theta, space.D), dtype=torch.float64, device=dev))
+        ws_bytes = int(space._ctx.lib.cpab_batched_workspace_bytes(n_theta)) if offsets is not None else 0
+        self.workspace = torch.empty(max(ws_bytes, 256), dtype=torch.uint8, device=dev)
+        self._launches()                      # eager: sets kernel attributes before capture
+        torch.cuda.current_stream(dev).synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream(device=dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            self.graph.capture_begin(capture_error_mode="thread_local")
+            try:
+                self._launches()
+            finally:
+                self.graph.capture_end()
+        torch.cuda.current_stream(dev).wait_stream(side)
+
+    def _launches(self) -> None:
+        sp = self.space
+        sp.tables_from_theta(self.theta, self.dt, self.mysign, out=self.tables)
+        sp.calc_T_batched(self.tables, self.pts, self.out, offsets=self.offsets, scheme=self.scheme,
+                          counters=self.counters, workspace=self.workspace, **self.params)
+
+    def __call__(self, theta: torch.Tensor | None = None) -> torch.Tensor:
+        """Replay the step (after copying `theta` into the graph's buffer when
+        given); returns `out`."""
+        if theta is not None:
+            self.theta.copy_(torch.as_tensor(theta, dtype=torch.float64), non_blocking=True)
+        self.graph.replay()
+        return self.out

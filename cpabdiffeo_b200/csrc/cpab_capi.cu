@@ -66,6 +66,24 @@ int cpab_ctx_create(cpab_ctx **out, int dim, int tess, const int *nCs, const dou
         if (h) cudaFreeHost(h);
         if (st) cudaStreamDestroy(st);
         if (!c->cancel_dev) c->device = -1;
+        // facet tables of the 2D/3D exact scheme
+        if (c->device >= 0 && dim >= 2) {
+            std::vector<double> F;
+            std::vector<int> nb;
+            const int nF = build_facets(c->t, c->nCs, F, nb);
+            void *fd = nullptr, *nd = nullptr;
+            if (cudaMalloc(&fd, F.size() * sizeof(double)) == cudaSuccess &&
+                cudaMalloc(&nd, nb.size() * sizeof(int)) == cudaSuccess &&
+                cudaMemcpy(fd, F.data(), F.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+                cudaMemcpy(nd, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess) {
+                c->facets_dev = static_cast<double *>(fd);
+                c->nbr_dev = static_cast<int *>(nd);
+                c->nF = nF;
+                fd = nd = nullptr;
+            }
+            if (fd) cudaFree(fd);
+            if (nd) cudaFree(nd);
+        }
     }
     cudaGetLastError();  // a missing device is not an error here
     *out = c;
@@ -82,6 +100,8 @@ int cpab_ctx_destroy(cpab_ctx *ctx)
         cudaStreamDestroy(ctx->cancel_stream);
         cudaFree(ctx->cancel_dev);
         cudaFreeHost(ctx->cancel_src);
+        if (ctx->facets_dev) cudaFree(ctx->facets_dev);
+        if (ctx->nbr_dev) cudaFree(ctx->nbr_dev);
         cudaSetDevice(prev);
     }
     delete ctx;
@@ -138,6 +158,14 @@ int cpab_set_launch(cpab_ctx *ctx, int block, int ctas_per_sm, int tile_pts)
     if (block) ctx->cfg.block = block;
     if (ctas_per_sm) ctx->cfg.ctas_per_sm = ctas_per_sm;
     if (tile_pts) ctx->cfg.tile_pts = tile_pts;
+    return CPAB_OK;
+}
+
+int cpab_set_max_ctas(cpab_ctx *ctx, int max_ctas)
+{
+    if (!ctx) return fail(nullptr, CPAB_BAD_ARG, "ctx is NULL");
+    if (max_ctas < 0) return fail(ctx, CPAB_BAD_ARG, "max_ctas < 0");
+    ctx->cfg.max_ctas = max_ctas;
     return CPAB_OK;
 }
 
@@ -210,8 +238,10 @@ static int check_integrate(cpab_ctx *ctx, const double *signedA, const double *T
         return fail(ctx, CPAB_BAD_DTYPE, "precision must be CPAB_F64 or CPAB_F32");
     if (scheme != CPAB_SCHEME_REF && scheme != CPAB_SCHEME_SIMPLE && scheme != CPAB_SCHEME_EXACT)
         return fail(ctx, CPAB_BAD_ARG, "unknown scheme %d", scheme);
-    if (scheme == CPAB_SCHEME_EXACT && ctx->t.dim != 1)
-        return fail(ctx, CPAB_UNSUPPORTED, "the exact scheme is built for 1D spaces");
+    if (scheme == CPAB_SCHEME_EXACT && ctx->t.dim != 1 && !ctx->facets_dev)
+        return fail(ctx, CPAB_UNSUPPORTED, "this context has no facet tables (created without a device)");
+    if (scheme == CPAB_SCHEME_EXACT && ctx->t.dim != 1 && !Trels)
+        return fail(ctx, CPAB_BAD_ARG, "Trels is NULL");
     if (nPts < 0) return fail(ctx, CPAB_BAD_SHAPE, "nPts < 0");
     if (nTimeSteps < 1) return fail(ctx, CPAB_BAD_ARG, "nTimeSteps must be >= 1");
     if (nStepsODE < 1) return fail(ctx, CPAB_BAD_ARG, "nStepsODE must be >= 1");
@@ -227,7 +257,7 @@ static int check_integrate(cpab_ctx *ctx, const double *signedA, const double *T
     if (nPts > 0 && overlaps(pts, bytes, out, bytes))
         return fail(ctx, CPAB_ALIAS, "pts and out cannot point to the same memory (_CpaCalcs.py:388)");
     size_t need;
-    if (scheme == CPAB_SCHEME_EXACT) {
+    if (scheme == CPAB_SCHEME_EXACT && ctx->t.dim == 1) {
         need = exact1d_smem_bytes(ctx->t.nC, ctx->cfg.tile_pts, ctx->cfg.sort,
                                   precision == CPAB_F64 ? PREC_F64 : PREC_F32);
     } else {
@@ -260,6 +290,9 @@ static IntegrateArgs make_args(cpab_ctx *ctx, const double *signedA, const doubl
     a.max_crossings = 4 * ctx->t.nC + 8;
     a.sort = ctx->cfg.sort;
     a.cancel = cancel_ptr(ctx);
+    a.facets = ctx->facets_dev;
+    a.nbr = ctx->nbr_dev;
+    a.nF = ctx->nF;
     return a;
 }
 
@@ -269,8 +302,9 @@ static int run_integrate(cpab_ctx *ctx, IntegrateArgs &a, int precision, int sch
     LaunchCfg cfg = ctx->cfg;
     // small uniform launches: one CTA per tile (the persistent grid would leave CTAs idle)
     if (uniform_tiles_total > 0 && uniform_tiles_total < (int64_t)num_sms() * 2) cfg.grid = (int)uniform_tiles_total;
-    cudaError_t e = (scheme == CPAB_SCHEME_EXACT) ? launch_integrate_exact1d(a, precision, cfg, s)
-                                                   : launch_integrate(a, precision, scheme, cfg, s);
+    if (cfg.grid > 0 && cfg.max_ctas > 0 && cfg.grid > cfg.max_ctas) cfg.grid = cfg.max_ctas;
+    cudaError_t e = (scheme == CPAB_SCHEME_EXACT && a.t.dim == 1) ? launch_integrate_exact1d(a, precision, cfg, s)
+                                                                   : launch_integrate(a, precision, scheme, cfg, s);
     return cuda_status(ctx, e, "integrate launch");
 }
 

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <cstdint>
 #include <initializer_list>
+#include <vector>
 
 #include "../../include/cpab_b200.h"
 #include "cpab_internal.h"
@@ -27,6 +28,10 @@ struct cpab_ctx {
     cudaStream_t cancel_stream = nullptr;
     int cancel_state = 0;              // host mirror (atomic)
     int device = -1;                   // the device the flag lives on
+    // facet tables for the 2D/3D exact scheme, on the same device
+    double *facets_dev = nullptr;
+    int *nbr_dev = nullptr;
+    int nF = 0;
     char err[512] = {0};
 };
 
@@ -87,5 +92,6 @@ inline const volatile int *cancel_ptr(const cpab_ctx *c)
 }
 
 int max_smem_optin();
+int build_facets(const Tess &t, const int *nCs, std::vector<double> &F, std::vector<int> &nbr);
 
 }  // namespace cpab

@@ -99,12 +99,21 @@ struct TableLayout {
 // Stage one instance's tables in shared memory (layout above); h is the
 // sub-step length dt / nStepsODE (float tables only), passed from the
 // kernel's parameters so that no register holds it during integration.
+// EXACT scheme (2D/3D): the sub-step map is the exact flow S = expm(h A)
+// instead of the midpoint map, staged by stage_exact_substeps below.
+template <int DIM, typename Real>
+__device__ void stage_exact_substeps(const double *gA, const double *gT, int nC, double h, Real *sS, Real *sT);
+
 template <int DIM, typename Real>
 __device__ __forceinline__ void stage_tables(const double *gA, const double *gT, int nC, bool with_T, double h,
-                                             Real *sA, Real *sT)
+                                             Real *sA, Real *sT, bool exact_sub = false)
 {
     constexpr int NE = DIM * (DIM + 1);
     const int tab = nC * NE;
+    if (exact_sub) {
+        stage_exact_substeps<DIM, Real>(gA, gT, nC, h, sA, sT);
+        return;
+    }
     // not unrolled: the staging loop's loads in flight would otherwise set
     // the register count of the integration loop that follows
 #pragma unroll 1
@@ -210,6 +219,296 @@ __device__ __forceinline__ void advance(bool fast, const PState<DIM, float> &s, 
     for (int r = 0; r < DIM; ++r) q.add(r, d[r]);
 }
 
+// ------------------------------------------------------------ exact scheme (2D/3D)
+//
+// Sub-step map of the exact flow: column j of S - I is
+// sum_{k>=1} h^k/k! L^{k-1} A[:, j]  (A = [L | b], homogeneous bottom row 0),
+// summed per column until the terms fall below the sum's rounding.
+// double tables: S row-major (the layout exact_affine-style code reads);
+// float tables: S - I column-major (the layout of the float sub-step table).
+template <int DIM, typename Real>
+__device__ void stage_exact_substeps(const double *gA, const double *gT, int nC, double h, Real *sS, Real *sT)
+{
+    constexpr int NE = DIM * (DIM + 1);
+#pragma unroll 1
+    for (int c = threadIdx.x; c < nC; c += blockDim.x) {
+        const double *a = gA + (size_t)c * NE;
+        double L[DIM * DIM];
+#pragma unroll
+        for (int r = 0; r < DIM; ++r)
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) L[r * DIM + k] = a[r * (DIM + 1) + k];
+#pragma unroll 1
+        for (int col = 0; col <= DIM; ++col) {
+            double w[DIM], acc[DIM];
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) {
+                w[r] = h * a[r * (DIM + 1) + col];
+                acc[r] = w[r];
+            }
+#pragma unroll 1
+            for (int k = 2; k <= 40; ++k) {
+                double nw[DIM], big = 0.0, am = 0.0;
+#pragma unroll
+                for (int r = 0; r < DIM; ++r) {
+                    double v = 0.0;
+#pragma unroll
+                    for (int m = 0; m < DIM; ++m) v = fma(L[r * DIM + m], w[m], v);
+                    nw[r] = v * (h / k);
+                }
+#pragma unroll
+                for (int r = 0; r < DIM; ++r) {
+                    w[r] = nw[r];
+                    acc[r] += w[r];
+                    big = fmax(big, fabs(w[r]));
+                    am = fmax(am, fabs(acc[r]));
+                }
+                if (!(big > 1e-18 * am)) break;
+            }
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) {
+                if (sizeof(Real) == 8)
+                    sS[c * NE + r * (DIM + 1) + col] = (Real)(acc[r] + (r == col ? 1.0 : 0.0));
+                else
+                    sS[c * NE + col * DIM + r] = (Real)acc[r];
+            }
+        }
+    }
+    const int tab = nC * NE;
+#pragma unroll 1
+    for (int i = threadIdx.x; i < tab; i += blockDim.x) {
+        if (sizeof(Real) == 8) {
+            sT[i] = (Real)gT[i];
+        } else {
+            const int c = i / NE, e = i - c * NE, r = e / (DIM + 1), col = e - r * (DIM + 1);
+            sT[c * NE + col * DIM + r] = (Real)(gT[i] - (r == col ? 1.0 : 0.0));
+        }
+    }
+}
+
+// What a lane needs to resolve an exit: the instance's signed A (global,
+// row-major [nC, DIM*(DIM+1)]), the facet tables, the sub-step length and
+// the lane's counters.
+struct ExactCross {
+    const double *A;
+    const double *F;
+    const int *nbr;
+    int nF;
+    double h;
+    int cap;
+    unsigned long long crossings, unresolved;
+};
+
+template <int DIM, int TESS>
+__device__ __forceinline__ int lookup_d(const Tess &t, const double *p, double)
+{
+    return exact_cell<DIM, TESS>(t, p);
+}
+template <int DIM, int TESS>
+__device__ __forceinline__ int lookup_d(const Tess &t, const double *p, float)
+{
+    float x[DIM];
+#pragma unroll
+    for (int i = 0; i < DIM; ++i) x[i] = (float)p[i];
+    return fast_cell<DIM, TESS>(t, x);
+}
+
+// out = expm(t A)[p; 1]: x(t) = p + sum_k t^k/k! u_k, u_1 = L p + b,
+// u_k = L u_{k-1}, until the terms fall below the rounding of the sum.
+template <int DIM>
+__device__ __noinline__ void flow_taylor(const double *__restrict__ A, const double *p, double t, double *out)
+{
+    double u[DIM], x[DIM];
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) {
+        double v = __ldg(A + r * (DIM + 1) + DIM);
+#pragma unroll
+        for (int m = 0; m < DIM; ++m) v = fma(__ldg(A + r * (DIM + 1) + m), p[m], v);
+        u[r] = t * v;
+        x[r] = p[r] + u[r];
+    }
+#pragma unroll 1
+    for (int k = 2; k <= 40; ++k) {
+        double nu[DIM], big = 0.0, xm = 0.0;
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) {
+            double v = 0.0;
+#pragma unroll
+            for (int m = 0; m < DIM; ++m) v = fma(__ldg(A + r * (DIM + 1) + m), u[m], v);
+            nu[r] = v * (t / k);
+        }
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) {
+            u[r] = nu[r];
+            x[r] += u[r];
+            big = fmax(big, fabs(u[r]));
+            xm = fmax(xm, fabs(x[r]));
+        }
+        if (!(big > 1e-18 * (xm + 1e-300))) break;
+    }
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) out[r] = x[r];
+}
+
+// First root in [0, s] of g(t) = F . x(t) + F[DIM] along the flow of A from
+// p, given g(0) = g0 < 0 < g(s): the Taylor coefficients of g
+// (c_k = F . u_k / k!) and a safeguarded Newton iteration on that polynomial.
+template <int DIM>
+__device__ __noinline__ double facet_hit_time(const double *__restrict__ A, const double *__restrict__ F,
+                                              const double *p, double s, double g0)
+{
+    constexpr int KMAX = 24;
+    double c[KMAX + 1];
+    c[0] = g0;
+    double u[DIM], fact = 1.0, sk = 1.0, scale = fabs(g0);
+    int K = 1;
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) {
+        double v = __ldg(A + r * (DIM + 1) + DIM);
+#pragma unroll
+        for (int m = 0; m < DIM; ++m) v = fma(__ldg(A + r * (DIM + 1) + m), p[m], v);
+        u[r] = v;
+    }
+#pragma unroll 1
+    for (int k = 1; k <= KMAX; ++k) {
+        if (k > 1) {
+            double nu[DIM];
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) {
+                double v = 0.0;
+#pragma unroll
+                for (int m = 0; m < DIM; ++m) v = fma(__ldg(A + r * (DIM + 1) + m), u[m], v);
+                nu[r] = v;
+            }
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) u[r] = nu[r];
+        }
+        fact *= k;
+        sk *= s;
+        double d = 0.0;
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) d = fma(__ldg(F + r), u[r], d);
+        c[k] = d / fact;
+        K = k;
+        const double term = fabs(c[k]) * sk;
+        scale = fmax(scale, term);
+        if (k >= 2 && !(term > 1e-18 * scale)) break;
+    }
+    auto P = [&](double t, double &dP) {
+        double v = c[K], dv = 0.0;
+#pragma unroll 1
+        for (int k = K - 1; k >= 0; --k) {
+            dv = fma(dv, t, v);
+            v = fma(v, t, c[k]);
+        }
+        dP = dv;
+        return v;
+    };
+    double lo = 0.0, hi = s, dP;
+    const double ps = P(s, dP);
+    if (!(ps > 0)) return s;
+    double t = s * (-g0) / (ps - g0);
+    if (!(t > lo && t < hi)) t = 0.5 * (lo + hi);
+#pragma unroll 1
+    for (int it = 0; it < 60; ++it) {
+        const double g = P(t, dP);
+        if (g > 0) hi = t; else lo = t;
+        if (g == 0) return t;
+        double tn = t - g / dP;
+        if (!(tn > lo && tn < hi)) tn = 0.5 * (lo + hi);
+        if (fabs(tn - t) <= 2e-16 * fabs(t) || hi - lo <= 2e-16 * hi) return tn;
+        t = tn;
+    }
+    return 0.5 * (lo + hi);
+}
+
+// A sub-step of length h from st in cell c ended at q outside c: the exact
+// flow from st, exit times through interior facets, the neighbour across the
+// exited facet, the rest of the sub-step there (and so on).  q becomes the
+// point at the sub-step's end; returns its cell.  FP64 throughout (the
+// hitting times); q keeps the state's precision.  When no interior facet
+// explains the exit (a point on the domain boundary) or the crossings exceed
+// the cap, q is the end point of the flow in the current cell (as in the
+// reference scheme, which keeps its sub-step's end wherever it lands).
+template <int DIM, int TESS, typename Real>
+__device__ __noinline__ int exact_substep_cross(const Tess &t, ExactCross &ex, int c, const PState<DIM, Real> &st,
+                                                PState<DIM, Real> &q)
+{
+    constexpr int NH = DIM + 1, NE = DIM * NH;
+    double p[DIM], y[DIM];
+    st.get(p);
+    q.get(y);
+    double s = ex.h;
+#pragma unroll 1
+    for (int crossings = 0;;) {
+        if (lookup_d<DIM, TESS>(t, y, Real(0)) == c) {
+            q.set(y);
+            return c;
+        }
+        const double *A = ex.A + (size_t)c * NE;
+        const double *Fc = ex.F + (size_t)c * ex.nF * NH;
+        double tau = s;
+        int kbest = -1;
+#pragma unroll 1
+        for (int k = 0; k < ex.nF; ++k) {
+            if (__ldg(ex.nbr + c * ex.nF + k) < 0) continue;
+            const double *F = Fc + k * NH;
+            double ge = __ldg(F + DIM), g0 = ge;
+#pragma unroll
+            for (int r = 0; r < DIM; ++r) {
+                const double n = __ldg(F + r);
+                ge = fma(n, y[r], ge);
+                g0 = fma(n, p[r], g0);
+            }
+            if (!(ge > 0)) continue;
+            const double r = (g0 >= 0) ? 0.0 : facet_hit_time<DIM>(A, F, p, s, g0);
+            if (kbest < 0 || r < tau) {
+                tau = r;
+                kbest = k;
+            }
+        }
+        if (kbest < 0 || !(tau == tau) || ++crossings > ex.cap) {
+            ++ex.unresolved;
+            q.set(y);
+            return lookup_d<DIM, TESS>(t, y, Real(0));
+        }
+        flow_taylor<DIM>(A, p, tau, p);
+        s -= tau;
+        c = __ldg(ex.nbr + c * ex.nF + kbest);
+        ++ex.crossings;
+        if (!(s > 0)) {
+            q.set(p);
+            return c;
+        }
+        flow_taylor<DIM>(ex.A + (size_t)c * NE, p, s, y);
+    }
+}
+
+// EXACT unit: the closed-form step with T (the reference's arithmetic in
+// double) or one sub-step of the exact flow with S.
+template <int DIM>
+__device__ __forceinline__ void advance_exact(bool fast, const PState<DIM, double> &s, const double *S,
+                                              const double *T, PState<DIM, double> &q)
+{
+    if (fast) {
+        exact_affine<DIM>(q.p, T, s.p);
+    } else {
+#pragma unroll
+        for (int r = 0; r < DIM; ++r) {
+            double v = S[r * (DIM + 1) + DIM];
+#pragma unroll
+            for (int m = 0; m < DIM; ++m) v = fma(S[r * (DIM + 1) + m], s.p[m], v);
+            q.p[r] = v;
+        }
+    }
+}
+template <int DIM>
+__device__ __forceinline__ void advance_exact(bool fast, const PState<DIM, float> &s, const float *S, const float *T,
+                                              PState<DIM, float> &q)
+{
+    advance<DIM>(fast, s, S, T, nullptr, 0.0f, q);
+}
+
 // ------------------------------------------------------------ integration
 
 // One warp integrates the points [ws, we).  Every lane owns one point and
@@ -242,7 +541,7 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
                                                 unsigned long long &c_sub, unsigned long long &c_pts,
                                                 const int *perm = nullptr, int64_t perm_base = 0,
                                                 unsigned long long *claim = nullptr,
-                                                const int *start_cells = nullptr)
+                                                const int *start_cells = nullptr, ExactCross *ex = nullptr)
 {
     constexpr int NE = DIM * (DIM + 1);
     const int lane = threadIdx.x & 31;
@@ -275,10 +574,15 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
 #pragma unroll
         for (int u = 0; u < kUnits; ++u) {
             if (active && !fin) {
-                const bool fast = (SCHEME == SCHEME_REF) && sub_left == 0;
+                const bool fast = (SCHEME == SCHEME_REF || SCHEME == SCHEME_EXACT) && sub_left == 0;
                 PState<DIM, Real> q;
-                advance<DIM>(fast, st, sA + c * NE, sT + c * NE, nullptr, h, q);
-                const int cq = cell_of<DIM, TESS>(t, q);
+                if (SCHEME == SCHEME_EXACT)
+                    advance_exact<DIM>(fast, st, sA + c * NE, sT + c * NE, q);
+                else
+                    advance<DIM>(fast, st, sA + c * NE, sT + c * NE, nullptr, h, q);
+                int cq = cell_of<DIM, TESS>(t, q);
+                if (SCHEME == SCHEME_EXACT && !fast && cq != c)
+                    cq = exact_substep_cross<DIM, TESS, Real>(t, *ex, c, st, q);
                 if (fast && cq != c) {
                     // the end point left the cell: redo the step with nStepsODE sub-steps from p
                     sub_left = nODE;
@@ -292,7 +596,7 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
                     } else {
                         --sub_left;
                         ++c_sub;
-                        if (SCHEME == SCHEME_REF && sub_left == 0) --steps_left;
+                        if (SCHEME != SCHEME_SIMPLE && sub_left == 0) --steps_left;
                     }
                 }
                 fin = (SCHEME == SCHEME_SIMPLE) ? (sub_left == 0) : (steps_left == 0);

@@ -108,6 +108,7 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
     int loaded = -1;
     const ArraySrc<DIM> src{a.pts_in};
     ArraySnk<DIM> snk{a.pts_out, a.clamp, a.clamp_lo, a.clamp_hi, 0ull};
+    ExactCross ex{nullptr, a.facets, a.nbr, a.nF, a.h_sub, a.max_crossings, 0ull, 0ull};
 
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         if ((((tile - blockIdx.x) / gridDim.x) & 7) == 0 && cta_cancelled(a.cancel, a.counters)) break;
@@ -119,7 +120,8 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
         const TileInfo ti = s_tile;
         if (ti.inst != loaded) {
             stage_tables<DIM, Real>(a.A + (size_t)ti.inst * tab, a.T + (size_t)ti.inst * tab, a.t.nC,
-                                    SCHEME == SCHEME_REF, a.h_sub, sA, sT);
+                                    SCHEME != SCHEME_SIMPLE, a.h_sub, sA, sT, SCHEME == SCHEME_EXACT);
+            ex.A = a.A + (size_t)ti.inst * tab;
             loaded = ti.inst;
             __syncthreads();
         }
@@ -147,7 +149,7 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
         // every warp works on the whole tile through the shared claim counter
         integrate_range<DIM, TESS, Real, SCHEME>(a.t, a.nTimeSteps, a.nStepsODE, sA, sT, ti.start, ti.end, h, src,
                                                  snk, c_fast, c_fb, c_sub, c_pts, perm, ti.start, &s_claim,
-                                                 perm ? s_cell : nullptr);
+                                                 perm ? s_cell : nullptr, &ex);
         __syncthreads();
     }
     if (a.counters) {
@@ -156,12 +158,19 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
         c_sub = warp_sum_u64(c_sub);
         c_pts = warp_sum_u64(c_pts);
         unsigned long long c_nan = warp_sum_u64(snk.nan);
+        unsigned long long c_cross = 0, c_unres = 0;
+        if (SCHEME == SCHEME_EXACT) {
+            c_cross = warp_sum_u64(ex.crossings);
+            c_unres = warp_sum_u64(ex.unresolved);
+        }
         if ((threadIdx.x & 31) == 0) {
             atomicAdd(a.counters + CNT_FAST, c_fast);
             atomicAdd(a.counters + CNT_FALLBACK, c_fb);
             atomicAdd(a.counters + CNT_SUBSTEPS, c_sub);
             atomicAdd(a.counters + CNT_POINTS, c_pts);
             if (c_nan) atomicAdd(a.counters + CNT_NAN, c_nan);
+            if (c_cross) atomicAdd(a.counters + CNT_CROSSINGS, c_cross);
+            if (c_unres) atomicAdd(a.counters + CNT_FAILED, c_unres);
         }
     }
 }
@@ -429,7 +438,8 @@ int persistent_grid_impl(const void *kern, const LaunchCfg &cfg, size_t smem)
         }
     }
     if (cfg.ctas_per_sm > 0 && cfg.ctas_per_sm < per_sm) per_sm = cfg.ctas_per_sm;
-    return num_sms() * per_sm;
+    const int g = num_sms() * per_sm;
+    return (cfg.max_ctas > 0 && cfg.max_ctas < g) ? cfg.max_ctas : g;
 }
 
 static int grid_for(int64_t n, int block, int per_sm = 8)
@@ -461,6 +471,12 @@ template <int DIM, int TESS>
 static cudaError_t launch_integrate_dt(const IntegrateArgs &a, int prec, int scheme, const LaunchCfg &cfg,
                                        cudaStream_t s)
 {
+    if constexpr (DIM > 1) {
+        // the 2D/3D exact scheme (1D has its own kernel, k_exact1d)
+        if (scheme == SCHEME_EXACT)
+            return prec == PREC_F64 ? launch_integrate_t<DIM, TESS, double, SCHEME_EXACT>(a, cfg, s)
+                                    : launch_integrate_t<DIM, TESS, float, SCHEME_EXACT>(a, cfg, s);
+    }
     if (prec == PREC_F64) {
         if (scheme == SCHEME_REF) return launch_integrate_t<DIM, TESS, double, SCHEME_REF>(a, cfg, s);
         return launch_integrate_t<DIM, TESS, double, SCHEME_SIMPLE>(a, cfg, s);

@@ -15,6 +15,7 @@ struct LaunchCfg {
     int grid = 0;          // explicit grid (0 = persistent default)
     int tile_pts = 2048;   // points per CTA tile
     int sort = 0;          // cell-sort the points of each tile
+    int max_ctas = 0;      // cap on the CTAs of every persistent launch of the context (0 = none)
 };
 
 // Kernels opt in to more than the default 48 KB of shared memory when their

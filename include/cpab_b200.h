@@ -58,16 +58,27 @@ enum { CPAB_F64 = 0, CPAB_F32 = 1 };
  *                     reference's double arithmetic in CPAB_F64.
  *  CPAB_SCHEME_SIMPLE calc_T_simple: midpoint sub-steps only
  *                     (cpab/gpu/calc_2Dto2D.cu:412-445).
- *  CPAB_SCHEME_EXACT  closed-form flow with cell-boundary hitting times
- *                     (1D; cpab/cpa1d/calcs/ClosedFormInt.py:64-256). */
+ *  CPAB_SCHEME_EXACT  the flow across cell boundaries with hitting times.
+ *                     1D: closed form (cpab/cpa1d/calcs/ClosedFormInt.py:
+ *                     64-256).  2D/3D (no reference counterpart; replaces
+ *                     the midpoint fallback of calc_2Dto2D.cu:167-197):
+ *                     REF's closed-form steps and keep test; a step that
+ *                     leaves its cell is re-integrated in nStepsODE
+ *                     sub-steps of the exact flow expm(h*A_c), and a
+ *                     sub-step whose end leaves the cell moves to the
+ *                     facet at its hitting time and on in the neighbour.
+ *                     Hitting times in FP64 in both precisions. */
 enum { CPAB_SCHEME_REF = 0, CPAB_SCHEME_SIMPLE = 1, CPAB_SCHEME_EXACT = 2 };
 
 /* Counter slots written by calls that take `counters` (uint64[CPAB_CNT_N],
- * added to): closed-form steps kept (cell visits for the exact scheme),
- * fallback steps, midpoint sub-steps, points finished, points that hit the
- * crossing cap, points with a NaN result, CTAs stopped by cpab_cancel. */
+ * added to): closed-form steps kept (cell visits for the 1D exact scheme),
+ * fallback steps, sub-steps, points finished, points that hit the crossing
+ * cap (2D/3D exact: sub-steps whose exit no interior facet explained),
+ * points with a NaN result, CTAs stopped by cpab_cancel, facet crossings
+ * resolved at their hitting time (2D/3D exact). */
 enum { CPAB_CNT_FAST = 0, CPAB_CNT_FALLBACK = 1, CPAB_CNT_SUBSTEPS = 2, CPAB_CNT_POINTS = 3,
-       CPAB_CNT_FAILED = 4, CPAB_CNT_NAN = 5, CPAB_CNT_CANCELLED = 6, CPAB_CNT_N = 7 };
+       CPAB_CNT_FAILED = 4, CPAB_CNT_NAN = 5, CPAB_CNT_CANCELLED = 6, CPAB_CNT_CROSSINGS = 7,
+       CPAB_CNT_N = 8 };
 
 /* ------------------------------------------------------------------ context */
 
@@ -78,6 +89,17 @@ enum { CPAB_CNT_FAST = 0, CPAB_CNT_FALLBACK = 1, CPAB_CNT_SUBSTEPS = 2, CPAB_CNT
  * (cpab/cpaNd/_CpaSpace.py:278-294).  Replaces the per-space kernel JIT
  * (cpab/gpu/Calcs.py:66-203, N_CELLS/DIM/TESS_TYPE macros :159-162). */
 int cpab_ctx_create(cpab_ctx **out, int dim, int tess, const int *nCs_host, const double *incs_host);
+/* Facet tables of a tessellation (host only; no device needed): per cell,
+ * n_facets rows (outward unit normal, -offset) -- g(x) = n.x - offset <= 0
+ * inside -- in facets[nC * n_facets * (dim+1)], and the cell across each
+ * facet (-1 on the domain boundary) in nbr[nC * n_facets].  Simplex facet k
+ * is opposite vertex k of the reference's vertex order
+ * (cpab/cpa2d/Tessellation.py:73-138, cpab/cpa3d/Tessellation.py:62-200);
+ * box facets are (x_lo, x_hi, y_lo, y_hi, z_lo, z_hi).  facets/nbr may be
+ * NULL to query n_facets.  The tables the 2D/3D exact scheme uses; no
+ * counterpart in the reference. */
+int cpab_tess_facets(int dim, int tess, const int *nCs_host, const double *incs_host, double *facets, int *nbr,
+                     int *n_facets);
 int cpab_ctx_destroy(cpab_ctx *ctx);
 /* Last error of this context (or of the calling thread when ctx == NULL). */
 const char *cpab_last_error_string(const cpab_ctx *ctx);
@@ -116,6 +138,12 @@ int cpab_set_launch(cpab_ctx *ctx, int block, int ctas_per_sm, int tile_pts);
  * integrated on its own).  Off by default; the autotuner decides.  No
  * reference counterpart (the reference launches one thread per point in input
  * order, cpab/gpu/Calcs.py:515). */
+/* Cap every persistent launch of this context (integration, exact,
+ * registration and landmark kernels) at max_ctas CTAs (0 = no cap), leaving
+ * the other SMs to kernels of other streams -- a server keeps long
+ * registration jobs from occupying every SM while transform batches wait.
+ * Results do not depend on the cap.  No counterpart in the reference. */
+int cpab_set_max_ctas(cpab_ctx *ctx, int max_ctas);
 int cpab_set_cell_sort(cpab_ctx *ctx, int enable);
 
 /* ------------------------------------------------------------------ prologue */
