@@ -12,8 +12,10 @@
 // endpoint (sign change / zero velocity), with the reference's 1e-16 and
 // 1e-12 nudges at endpoints and its np.allclose(., 0) tests (|.| <= 1e-8).
 //
-// Arithmetic is double in both precisions: the FP32 mode only stores the
-// points in float (hitting times and exponentials stay in double).
+// Hitting times are double in both precisions.  The FP32 mode stores the
+// points in float, takes the first cell's exit time as a difference of
+// logarithms (per-cell exit logarithms staged with the tables) and the
+// final position's exponential in float (cf_crossing_f32, cf_phi_f32).
 #include <math_constants.h>
 
 #include "cpab_device.cuh"
@@ -25,6 +27,7 @@ struct Exact1D {
     const double *A;  // [nC, 2] signed (a, b) of the current instance, shared memory
     const double *ba; // [nC] b / a
     const double *ia; // [nC] 1.0 / a
+    const double *lx; // [2 nC] log|xn + b/a| of the cell's exit points (xn: right, then left), FP32 mode
     int nC;
     double step;      // 1/nC: vertices x_k = k*step, x_nC = 1 (np.linspace(0,1,nC+1))
 };
@@ -65,6 +68,47 @@ __device__ double cf_crossing(const Exact1D &e, double x, int c, int &next)
     else t = e.ia[c] * log((xn + e.ba[c]) / (x + e.ba[c]));   // 1.0/a * log((xn + b/a) / (x + b/a))
     next = cn;
     return t;
+}
+
+// FP32 mode (float points; hitting times stay FP64): the time to the exit
+// of the first cell as a difference of logarithms, log|xn + b/a| taken from
+// the per-cell table, so that a point costs one log and no division; within
+// a few ulps of the reference's log of the ratio, i.e. a time error of order
+// 1e-16 |log(...)| / |a| -- far below the float result's rounding.
+__device__ double cf_crossing_f32(const Exact1D &e, double x, int c, int &next)
+{
+    const double a = e.A[2 * c], b = e.A[2 * c + 1];
+    const double v = cf_v(e, x, c);
+    next = -1;
+    if (near0(v)) return CUDART_INF;
+    const int cn = c + (v > 0 ? 1 : -1);
+    if (!(0 <= cn && cn < e.nC)) return CUDART_INF;
+    const double xn = (v > 0) ? vert(e, cn) + 1e-16 : vert(e, c) - 1e-16;
+    const double vn = cf_v(e, xn, cn);
+    if (near0(vn)) return CUDART_INF;
+    if ((v > 0) != (vn > 0)) return CUDART_INF;
+    double t;
+    if (xn == 0 || xn == 1) t = CUDART_INF;
+    else if (near0(a)) t = (xn - x) / b;
+    else t = e.ia[c] * (e.lx[2 * c + (v > 0 ? 0 : 1)] - log(fabs(x + e.ba[c])));
+    next = cn;
+    return t;
+}
+
+// FP32 mode: the final position x + t v(x) phi(a t), phi(z) = (e^z - 1)/z,
+// with v in FP64 (it multiplies the flow's expansion e^{a t}) and phi in
+// FP32 (relative error ~2e-7 of a displacement within one cell).  Equal in
+// exact arithmetic to the reference's e^{at} x + b (e^{at} - 1)/a.
+__device__ __forceinline__ double cf_phi_f32(const Exact1D &e, int c, double x, double t)
+{
+    const double a = e.A[2 * c], b = e.A[2 * c + 1];
+    if (!(0 <= x && x <= 1)) return x;
+    if (a == 0) return x + t * b;
+    const double v = fma(a, x, b);
+    const float z = (float)(a * t);
+    const float phi = fabsf(z) < 1e-3f ? fmaf(z, fmaf(z, fmaf(z, 1.f / 24.f, 1.f / 6.f), 0.5f), 1.f)
+                                       : expm1f(z) / z;
+    return fma(t * v, (double)phi, x);
 }
 
 __device__ __forceinline__ double cf_phi(const Exact1D &e, int c, double x, double t)
@@ -112,7 +156,9 @@ __device__ void build_transit(const Exact1D &e, Transit tr)
 }
 
 // calc_phi for one point; returns false when the crossing cap is hit
-// (the reference raises ValueError, ClosedFormInt.py:155-160).
+// (the reference raises ValueError, ClosedFormInt.py:155-160).  F32: the
+// first hitting time and the final position of the FP32 mode (above).
+template <bool F32>
 __device__ bool cf_point(const Exact1D &e, const Transit &tr, double x, double t, int cap, double &out,
                          unsigned &visits)
 {
@@ -129,7 +175,7 @@ __device__ bool cf_point(const Exact1D &e, const Transit &tr, double x, double t
     }
     // first visit: general position
     int c = cf_cell(e, x_old), cn;
-    double tc = cf_crossing(e, x_old, c, cn);
+    double tc = F32 ? cf_crossing_f32(e, x_old, c, cn) : cf_crossing(e, x_old, c, cn);
     // the record of the next cell (entered at its nudged vertex, from the left when moving right)
     int idx = record_of(cn, c);
     bool ok = true;
@@ -155,18 +201,27 @@ __device__ bool cf_point(const Exact1D &e, const Transit &tr, double x, double t
         c = nn.x;
         idx = nn.y;
     }
-    out = ok ? fmin(1.0, fmax(0.0, cf_phi(e, c, x_old, t_rem))) : x_old;
+    out = ok ? fmin(1.0, fmax(0.0, F32 ? cf_phi_f32(e, c, x_old, t_rem) : cf_phi(e, c, x_old, t_rem))) : x_old;
     return ok;
 }
 
-// Shared memory of k_exact1d: per cell A (2 doubles), b/a and 1/a (2), and
-// two transit records (2 x (16 + 8) bytes) -- 80 bytes, so what follows is
-// 16-byte aligned -- and, when cell-sorting, sorted start points and results
-// in input order [tile_pts] (Real), the permutation [tile_pts] (16-bit) and
-// the histogram [nC] (int).
+// Cell-sort key of a start point: only groups points (any key in [0, nC)
+// keeps the results; the walk itself uses cf_cell), so float points take a
+// float product and a conversion (NaN converts to 0).
+__device__ __forceinline__ int sort_key(const Exact1D &e, double x) { return cf_cell(e, x); }
+__device__ __forceinline__ int sort_key(const Exact1D &e, float x)
+{
+    return min(max((int)(x * (float)e.nC), 0), e.nC - 1);
+}
+
+// Shared memory of k_exact1d: per cell A (2 doubles), b/a and 1/a (2), the
+// two exit logarithms (2), and two transit records (2 x (16 + 8) bytes) --
+// 96 bytes, so what follows is 16-byte aligned -- and, when cell-sorting,
+// sorted start points and results in input order [tile_pts] (Real), the
+// permutation [tile_pts] (16-bit) and the histogram [nC] (int).
 size_t exact1d_smem_bytes(int nC, int tile_pts, int sort, int prec)
 {
-    size_t b = (size_t)nC * (4 * sizeof(double) + 2 * (sizeof(double2) + sizeof(int2)));
+    size_t b = (size_t)nC * (6 * sizeof(double) + 2 * (sizeof(double2) + sizeof(int2)));
     if (sort)
         b += 2 * (size_t)tile_pts * (prec == PREC_F64 ? sizeof(double) : sizeof(float)) +
              (size_t)tile_pts * sizeof(unsigned short) + ((size_t)nC + 2) * sizeof(int);
@@ -179,9 +234,9 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nC = a.t.nC;
     double *sA = reinterpret_cast<double *>(smem_raw);
-    double *s_ba = sA + 2 * nC, *s_ia = s_ba + nC;
+    double *s_ba = sA + 2 * nC, *s_ia = s_ba + nC, *s_lx = s_ia + nC;
     Transit tr;
-    tr.te = reinterpret_cast<double2 *>(s_ia + nC);
+    tr.te = reinterpret_cast<double2 *>(s_lx + 2 * nC);
     tr.cn = reinterpret_cast<int2 *>(tr.te + 2 * nC);
     // cell-sort scratch (see exact1d_smem_bytes)
     const int tp = a.batch.tile_pts;
@@ -202,6 +257,7 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
     e.A = sA;
     e.ba = s_ba;
     e.ia = s_ia;
+    e.lx = s_lx;
     e.nC = nC;
     e.step = 1.0 / (double)nC;
     // the reference gives up after nC crossings
@@ -219,8 +275,13 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
             for (int i = threadIdx.x; i < nC * 2; i += blockDim.x) sA[i] = gA[i];
             for (int c = threadIdx.x; c < nC; c += blockDim.x) {
                 const double ac = gA[2 * c], bc = gA[2 * c + 1];
-                s_ba[c] = bc / ac;
+                const double ba = bc / ac;
+                s_ba[c] = ba;
                 s_ia[c] = 1.0 / ac;
+                if (sizeof(Real) == 4) {
+                    s_lx[2 * c] = log(fabs(vert(e, c + 1) + 1e-16 + ba));
+                    s_lx[2 * c + 1] = log(fabs(vert(e, c) - 1e-16 + ba));
+                }
             }
             __syncthreads();
             build_transit(e, tr);
@@ -238,14 +299,14 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
                 Real xin;
                 load_pt<1, Real>(a.pts_in, ti.start + j, &xin);
                 s_y[j] = xin;
-                atomicAdd(s_hist + cf_cell(e, (double)xin), 1);
+                atomicAdd(s_hist + sort_key(e, xin), 1);
             }
             __syncthreads();
             warp0_exclusive_scan(s_hist, nC);
             __syncthreads();
             for (int j = threadIdx.x; j < n; j += blockDim.x) {
                 const Real xin = s_y[j];
-                const int pos = atomicAdd(s_hist + cf_cell(e, (double)xin), 1);
+                const int pos = atomicAdd(s_hist + sort_key(e, xin), 1);
                 s_perm[pos] = (unsigned short)j;
                 s_xs[pos] = xin;
             }
@@ -263,7 +324,7 @@ __global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
                 if (a.sort) xin = s_xs[k];
                 else load_pt<1, Real>(a.pts_in, ti.start + k, &xin);
                 double y;
-                bool ok = cf_point(e, tr, (double)xin, T_total, cap, y, visits);
+                bool ok = cf_point<sizeof(Real) == 4>(e, tr, (double)xin, T_total, cap, y, visits);
                 if (a.clamp) y = clamp_ref(y, a.clamp_lo, a.clamp_hi);
                 Real yo = (Real)y;
                 if (a.sort) s_y[s_perm[k]] = yo;
