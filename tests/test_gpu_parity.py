@@ -292,6 +292,32 @@ def test_batched_host_pipeline_equals_device(scheme):
     np.testing.assert_array_equal(oh.numpy(), od.cpu().numpy())
 
 
+@pytest.mark.parametrize("chunks", [1, 2, 3, 7])
+def test_batched_host_pipeline_back_to_back(chunks):
+    """Several calc_T_batched_host calls in a row with no synchronisation in
+    between (the device buffers are reused across calls; larger batches grow
+    them): every result equals calc_T_batched on device buffers."""
+    sp, _, rng = _prior_space(1, (100,), "II", 19, torch.float32)
+    prior = Prior.create(sp.geo, 0.1, 1.0)
+    p = dict(dt=0.02, nTimeSteps=50, nStepsODEsolver=100)
+    calls = []
+    for n_inst, max_pts in ((23, 2000), (41, 4000), (9, 500), (64, 6000)):
+        theta = prior.sample(n_inst, rng)
+        sizes = rng.integers(0, max_pts, size=n_inst)
+        offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        xh = torch.from_numpy(rng.uniform(0, 1, size=(int(offs[-1]), 1)).astype(np.float32)).pin_memory()
+        oh = torch.full_like(xh, float("nan")).pin_memory()
+        sp.calc_T_batched_host(theta, xh, oh, offs, scheme=_lib.SCHEME_EXACT, chunks=chunks, **p)
+        calls.append((theta, offs, xh, oh))
+    torch.cuda.synchronize()
+    for theta, offs, xh, oh in calls:
+        tables = sp.tables_from_theta(torch.as_tensor(theta, device=DEV), 0.02, 1)
+        xd = xh.to(DEV)
+        od = torch.empty_like(xd)
+        sp.calc_T_batched(tables, xd, od, offsets=torch.as_tensor(offs, device=DEV), scheme=_lib.SCHEME_EXACT, **p)
+        np.testing.assert_array_equal(oh.numpy(), od.cpu().numpy())
+
+
 @pytest.mark.parametrize("dim,nCs,tess,precision", [(2, (4, 4), "I", torch.float64), (2, (4, 4), "I", torch.float32),
                                                     (3, (4, 4, 4), "I", torch.float32), (1, (100,), "II", torch.float64)])
 def test_launch_shape_and_cell_sort_do_not_change_results(dim, nCs, tess, precision):
