@@ -58,8 +58,10 @@ def parse():
     ap.add_argument("--theta", type=int, default=N_THETA)
     ap.add_argument("--e2e-chunks", type=int, default=16,
                     help="instance groups of the host-buffer pipeline (copy in / integrate / copy out overlap)")
-    ap.add_argument("--serve-seconds", type=float, default=0.5,
-                    help="seconds of Poisson arrivals (2000 req/s) for the serving leg; 0 skips it")
+    ap.add_argument("--serve-seconds", type=float, default=2.0,
+                    help="seconds of Poisson arrivals at 2000 req/s for the serving leg; 0 skips serving")
+    ap.add_argument("--serve-sustained-seconds", type=float, default=10.0,
+                    help="seconds of arrivals at 80%% of the measured serving capacity; 0 skips that run")
     ap.add_argument("--workload", default="batched_1d",
                     choices=["batched_1d", "batched_2d_nc64", "remap_ssd", "mcmc_c3"],
                     help="batched_1d: the headline (1D nC=100, 4096 theta, ragged); batched_2d_nc64: the reference "
@@ -275,6 +277,25 @@ def cpu_reference_rate(theta, offsets, pts, geo, budget_pts: int, rank_seed: int
     return npts / dt, f"first {n_inst} of {len(offsets) - 1} instances ({npts} points), FP64", kind, O.nproc(), dt
 
 
+def cpu_closed_form_rate(theta, offsets, pts, geo, budget_pts: int):
+    """The closed form (the oracle's C restatement of ClosedFormInt, FP64,
+    OpenMP over points, all host threads) on the first instances covering
+    ~budget_pts points.  Returns (points/s, sample text, cores)."""
+    from oracle import oracle as O
+    n_inst = int(np.searchsorted(offsets, budget_pts)) + 1
+    n_inst = max(1, min(n_inst, len(offsets) - 1))
+    As = [(geo.B @ theta[i]).reshape(NC, 2) for i in range(n_inst)]
+    xs = [pts[offsets[i]:offsets[i + 1]].astype(np.float64)[:, 0] for i in range(n_inst)]
+    O.closed_form_1d(As[0], NC, xs[0], DT * NT)          # warm the library and the threads
+    t0 = time.perf_counter()
+    npts = 0
+    for A, x in zip(As, xs):
+        O.closed_form_1d(A, NC, x, DT * NT)
+        npts += x.size
+    dt = time.perf_counter() - t0
+    return npts / dt, f"first {n_inst} of {len(offsets) - 1} instances ({npts} points), FP64", O.nproc()
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -312,19 +333,25 @@ def plain_vs_batched_2d(torch, dev):
     theta = Prior.create(sp64.geo, 0.1, 1.0).sample(nth, rng)
     x = rng.uniform(0, 1, size=(nth * npt, 2))
     p = dict(dt=DT, nTimeSteps=NT, nStepsODEsolver=NODE)
-    # plain: first 64 theta, FP64 (the drop-in default), one call each
-    xs = torch.as_tensor(x[:npt], device=dev)
-    out = torch.empty_like(xs)
+    # plain: first 64 theta, one call each (host A = B theta, expm launch, calc_T launch, stream sync),
+    # in FP64 (the drop-in default) and in FP32 (the batched arm's precision)
     n_plain = 64
-    for rep in range(2):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for i in range(n_plain):
-            sp64.update_pat(sp64.B_host @ theta[i])
-            sp64.calc_T_fwd(pts=xs, out=out, **p)
-            torch.cuda.current_stream().synchronize()
-        t_plain = time.perf_counter() - t0
-    plain = n_plain * npt / t_plain
+
+    def plain_rate(sp, dtype):
+        xs = torch.as_tensor(x[:npt], device=dev, dtype=dtype)
+        out = torch.empty_like(xs)
+        for rep in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for i in range(n_plain):
+                sp.update_pat(sp.B_host @ theta[i])
+                sp.calc_T_fwd(pts=xs, out=out, **p)
+                torch.cuda.current_stream().synchronize()
+            t_plain = time.perf_counter() - t0
+        return n_plain * npt / t_plain
+
+    plain = plain_rate(sp64, torch.float64)
+    plain32 = plain_rate(sp32, torch.float32)
     xb = torch.as_tensor(x, device=dev, dtype=torch.float32)
     ob = torch.empty_like(xb)
     th = torch.as_tensor(theta, device=dev)
@@ -345,9 +372,11 @@ def plain_vs_batched_2d(torch, dev):
     e.record()
     e.synchronize()
     batched = 5 * nth * npt / (s.elapsed_time(e) * 1e-3)
-    return {"workload": "2d_tessI_4x4_nc64_1024theta_x_4096pts", "plain_per_call_points_per_s": plain,
-            "plain_precision": "f64", "batched_points_per_s": batched, "batched_precision": "f32",
-            "ratio": batched / plain}
+    return {"workload": "2d_tessI_4x4_nc64_1024theta_x_4096pts", "batched_points_per_s": batched,
+            "batched_precision": "f32", "plain_per_call_f32_points_per_s": plain32,
+            "plain_per_call_f64_points_per_s": plain, "ratio": batched / plain32,
+            "ratio_precision": "f32 batched / f32 plain (same scheme, same precision)",
+            "ratio_vs_f64_plain": batched / plain}
 
 
 def other_configs(torch, dev) -> dict:
@@ -713,8 +742,47 @@ def bench_remap(args, torch, dev) -> dict:
                          "bytes_per_pixel": 16, "traffic": TRAFFIC_REMAP_BYTES_PER_LAUNCH}}
 
 
+def spawn_ranks(n: int) -> int:
+    """`bench.py --gpus N` started without a launcher: run this script under
+    torch.distributed.run with N local ranks (rendezvous on 127.0.0.1) and
+    return its exit status; rank 0 prints the line."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve()), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
+def serving_legs(args, dev) -> dict:
+    """The serving mix: the capacity one GPU has for it (service times per
+    request type), the mix at 200 req/s, at 80 % of that capacity for
+    --serve-sustained-seconds, and at the configuration's 2000 req/s for
+    --serve-seconds (above capacity: the server keeps serving transforms while
+    registrations queue)."""
+    from cpabdiffeo_b200.serving_load import capacity_estimate, make_requests, run_load
+    mix = ("1D/2D/3D, nC in {16,64,256,1024}, 1e3-4e6 pts, 10% 200-step registrations (side 64-1024)")
+    out = {"serving_capacity": capacity_estimate(device=dev)}
+    reqs = make_requests(200.0, 2.0, seed=5)
+    out["serving_200hz"] = dict(run_load(reqs, device=dev), arrival_rate_hz=200.0, arrivals_s=2.0)
+    cap = out["serving_capacity"]["capacity_req_per_s"]
+    if args.serve_sustained_seconds > 0:
+        rate = 0.8 * cap
+        reqs = make_requests(rate, args.serve_sustained_seconds, seed=6)
+        out["serving_sustained"] = dict(run_load(reqs, device=dev, time_limit_s=4 * args.serve_sustained_seconds + 60),
+                                        arrival_rate_hz=rate, arrivals_s=args.serve_sustained_seconds, mix=mix)
+    reqs = make_requests(2000.0, args.serve_seconds, seed=4)
+    out["serving"] = dict(run_load(reqs, device=dev, grace_s=1.0), arrival_rate_hz=2000.0,
+                          arrivals_s=args.serve_seconds, mix=mix,
+                          window="arrivals + 1 s; what is still queued or running then is reported, not waited for")
+    return out
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -746,20 +814,8 @@ def main():
     offsets = torch.as_tensor(offsets_h, device=dev)
     pts = torch.as_tensor(pts_h, device=dev)
     out = torch.empty_like(pts)
-    ws = torch.empty(int(sp._ctx.lib.cpab_batched_workspace_bytes(args.theta)), dtype=torch.uint8, device=dev)
     p = dict(dt=DT, nTimeSteps=NT, nStepsODEsolver=NODE)
     stream = torch.cuda.current_stream()
-    k_ev = []
-
-    def step(record=False, scheme=_lib.SCHEME_EXACT):
-        tables = sp.tables_from_theta(theta, DT, 1)
-        if record:
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-        sp.calc_T_batched(tables, pts, out, offsets=offsets, workspace=ws, scheme=scheme, **p)
-        if record:
-            b.record(stream)
-            k_ev.append((a, b))
 
     def barrier():
         if world > 1:
@@ -767,6 +823,20 @@ def main():
 
     from cpabdiffeo_b200 import autotune
     tuned = autotune.tune(sp, sp.tables_from_theta(theta, DT, 1), pts, offsets, _lib.SCHEME_EXACT, **p)
+    # the step (prologue + tile prefix + integration) captured once in a CUDA graph, replayed per step
+    graph_step = sp.capture_batched(args.theta, pts, out, offsets=offsets, scheme=_lib.SCHEME_EXACT, **p)
+    graph_step.theta.copy_(theta)
+    k_ev = []
+
+    def step(record=False):
+        if record:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+        graph_step()
+        if record:
+            b.record(stream)
+            k_ev.append((a, b))
+
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
@@ -783,22 +853,35 @@ def main():
         torch.cuda.nvtx.range_pop()
     barrier()
     ms = s.elapsed_time(e)
-    kern_ms = float(np.mean([a.elapsed_time(b) for a, b in k_ev]))
+    step_ms = float(np.mean([a.elapsed_time(b) for a, b in k_ev]))
     from cpabdiffeo_b200.distributed import max_over_ranks
     ms = max_over_ranks(ms, dev)
     value = n_total * world * args.steps / (ms * 1e-3)
+    out_dev_h = out.cpu().numpy()
+
+    # the integration kernel alone (the graph's other two launches are a few microseconds): eager launches
+    # on the same buffers, timed with events on the launching stream
+    tables = sp.tables_from_theta(theta, DT, 1)
+    ws = torch.empty(int(sp._ctx.lib.cpab_batched_workspace_bytes(args.theta)), dtype=torch.uint8, device=dev)
+    kt = []
+    for _ in range(5):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sp.calc_T_batched(tables, pts, out, offsets=offsets, workspace=ws, scheme=_lib.SCHEME_EXACT, **p)
+        b.record(stream)
+        kt.append((a, b))
+    torch.cuda.synchronize()
+    kern_ms = float(np.median([a.elapsed_time(b) for a, b in kt]))
 
     # end to end through the public API, host buffers (pinned), copies inside the timed region
     pts_pin = torch.from_numpy(pts_h).pin_memory()
     out_pin = torch.empty_like(pts_pin).pin_memory()
     th_pin = torch.from_numpy(theta_h).pin_memory()
-    off_pin = torch.from_numpy(offsets_h).pin_memory()
 
     def e2e_step():
         # the public host-buffer entry point: chunked copy-in / integrate / copy-out on three streams
         sp.calc_T_batched_host(th_pin, pts_pin, out_pin, offsets_h, mysign=1, scheme=_lib.SCHEME_EXACT,
-                               chunks=args.e2e_chunks,
-                               **p)
+                               chunks=args.e2e_chunks, **p)
 
     for _ in range(2):
         e2e_step()
@@ -815,6 +898,8 @@ def main():
     ms_e2e = max_over_ranks(ms_e2e, dev)
     h2d = pts_h.nbytes + theta_h.nbytes + offsets_h.nbytes
     d2h = pts_h.nbytes
+    # the host-buffer result must equal the device-resident one (same inputs, same kernels)
+    e2e_equal = bool(np.array_equal(out_pin.numpy(), out_dev_h))
 
     # the host link alone: the same bytes copied in and out concurrently on two streams (no compute);
     # the end-to-end figure cannot beat n_total / this time
@@ -836,53 +921,47 @@ def main():
         lb.synchronize()
         link_ms.append(la.elapsed_time(lb))
     link_ms = min(link_ms)
-    # the same copies cut into the pipeline's chunks, chunk k copied out after it was copied in (no
-    # compute): the end-to-end pipeline's own copy schedule, whose start (first chunk in alone) and
-    # end (last chunk out alone) run one direction only
-    cuts = np.linspace(0, n_total, args.e2e_chunks + 1).astype(np.int64)
-    chunk_ms = []
-    for _ in range(3):
-        torch.cuda.synchronize()
-        la, lb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        la.record(stream)
-        s_a.wait_stream(stream)
-        for k in range(args.e2e_chunks):
-            o0, o1 = int(cuts[k]), int(cuts[k + 1])
-            with torch.cuda.stream(s_a):
-                pts[o0:o1].copy_(pts_pin[o0:o1], non_blocking=True)
-                ev_k = torch.cuda.Event()
-                ev_k.record(s_a)
-            s_b.wait_event(ev_k)
-            with torch.cuda.stream(s_b):
-                out_pin[o0:o1].copy_(out[o0:o1], non_blocking=True)
-        stream.wait_stream(s_a)
-        stream.wait_stream(s_b)
-        lb.record(stream)
-        lb.synchronize()
-        chunk_ms.append(la.elapsed_time(lb))
-    chunk_ms = min(chunk_ms)
 
     # work accounting (counters) of the timed scheme
     cnt = torch.zeros(_lib.CNT_N, dtype=torch.int64, device=dev)
-    tables = sp.tables_from_theta(theta, DT, 1)
     sp.calc_T_batched(tables, pts, out, offsets=offsets, workspace=ws, counters=cnt, scheme=_lib.SCHEME_EXACT, **p)
     torch.cuda.synchronize()
     cnt_h = cnt.cpu().numpy()
     flops = flops_exact(cnt_h)
-    out_h = out.cpu().numpy()
+
+    # the same workload with FP64 points (the configuration names both precisions)
+    sp64 = CpaSpace([0.0], [1.0], (NC,), device=dev, precision=torch.float64)
+    pts64 = pts.double()
+    out64 = torch.empty_like(pts64)
+    autotune.tune(sp64, sp64.tables_from_theta(theta, DT, 1), pts64, offsets, _lib.SCHEME_EXACT, **p)
+    g64 = sp64.capture_batched(args.theta, pts64, out64, offsets=offsets, scheme=_lib.SCHEME_EXACT, **p)
+    g64.theta.copy_(theta)
+    for _ in range(3):
+        g64()
+    torch.cuda.synchronize()
+    s4, e4 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s4.record(stream)
+    for _ in range(args.steps):
+        g64()
+    e4.record(stream)
+    torch.cuda.synchronize()
+    ms64 = max_over_ranks(s4.elapsed_time(e4), dev) / args.steps
+    out64_h = out64.cpu().numpy()
+    del pts64, out64, g64
 
     # the same workload through the reference's REF scheme (FP32 on the GPU), its own tuned launch shape
     sp_ref = CpaSpace([0.0], [1.0], (NC,), device=dev, precision=torch.float32)
     tab_ref = sp_ref.tables_from_theta(theta, DT, 1)
     tuned_ref = autotune.tune(sp_ref, tab_ref, pts, offsets, _lib.SCHEME_REF, sample_points=2_000_000, **p)
-    sp_ref.calc_T_batched(tab_ref, pts, out, offsets=offsets, workspace=ws, scheme=_lib.SCHEME_REF, **p)
+    cnt_ref = torch.zeros(_lib.CNT_N, dtype=torch.int64, device=dev)
+    sp_ref.calc_T_batched(tab_ref, pts, out, offsets=offsets, workspace=ws, scheme=_lib.SCHEME_REF,
+                          counters=cnt_ref, **p)
     torch.cuda.synchronize()
     s3, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     n_ref_steps = 2
     torch.cuda.nvtx.range_push("timed_ref")
     s3.record(stream)
     for _ in range(n_ref_steps):
-        tab_ref = sp_ref.tables_from_theta(theta, DT, 1)
         sp_ref.calc_T_batched(tab_ref, pts, out, offsets=offsets, workspace=ws, scheme=_lib.SCHEME_REF, **p)
     e3.record(stream)
     torch.cuda.synchronize()
@@ -896,23 +975,26 @@ def main():
             "data": "synthetic (seeded prior draws, log-uniform ragged sizes, uniform points)",
             "config": {"workload": WORKLOAD, "n_theta_per_gpu": args.theta, "points_per_gpu": n_total,
                        "nC": NC, "integration_time": 1.0,
-                       "scheme": "closed form across cells (hitting times, FP64); checked against the "
-                                 "reference calc_T scheme dt=0.02 nT=50 nODE=100 in FP64",
+                       "scheme": "closed form across cells (ClosedFormInt restated: hitting times in FP64)",
                        "precision": "f32 points, f64 hitting times and expm",
+                       "step": "CUDA graph replay: theta -> A -> expm prologue, tile prefix, persistent integration",
                        "l2": "inputs larger than L2 (352 MB of points per GPU)",
                        "parallelism": f"independent shards x{world}"},
             "e2e": {"value": n_total * world * args.steps / (ms_e2e * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "result_equals_device_run": e2e_equal,
                     "link_only_ms": link_ms,
                     "link_bound_points_per_s": n_total * world / (link_ms * 1e-3),
-                    "chunked_copies_only_ms": chunk_ms,
-                    "chunked_copies_points_per_s": n_total * world / (chunk_ms * 1e-3),
-                    "pipeline": f"{args.e2e_chunks} chunks, 3 streams (copy in / integrate / copy out), pinned host buffers"},
+                    "pipeline": f"{args.e2e_chunks} instance groups (1/4, 1/2, 1, ..., 1, 1/2, 1/4 of the points), "
+                                "3 streams (copy in / integrate / copy out), pinned host buffers"},
             "gpu_launches": 3 * args.steps,
             "clocks": clk.summary(),
             "work": {"cell_visits": int(cnt_h[0]), "points": int(cnt_h[3]), "failed": int(cnt_h[4])},
+            "fp64": {"value": n_total * world / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64,
+                     "precision": "f64 points and arithmetic"},
             "ref_scheme_gpu": {"points_per_s": n_total * world / (ms_ref * 1e-3), "ms_per_step": ms_ref,
-                               "precision": "f32", "launch": tuned_ref},
+                               "precision": "f32", "scheme": "reference calc_T dt=0.02 nT=50 nODE=100",
+                               "launch": tuned_ref},
             "launch": tuned}
     if rank == 0:
         peaks = measured_peaks(torch)
@@ -923,14 +1005,40 @@ def main():
                             "peak_source": "measured here: cuBLAS DGEMM 4096^3",
                             "flop_model": f"{EXACT_FLOP_PER_VISIT} per cell visit + {EXACT_FLOP_PER_POINT} per point "
                                           "(log/exp counted as 20)",
-                            "kernel_ms": kern_ms,
+                            "kernel_ms": kern_ms, "step_ms_events": step_ms,
                             "traffic": TRAFFIC_EXACT1D_BYTES_PER_POINT * n_total,
                             "traffic_note": "ncu DRAM bytes of one launch on the 2048-theta case, scaled by points",
                             "algorithmic_flop_per_launch": flops,
                             "hbm_achieved_gbs": 2 * pts_h.nbytes / (kern_ms * 1e-3) / 1e9,
                             "hbm_peak_gbs": peaks.get("hbm_gbs")}
-        # error of both GPU results against the reference scheme in FP64 (oracle) on a sample
+        flops_ref = flops_from_counters(cnt_ref.cpu().numpy(), 1)
+        ach_ref = flops_ref / (ms_ref * 1e-3) / 1e12
+        line["ref_scheme_gpu"]["roofline"] = {
+            "bound": "fp32", "kernel": "k_integrate<1, float, ref>", "achieved": ach_ref,
+            "peak": peaks["fp32_simt_tflops"], "unit": "TFLOP/s", "frac": ach_ref / peaks["fp32_simt_tflops"],
+            "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off",
+            "flop_model": "per step 2*5+2, per midpoint sub-step 5+2*2+4 (algorithmic)"}
+        # errors: the timed FP32 result and the FP64 run against the FP64 closed form (oracle) on 64
+        # instances; both GPU schemes against the reference's calc_T scheme in FP64 on 8
         from oracle import oracle as O
+        rel32 = rel64 = abs32 = 0.0
+        n_cf = 0
+        for i in range(min(64, args.theta)):
+            A = (geo.B @ theta_h[i]).reshape(NC, 2)
+            sl = slice(offsets_h[i], offsets_h[i + 1])
+            x = pts_h[sl].astype(np.float64)[:, 0]
+            ref, _ = O.closed_form_1d(A, NC, x, DT * NT)
+            g32 = out_dev_h[sl].astype(np.float64)[:, 0]
+            den = np.maximum(np.abs(ref), 1e-6)
+            rel32 = max(rel32, float((np.abs(g32 - ref) / den).max()))
+            abs32 = max(abs32, float(np.abs(g32 - ref).max()))
+            rel64 = max(rel64, float((np.abs(out64_h[sl][:, 0] - ref) / den).max()))
+            n_cf += x.size
+        line["error_vs_fp64_closed_form"] = {
+            "max_rel_f32": rel32, "max_abs_f32": abs32, "max_rel_f64": rel64, "instances_checked": min(64, args.theta),
+            "points_checked": n_cf, "tolerance_rel_f32": 1e-5, "tolerance_f64": 1e-12,
+            "relative_to": "max(|closed form|, 1e-6)"}
+        line["fp64"]["max_rel_error_vs_closed_form"] = rel64
         t = O.tess_struct(1, 2, geo.nCs, geo.incs)
         err_exact = err_ref = 0.0
         n_chk = 0
@@ -941,37 +1049,44 @@ def main():
             x = pts_h[sl].astype(np.float64)
             ref, _ = O.calc_T(t, Tro, sAo, x, DT, NT, NODE)
             ref = O.clamp_1d(ref)
-            err_exact = max(err_exact, float(np.abs(out_h[sl].astype(np.float64) - ref).max()))
+            err_exact = max(err_exact, float(np.abs(out_dev_h[sl].astype(np.float64) - ref).max()))
             err_ref = max(err_ref, float(np.abs(out_ref_h[sl].astype(np.float64) - ref).max()))
             n_chk += x.shape[0]
-        line["error_vs_fp64_reference_scheme"] = {"max_abs_timed_result": err_exact, "max_abs_ref_scheme_f32": err_ref,
-                                                  "points_checked": n_chk, "tolerance": 1e-5}
+        line["error_vs_fp64_reference_scheme"] = {"max_abs_closed_form_f32": err_exact,
+                                                  "max_abs_ref_scheme_f32": err_ref,
+                                                  "points_checked": n_chk,
+                                                  "note": "the closed form is the exact flow the reference's "
+                                                          "step scheme approximates"}
         if world == 1 and not args.no_extras:
             r, sample, kind, cores, _ = cpu_reference_rate(theta_h, offsets_h, pts_h, geo, 400_000)
-            line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+            line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
+                                    "scheme": "the reference's calc_T (its own CPU-compiled kernel source, FP64)"}
+            r2, sample2, cores2 = cpu_closed_form_rate(theta_h, offsets_h, pts_h, geo, 4_000_000)
+            line["cpu_baseline_same_scheme"] = {
+                "value": r2, "unit": UNIT, "cores": cores2, "kind": "port", "sample": sample2,
+                "scheme": "closed form (ClosedFormInt restated in C, pinned to the reference's calc_phi), FP64",
+                "gpu_over_cpu_device": value / r2, "gpu_over_cpu_e2e": line["e2e"]["value"] / r2}
             try:
                 line["plain_vs_batched_2d"] = plain_vs_batched_2d(torch, dev)
             except Exception as ex:  # reported, never fatal
                 line["plain_vs_batched_2d"] = {"error": repr(ex)}
+            try:
+                line["batched_2d_ref_f32"] = bench_2d(argparse.Namespace(steps=3, warmup=3), torch, dev)
+                for k in ("metric", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "data"):
+                    line["batched_2d_ref_f32"].pop(k, None)
+            except Exception as ex:
+                line["batched_2d_ref_f32"] = {"error": repr(ex)}
             try:
                 line["other_configs"] = other_configs(torch, dev)
             except Exception as ex:
                 line["other_configs"] = {"error": repr(ex)}
             if args.serve_seconds > 0:
                 try:
-                    from cpabdiffeo_b200.serving_load import make_requests, run_load
-                    # the mix at 200 req/s (latency when the GPU keeps up) before the overload run
-                    reqs = make_requests(200.0, 2.0, seed=5)
-                    line["serving_200hz"] = dict(run_load(reqs, device=dev), arrival_rate_hz=200.0, arrivals_s=2.0)
-                    reqs = make_requests(2000.0, args.serve_seconds, seed=4)
-                    line["serving"] = dict(run_load(reqs, device=dev), arrival_rate_hz=2000.0,
-                                           arrivals_s=args.serve_seconds,
-                                           mix="1D/2D/3D, nC in {16,64,256,1024}, 1e3-4e6 pts, 10% 200-step "
-                                               "registrations (side 64-1024)")
-                    del reqs
+                    line.update(serving_legs(args, dev))
                 except Exception as ex:
                     line["serving"] = {"error": repr(ex)}
         print(json.dumps(line), flush=True)
+    del graph_step
     if world > 1:
         dist.destroy_process_group()
 

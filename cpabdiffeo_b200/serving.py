@@ -13,9 +13,10 @@ Requests of mixed dimension, tessellation and size arrive at any time
   4. advances every running registration job by a slice of MCMC steps on a
      low-priority stream, one slice in flight per job, so registration slices
      and transform batches overlap and transform batches (high-priority
-     streams) are not queued behind long registrations (priority orders
-     kernels: a transform batch may wait for the one likelihood launch in
-     flight, not for a job's remaining steps).
+     streams) are not queued behind long registrations: priority orders
+     kernels, and the registration kernels run capped at a share of the SMs
+     (the rest stays free for transform batches); at most max_jobs jobs run
+     at once, further ones wait without blocking the transforms behind them.
 State kept resident on the GPU: the basis of each space, every job's theta,
 log-likelihood and chain state.  Results do not depend on what else was in
 the batch: the transform kernels are per point, the likelihood reduction has
@@ -77,8 +78,16 @@ class _Record:
 
 
 class CpabServer:
+    """max_jobs: registration jobs running at once (more wait, in arrival
+    order, while transforms keep being admitted); job_sm_fraction: the share
+    of the SMs one registration slice's kernels may occupy (their launches --
+    captured in CUDA graphs -- are capped at that many CTAs), so transform
+    batches on the high-priority streams find free SMs instead of waiting for
+    a registration kernel to drain."""
+
     def __init__(self, device=None, memory_budget_bytes: int | None = None, n_streams: int = 4,
-                 mcmc_slice: int = 20, max_batch_points: int = 1 << 26):
+                 mcmc_slice: int = 20, max_batch_points: int = 1 << 26, max_jobs: int = 8,
+                 job_sm_fraction: float = 0.25):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if memory_budget_bytes is None:
             free, _ = torch.cuda.mem_get_info(self.device)
@@ -101,13 +110,20 @@ class CpabServer:
         self.done: dict[int, _Record] = {}
         self._spaces: dict = {}
         self._priors: dict = {}
+        self.max_jobs = int(max_jobs)
+        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        self.job_max_ctas = max(1, int(sms * job_sm_fraction))
 
     # ---------------------------------------------------------------- helpers
-    def space(self, dim, nCs, tess, precision) -> CpaSpace:
-        key = (dim, tuple(nCs), tess, precision)
+    def space(self, dim, nCs, tess, precision, for_jobs: bool = False) -> CpaSpace:
+        """The space of a request shape; registration jobs get their own
+        context, whose persistent launches are capped at job_max_ctas CTAs."""
+        key = (dim, tuple(nCs), tess, precision, for_jobs)
         sp = self._spaces.get(key)
         if sp is None:
             sp = CpaSpace([0.0] * dim, [1.0] * dim, tuple(nCs), tess=tess, device=self.device, precision=precision)
+            if for_jobs:
+                sp.set_launch(max_ctas=self.job_max_ctas)
             self._spaces[key] = sp
         return sp
 
@@ -179,17 +195,30 @@ class CpabServer:
         self.inflight = still
 
     def _admit(self) -> None:
+        """Admit waiting requests in arrival order while their memory fits;
+        a registration finding max_jobs jobs running stays queued (in order)
+        without holding back the transforms behind it."""
+        kept: deque[_Record] = deque()
+        jobs = len(self.jobs)
         while self.waiting:
-            r = self.waiting[0]
+            r = self.waiting.popleft()
+            is_job = not isinstance(r.req, TransformRequest)
+            if is_job and jobs >= self.max_jobs:
+                kept.append(r)
+                continue
             if self.in_use + r.bytes > self.budget and self.in_use > 0:
-                break                      # wait for memory to free up (always admit when idle)
-            self.waiting.popleft()
+                kept.append(r)             # wait for memory to free up (always admit when idle)
+                kept.extend(self.waiting)
+                self.waiting.clear()
+                break
             r.t_admit = time.perf_counter()
             self.in_use += r.bytes
-            if isinstance(r.req, TransformRequest):
-                self.ready_transforms.append(r)
-            else:
+            if is_job:
                 self._start_job(r)
+                jobs += 1
+            else:
+                self.ready_transforms.append(r)
+        self.waiting = kept
 
     def _launch_transforms(self) -> None:
         if not self.ready_transforms:
@@ -259,7 +288,7 @@ class CpabServer:
 
     def _start_job(self, r: _Record) -> None:
         q: RegistrationRequest = r.req
-        sp = self.space(2, q.nCs, q.tess, torch.float32)
+        sp = self.space(2, q.nCs, q.tess, torch.float32, for_jobs=True)
         stream = self.job_streams[next(self._rr_jobs)]
         with torch.cuda.stream(stream):
             src = torch.as_tensor(np.asarray(q.src, dtype=np.float32), device=self.device)

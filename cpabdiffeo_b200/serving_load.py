@@ -89,7 +89,11 @@ def warm_up(srv: CpabServer, requests) -> int:
     return len(warm)
 
 
-def run_load(requests, device=None, time_limit_s: float = 120.0) -> dict:
+def run_load(requests, device=None, time_limit_s: float = 120.0, grace_s: float | None = None) -> dict:
+    """Replay `requests` in real time.  With grace_s None the server drains
+    (every request is served); otherwise the run stops grace_s after the
+    last arrival and reports what was served by then (an overloaded server
+    never drains), with the requests still queued or running."""
     srv = CpabServer(device=device)
     # spaces, kernels and graph capture warmed by one small request of each shape (not timed)
     n_warm = warm_up(srv, requests)
@@ -104,6 +108,8 @@ def run_load(requests, device=None, time_limit_s: float = 120.0) -> dict:
         srv.step()
         if now > time_limit_s:
             break
+        if grace_s is not None and i == len(requests) and now > (requests[-1][0] if requests else 0.0) + grace_s:
+            break
     wall = time.perf_counter() - t0
     lat = np.asarray([r.t_done - r.t_submit for r in srv.done.values()])
     pts = sum(int(np.asarray(r.req.pts).shape[0]) for r in srv.done.values() if isinstance(r.req, TransformRequest))
@@ -117,4 +123,64 @@ def run_load(requests, device=None, time_limit_s: float = 120.0) -> dict:
         "transform_p50_ms": float(np.percentile(lat_t, 50) * 1e3) if lat_t.size else None,
         "transform_p99_ms": float(np.percentile(lat_t, 99) * 1e3) if lat_t.size else None,
         "warm_up_requests": n_warm,
+        "left_unserved": len(requests) - len(srv.done),
+        "left_registrations": sum(1 for _, q in requests if isinstance(q, RegistrationRequest)) - n_reg,
     }
+
+
+def capacity_estimate(device=None, reg_sides=(128, 512, 1024), reg_steps: int = 40) -> dict:
+    """Requests per second one GPU can serve of the mix, from measured service
+    times of each request type served alone (host work, copies and kernels,
+    one request at a time -- concurrent service overlaps host and device work,
+    so the server can do somewhat better).
+
+    Transforms: for each (dim, grid) of the mix, the service time of 1e3 and
+    1e6 points gives t(n) = o + n / r; the mix's payload is log-uniform in
+    [1e3, 4e6] (mean (4e6 - 1e3) / ln 4000).  Registrations: the per-step time
+    at a few image sides gives t(side) = a + b side^2; sides are uniform in
+    [64, 1024] and each job takes 200 steps.  Capacity = 1 / (0.9 E[t_transform]
+    + 0.1 E[t_registration])."""
+    srv = CpabServer(device=device)
+    rng = np.random.default_rng(11)
+
+    def serve(req) -> float:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        srv.submit(req)
+        srv.run_until_idle()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    mean_n = (4e6 - 1e3) / np.log(4000.0)
+    per_cfg = {}
+    for dim, grids in GRIDS.items():
+        for nCs, tess in grids:
+            prior = Prior.create(build_space(dim, nCs, tess), 0.1, 1.0)
+            theta = prior.sample(1, rng)[0]
+            small = rng.uniform(0, 1, (1000, dim)).astype(np.float32)
+            big = rng.uniform(0, 1, (1_000_000, dim)).astype(np.float32)
+            serve(TransformRequest(dim, nCs, theta, small, tess=tess))          # warm the space and kernels
+            ts = min(serve(TransformRequest(dim, nCs, theta, small, tess=tess)) for _ in range(3))
+            tb = min(serve(TransformRequest(dim, nCs, theta, big, tess=tess)) for _ in range(2))
+            r = (1_000_000 - 1000) / max(tb - ts, 1e-9)
+            o = max(ts - 1000 / r, 0.0)
+            per_cfg[f"{dim}d_{'x'.join(map(str, nCs))}_{tess}"] = {"overhead_ms": o * 1e3, "points_per_s": r,
+                                                                 "mean_ms": (o + mean_n / r) * 1e3}
+    t_tr = float(np.mean([v["mean_ms"] for v in per_cfg.values()])) * 1e-3
+    per_step = {}
+    for side in reg_sides:
+        src = gaussian_filter(rng.uniform(0, 1, (side, side)).astype(np.float32), 8.0)
+        dst = np.roll(src, 2, axis=1)
+        serve(RegistrationRequest(src, dst, n_steps=2 * srv.mcmc_slice, seed=1))  # warm (graph capture)
+        t = serve(RegistrationRequest(src, dst, n_steps=reg_steps, seed=2))
+        per_step[side] = t / reg_steps
+    sides = np.array(sorted(per_step))
+    b, a = np.polyfit(sides.astype(float) ** 2, [per_step[s] for s in sides], 1)
+    e_side2 = (1024 ** 3 - 63 ** 3) / (3 * (1024 - 63))       # E[side^2], side uniform on 64..1024
+    t_reg = 200 * (a + b * e_side2)
+    mean_t = 0.9 * t_tr + 0.1 * t_reg
+    return {"transform_mean_ms": t_tr * 1e3, "registration_mean_ms": t_reg * 1e3,
+            "registration_step_ms": {int(s): v * 1e3 for s, v in per_step.items()},
+            "mean_service_ms": mean_t * 1e3, "capacity_req_per_s": 1.0 / mean_t,
+            "device_seconds_per_second_at_2000_req_per_s": 2000 * mean_t,
+            "transforms": per_cfg}
