@@ -25,8 +25,15 @@ them seeded inputs and stores inputs and outputs as .npz fixtures:
                      for the cells, stored as the per-entry diagonals of its
                      cell blocks (every other entry is zero, checked here).
 
+  pyref/metropolis.npz
+                     cpab/cpaNd/inference/Metropolis.py + Proposal.py, one
+                     chain per image pair, its random draws replaced by the
+                     library's Philox streams (see make_metropolis).
+  pyref/multiscale.npz
+                     cpab/cpaNd/_Multiscale.py propogate_Avees_coarser2fine.
+
 Run where the reference checkout exists (CPAB_REF_ROOT or the default mount):
-    python tests/golden/make_golden_py_ref.py [closedform] [setup]
+    python tests/golden/make_golden_py_ref.py [closedform] [setup] [metropolis] [multiscale]
 """
 from __future__ import annotations
 
@@ -226,13 +233,146 @@ def make_setup(L: Py2Loader, names=None) -> None:
               f"ours d={geo.d}")
 
 
+# ----------------------------------------------------------------------------- Metropolis
+
+
+MH = dict(H=24, W=24, chains=3, steps=14, seed=77, scale=0.05, sigma=0.05, dt=0.02, nT=50, nODE=100)
+
+
+def mh_problem():
+    """A small registration problem: 2D type I 4x4, three image pairs."""
+    from scipy.ndimage import gaussian_filter
+
+    from oracle import oracle as O
+    geo = build_space(2, (4, 4), "I")
+    prior = Prior.create(geo, *PRIOR[2])
+    rng = np.random.default_rng(101)
+    C, H, W = MH["chains"], MH["H"], MH["W"]
+    src = np.stack([gaussian_filter(rng.uniform(0, 1, (H, W)), 2.0).astype(np.float32) for _ in range(C)])
+    dst = np.stack([np.roll(src[c], 1, axis=1) + rng.normal(0, 0.02, (H, W)).astype(np.float32)
+                    for c in range(C)]).astype(np.float32)
+    t = O.tess_struct(2, 1, (4, 4), geo.incs)
+
+    def ll_one(theta, c):
+        sA, Tr = O.expm_cells(2, geo.B @ theta, MH["dt"], -1)
+        v, _ = O.register_ll(t, Tr, sA, src[c], dst[c], MH["sigma"], MH["dt"], MH["nT"], MH["nODE"])
+        return v
+    return geo, prior, src, dst, ll_one
+
+
+class _LLStandIn:
+    """What Metropolis reads from its likelihood: a call theta -> ll, .level
+    and ._ll_func.nPts (Metropolis.py:19, :31-32, :58-59)."""
+
+    def __init__(self, fn, n_pts):
+        self.fn = fn
+        self.level = 0
+        self._ll_func = types.SimpleNamespace(nPts=n_pts)
+
+    def __call__(self, theta):
+        return self.fn(theta)
+
+
+def make_metropolis(L: Py2Loader) -> None:
+    """cpab/cpaNd/inference/Metropolis.py (set_theta :25-40, step :41-85,
+    accept :87-99) with cpab/cpaNd/inference/Proposal.py (:29-64, the
+    diagonal-covariance random walk), one chain per image pair.  The two
+    random sources are replaced by the library's Philox streams: the
+    proposal's multivariate-normal draw (Proposal.py:61-64 passes
+    cov = scale^2 diag(Sigma_CPA)) returns mean + sqrt(diag(cov)) z with z
+    the chain's normals at that step, and np.random.rand returns the chain's
+    uniform at that step -- so the chain can be compared draw for draw."""
+    from oracle import oracle as O
+    met = L.load("cpab/cpaNd/inference/Metropolis.py")
+    prop_mod = L.load("cpab/cpaNd/inference/Proposal.py")
+    geo, prior, src, dst, ll_one = mh_problem()
+    C, d, n_steps, seed = MH["chains"], geo.d, MH["steps"], MH["seed"]
+    key = (seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF)
+    thetas = np.zeros((n_steps + 1, C, d))
+    lls = np.zeros((n_steps + 1, C))
+    acc = np.zeros((n_steps, C), dtype=bool)
+    for c in range(C):
+        state = {"step": 0}
+
+        def draw(mean, cov, c=c):
+            z = O.mcmc_normals(seed, state["step"], C, d)[c]
+            return mean + np.sqrt(np.diag(cov)) * z
+
+        def rand(c=c):
+            ch = np.array([c])
+            ctr = np.stack([ch, np.full_like(ch, state["step"] & 0xFFFFFFFF),
+                            np.full_like(ch, ((state["step"] >> 32) << 8) | 1), np.zeros_like(ch)], -1)
+            r = O.philox4x32_10(ctr.astype(np.uint64), key)
+            return float(O._u53(r[..., 0], r[..., 1])[0])
+
+        prop_mod.draw_from_mvnormal = draw
+        met.np = types.SimpleNamespace(**{k: getattr(np, k) for k in ("log", "float", "zeros_like", "copyto")},
+                                       random=types.SimpleNamespace(rand=rand))
+        ll_func = _LLStandIn(lambda th, c=c: ll_one(th, c), MH["H"] * MH["W"])
+        covs = types.SimpleNamespace(cpa_cov=prior.cov_cpa)
+        proposal = prop_mod.Proposal(ms=types.SimpleNamespace(L_cpa_space=[types.SimpleNamespace()]),
+                                     msp=types.SimpleNamespace(L_cpa_space_covs=[covs]), level=0, scale=MH["scale"])
+        mh = met.Metropolis(ll_func, proposal)
+        mh.set_theta(np.zeros(d))
+        thetas[0, c] = mh.theta_current
+        lls[0, c] = mh.ll_current
+        for k in range(n_steps):
+            state["step"] = k
+            before = mh.nAccepted
+            mh.step()
+            acc[k, c] = mh.nAccepted > before
+            thetas[k + 1, c] = mh.theta_current
+            lls[k + 1, c] = mh.ll_current
+    np.savez_compressed(OUT / "metropolis.npz", src=src, dst=dst, theta=thetas, ll_ave=lls, accepted=acc,
+                        prop_std=np.sqrt(np.diag(prior.cov_cpa)),
+                        **{k: np.array(v) for k, v in MH.items()})
+    print(f"metropolis: {C} chains x {n_steps} steps, accepted {acc.sum()}")
+
+
+# ----------------------------------------------------------------------------- multiscale
+
+
+MS_CASES = [("d1", 1, (4,), "II"), ("d2_II", 2, (2, 2), "II"), ("d2_I", 2, (2, 2), "I"), ("d3_II", 3, (2, 2, 2), "II")]
+
+
+def make_multiscale(L: Py2Loader) -> None:
+    """cpab/cpaNd/_Multiscale.py propogate_Avees_coarser2fine (:166-292):
+    every fine cell's affine map from the coarse level (one level up, twice
+    the cells per axis), on seeded random coarse matrices."""
+    L.stubs["_CpaSpace"] = types.SimpleNamespace(my_dtype=np.float64)
+    ms_mod = L.load("cpab/cpaNd/_Multiscale.py")
+    rng = np.random.default_rng(202)
+    out = {}
+    for name, dim, base, tess in MS_CASES:
+        ne = dim * (dim + 1)
+        per = {("I", 2): 4, ("I", 3): 5}.get((tess, dim), 1)
+
+        def sp(nCs):
+            n = int(np.prod(nCs)) * per
+            t = types.SimpleNamespace(nCx=nCs[0], nCy=nCs[1] if dim > 1 else 1, nCz=nCs[2] if dim > 2 else 1)
+            return types.SimpleNamespace(D=n * ne, tess=tess, tessellation=t)
+        coarse, fine = sp(base), sp(tuple(2 * b for b in base))
+        selfstub = types.SimpleNamespace(lengthAvee=ne, dim_domain=dim, L_cpa_space=[coarse, fine])
+        Ac = rng.standard_normal(coarse.D)
+        Af = np.zeros(fine.D)
+        ms_mod.Multiscale.propogate_Avees_coarser2fine(selfstub, Ac, Af)
+        out[f"{name}_coarse"] = Ac
+        out[f"{name}_fine"] = Af
+    np.savez_compressed(OUT / "multiscale.npz", **out)
+    print("multiscale:", ", ".join(c[0] for c in MS_CASES))
+
+
 def main(argv) -> None:
     L = Py2Loader()
-    what = set(argv[1:]) or {"closedform", "setup"}
+    what = set(argv[1:]) or {"closedform", "setup", "metropolis", "multiscale"}
     if "closedform" in what:
         make_closedform(L)
     if "setup" in what:
         make_setup(L)
+    if "metropolis" in what:
+        make_metropolis(L)
+    if "multiscale" in what:
+        make_multiscale(L)
 
 
 if __name__ == "__main__":

@@ -169,3 +169,50 @@ def test_reference_rerun_reproduces_fixture_when_checkout_present():
     vel = M.vertex_velocities(A, x_tess)
     got = np.array([cfi.calc_phi(float(v), velTess=vel, t=1.0) for v in x[:200]])
     np.testing.assert_array_equal(got, ref[:200])
+
+
+# ----------------------------------------------------------------------------- Metropolis and multiscale
+
+
+def test_metropolis_restatement_matches_reference_chain(oracle_mod):
+    """oracle.mcmc_run (the restatement the GPU chains are checked against)
+    reproduces the reference's Metropolis + Proposal chain (run by
+    make_golden_py_ref.py with the same Philox draws): same accept decisions,
+    same chain, same average log-likelihood."""
+    O = oracle_mod
+    z = np.load(PYREF / "metropolis.npz")
+    geo = build_space(2, (4, 4), "I")
+    H, W = int(z["H"]), int(z["W"])
+    dt, nT, nODE, sigma = float(z["dt"]), int(z["nT"]), int(z["nODE"]), float(z["sigma"])
+    t = O.tess_struct(2, 1, (4, 4), geo.incs)
+
+    def ll_of_theta(theta):
+        out = np.empty(theta.shape[0])
+        for c in range(theta.shape[0]):
+            sA, Tr = O.expm_cells(2, geo.B @ theta[c], dt, -1)
+            out[c], _ = O.register_ll(t, Tr, sA, z["src"][c], z["dst"][c], sigma, dt, nT, nODE)
+        return out
+
+    C, n_steps = int(z["chains"]), int(z["steps"])
+    theta, ll, acc = O.mcmc_run(geo.B, ll_of_theta, np.zeros((C, geo.d)), z["prop_std"], float(z["scale"]),
+                                int(z["seed"]), n_steps, 1.0 / (H * W), rule=0)
+    np.testing.assert_array_equal(acc, z["accepted"])
+    assert 0 < z["accepted"].sum() < C * n_steps             # both outcomes occur
+    np.testing.assert_allclose(theta, z["theta"][-1], rtol=0, atol=1e-13)
+    np.testing.assert_allclose(ll / (H * W), z["ll_ave"][-1], rtol=1e-13)
+
+
+@pytest.mark.parametrize("name,dim,base,tess", [("d1", 1, (4,), "II"), ("d2_II", 2, (2, 2), "II"),
+                                                ("d2_I", 2, (2, 2), "I"), ("d3_II", 3, (2, 2, 2), "II")])
+def test_multiscale_propagation_matches_reference(name, dim, base, tess):
+    """Every fine cell takes its parent's affine map: the nested-cell map of
+    cpabdiffeo_b200.multiscale equals the reference's hand-written
+    propogate_Avees_coarser2fine (cpab/cpaNd/_Multiscale.py:166-292)."""
+    from cpabdiffeo_b200.multiscale import parent_cells
+    z = np.load(PYREF / "multiscale.npz")
+    coarse = build_space(dim, base, tess)
+    fine = build_space(dim, tuple(2 * b for b in base), tess)
+    ne = dim * (dim + 1)
+    Ac = z[f"{name}_coarse"].reshape(coarse.nC, ne)
+    Af = Ac[parent_cells(coarse, fine)].ravel()
+    np.testing.assert_array_equal(Af, z[f"{name}_fine"])
