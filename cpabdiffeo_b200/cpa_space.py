@@ -9,13 +9,14 @@ there is no CPU path.
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 from typing import Sequence
 
 import numpy as np
 import torch
 
 from . import _lib
-from .space import TESS_I, TESS_II, Prior, SpaceGeometry, build_space
+from .space import TESS_I, TESS_II, Prior, SpaceGeometry, basis_from_reference_cache, build_space
 
 _DT = {torch.float64: _lib.CPAB_F64, torch.float32: _lib.CPAB_F32}
 
@@ -96,7 +97,11 @@ class CpaSpace:
     def __init__(self, XMINS: Sequence[float], XMAXS: Sequence[float], nCs: Sequence[int],
                  zero_v_across_bdry: Sequence[bool] | None = None, vol_preserve: bool = False,
                  tess: str = TESS_II, valid_outside: bool | None = None, device=None,
-                 precision: torch.dtype = torch.float64):
+                 precision: torch.dtype = torch.float64, reference_cache=None):
+        """reference_cache: the reference's cache directory of subspaces
+        (its <cache>/<dim>d/<subspace string>/subspace.pkl files); when it
+        holds this space, its B is used (checked to span the same subspace),
+        so theta values from the reference's runs map to the same A."""
         dim = len(nCs)
         if vol_preserve:
             raise NotImplementedError("volume-preserving spaces are outside the built path")
@@ -113,6 +118,10 @@ class CpaSpace:
         self.zero_v_across_bdry = tuple(zero_v_across_bdry if zero_v_across_bdry is not None else (True,) * dim)
         self.geo = build_space(dim, tuple(int(n) for n in nCs), tess, tuple(self.XMINS), tuple(self.XMAXS),
                                self.zero_v_across_bdry)
+        if reference_cache is not None:
+            B_ref = basis_from_reference_cache(self.geo, reference_cache)
+            if B_ref is not None:
+                self.geo = dataclasses.replace(self.geo, B=B_ref)
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.precision = precision
         self.nCs = self.geo.nCs

@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import hashlib
 import os
+import pickle
 from dataclasses import dataclass, field
 from functools import lru_cache
 from pathlib import Path
@@ -283,6 +284,76 @@ def build_space(dim: int, nCs: tuple, tess: str = TESS_II, xmins: tuple | None =
         except OSError:
             pass
     return geo
+
+
+# --------------------------------------------------------------------------- the reference's subspace cache
+
+
+def reference_subspace_string(dim: int, tess: str, xmins, xmaxs, nCs, zero_v_across_bdry,
+                              valid_outside: bool = False) -> str:
+    """The name of the reference's cached subspace for a zero-boundary space
+    without volume preservation, zero values or wrap-around
+    (create_subspace_string, cpab/cpaNd/_CpaSpace.py:525-566): numpy
+    integer arrays printed as "[a b]", then brackets dropped and blanks
+    turned into "_"."""
+    def arr(v):
+        return "[" + " ".join(str(int(x)) for x in v) + "]"
+    xbdry = [0 if z else 1 for z in zero_v_across_bdry]
+    s = ""
+    if dim > 1:
+        s += "tess" + str(tess) + "_"
+    s += f"R{dim}toR{dim}"
+    s += f"_MINS_{arr(xmins)}_MAXS_{arr(xmaxs)}"
+    s += f"_nc_{arr(nCs)}"
+    s += f"_Xbdr_{arr(xbdry)}"
+    s = s.replace("[", "").replace("]", "").replace(" ", "_")
+    if tess == TESS_I and dim == 2:
+        s += f"_ext_{int(bool(valid_outside))}"
+    return s
+
+
+class _Py2Unpickler(pickle.Unpickler):
+    """Python 2 pickles of numpy / scipy objects: the module paths of those
+    releases mapped to today's."""
+    RENAMES = {"copy_reg": "copyreg", "__builtin__": "builtins", "numpy.core.multiarray": "numpy._core.multiarray",
+               "numpy.core.numeric": "numpy._core.numeric"}
+
+    def find_class(self, module, name):
+        return super().find_class(self.RENAMES.get(module, module), name)
+
+
+def load_reference_subspace(path) -> dict:
+    """The reference's cached subspace, <cache>/<dim>d/<subspace string>/subspace.pkl
+    (cpab/cpaNd/_CpaSpace.py:224-230; written by cpab/cpa2d/CpaSpace.py:
+    173-178 and its 1D/3D twins: a dict with B, nConstraints, nEdges or
+    nSides, constraintMat, cont_constraints_are_separable).  The files are
+    Python 2 pickles: strings are read as latin-1, which also restores numpy
+    arrays' raw data."""
+    with open(path, "rb") as f:
+        d = _Py2Unpickler(f, encoding="latin1").load()
+    if not isinstance(d, dict) or "B" not in d:
+        raise ValueError(f"{path}: not a cpabDiffeo subspace file")
+    d["B"] = np.ascontiguousarray(np.asarray(d["B"], dtype=np.float64))
+    return d
+
+
+def basis_from_reference_cache(geo: "SpaceGeometry", cache_dir) -> np.ndarray | None:
+    """B from the reference's cache directory for this space, or None when the
+    file is absent.  The cached B must span the same subspace as this
+    package's construction (checked); using it keeps theta interchangeable
+    with the reference's runs (B is defined only up to a rotation)."""
+    path = Path(cache_dir) / f"{geo.dim}d" / reference_subspace_string(
+        geo.dim, geo.tess, geo.xmins, geo.xmaxs, geo.nCs, geo.zero_v_across_bdry) / "subspace.pkl"
+    if not path.exists():
+        return None
+    B = load_reference_subspace(path)["B"]
+    if B.shape != geo.B.shape:
+        raise ValueError(f"{path}: B has shape {B.shape}, the space needs {geo.B.shape}")
+    if np.abs(B.T @ B - np.eye(B.shape[1])).max() > 1e-8:
+        raise ValueError(f"{path}: B is not orthonormal")
+    if np.abs(geo.B @ (geo.B.T @ B) - B).max() > 1e-8:
+        raise ValueError(f"{path}: B spans a different subspace")
+    return B
 
 
 # --------------------------------------------------------------------------- prior
