@@ -63,10 +63,11 @@ def parse():
     ap.add_argument("--serve-sustained-seconds", type=float, default=10.0,
                     help="seconds of arrivals at 80%% of the measured serving capacity; 0 skips that run")
     ap.add_argument("--workload", default="batched_1d",
-                    choices=["batched_1d", "batched_2d_nc64", "remap_ssd", "mcmc_c3"],
+                    choices=["batched_1d", "batched_2d_nc64", "exact_2d_nc64", "remap_ssd", "mcmc_c3"],
                     help="batched_1d: the headline (1D nC=100, 4096 theta, ragged); batched_2d_nc64: the reference "
                          "scheme in FP32 on 2D tess I 4x4 (nC=64), 4096 theta x 8192 points, for the "
-                         "integration kernel's FP32 roofline; remap_ssd: remap + SSD of 256 pairs of 256x256 "
+                         "integration kernel's FP32 roofline; exact_2d_nc64: the same through the exact scheme "
+                         "(facet hitting times); remap_ssd: remap + SSD of 256 pairs of 256x256 "
                          "images through FP32 maps, for its HBM roofline; mcmc_c3: 256-chain MCMC registration of "
                          "256x256 FP32 image pairs, for the fused likelihood kernel's roofline")
     return ap.parse_args()
@@ -523,9 +524,11 @@ def flops_ref_2d(cnt) -> float:
     return steps * (2 * C_CELL_2D + M_2D) + float(cnt[2]) * (C_CELL_2D + 2 * M_2D + 4 * 2)
 
 
-def bench_2d(args, torch, dev) -> dict:
-    """The reference scheme in FP32, batched, on 2D tess I 4x4 (nC=64):
-    4096 theta x 8192 uniform points (268 MB in, larger than L2)."""
+def bench_2d(args, torch, dev, exact: bool = False) -> dict:
+    """FP32, batched, on 2D tess I 4x4 (nC=64): 4096 theta x 8192 uniform
+    points (268 MB in, larger than L2), through the reference scheme or
+    (exact=True) the exact scheme (hitting times), with the error against the
+    FP64 oracle of the same scheme on 4 instances."""
     from cpabdiffeo_b200 import _lib, autotune
     from cpabdiffeo_b200.cpa_space import CpaSpace
     from cpabdiffeo_b200.space import Prior
@@ -536,8 +539,8 @@ def bench_2d(args, torch, dev) -> dict:
     x = torch.as_tensor(rng.uniform(0, 1, size=(nth * npt, 2)), dtype=torch.float32, device=dev)
     out = torch.empty_like(x)
     p = dict(dt=DT, nTimeSteps=NT, nStepsODEsolver=NODE)
-    tuned = autotune.tune(sp, sp.tables_from_theta(theta, DT, 1), x, None, _lib.SCHEME_REF,
-                          sample_points=1 << 22, **p)
+    scheme = _lib.SCHEME_EXACT if exact else _lib.SCHEME_REF
+    tuned = autotune.tune(sp, sp.tables_from_theta(theta, DT, 1), x, None, scheme, sample_points=1 << 22, **p)
     stream = torch.cuda.current_stream()
     k_ev = []
 
@@ -546,7 +549,7 @@ def bench_2d(args, torch, dev) -> dict:
         if record:
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
-        sp.calc_T_batched(tables, x, out, **p)
+        sp.calc_T_batched(tables, x, out, scheme=scheme, **p)
         if record:
             b.record(stream)
             k_ev.append((a, b))
@@ -567,7 +570,7 @@ def bench_2d(args, torch, dev) -> dict:
     kern_ms = float(np.mean([a.elapsed_time(b) for a, b in k_ev]))
     n = nth * npt
     cnt = torch.zeros(_lib.CNT_N, dtype=torch.int64, device=dev)
-    sp.calc_T_batched(sp.tables_from_theta(theta, DT, 1), x, out, counters=cnt, **p)
+    sp.calc_T_batched(sp.tables_from_theta(theta, DT, 1), x, out, counters=cnt, scheme=scheme, **p)
     cnt_h = cnt.cpu().numpy()
     flops = flops_ref_2d(cnt_h)
     peaks = measured_peaks(torch)
@@ -575,25 +578,34 @@ def bench_2d(args, torch, dev) -> dict:
     # error against the FP64 oracle of the reference scheme on the first 4 instances
     from oracle import oracle as O
     t = O.tess_struct(2, sp.geo.tess_code, sp.geo.nCs, sp.geo.incs)
+    F, nb = O.cell_facets(t, sp.geo.cells)
     out_h, x_h, th_h = out.cpu().numpy(), x.cpu().numpy(), theta.cpu().numpy()
-    err = 0.0
+    err = err_fine = 0.0
     for i in range(4):
         A = (sp.geo.B @ th_h[i]).reshape(sp.nC, 6)
         sAo, Tro = O.expm_cells(2, A, DT, 1)
         sl = slice(i * npt, (i + 1) * npt)
-        ref, _ = O.calc_T(t, Tro, sAo, x_h[sl].astype(np.float64), DT, NT, NODE)
+        xi = x_h[sl].astype(np.float64)
+        if exact:
+            ref, _ = O.calc_T_exact(t, Tro, sAo, F, nb, xi, DT, NT, NODE)
+        else:
+            ref, _ = O.calc_T(t, Tro, sAo, xi, DT, NT, NODE)
+        fine, _ = O.calc_T(t, Tro, sAo, xi, DT, NT, 10000)
         err = max(err, float(np.abs(out_h[sl].astype(np.float64) - ref).max()))
+        err_fine = max(err_fine, float(np.abs(out_h[sl].astype(np.float64) - fine).max()))
     return {"metric": METRIC, "value": n * args.steps / (ms * 1e-3), "unit": UNIT, "n_gpus": 1,
             "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded prior draws, uniform points)",
-            "config": {"workload": "batched_2d_tessI_4x4_nc64_4096theta_x_8192pts", "scheme": "reference calc_T",
+            "config": {"workload": "batched_2d_tessI_4x4_nc64_4096theta_x_8192pts",
+                       "scheme": "exact (facet hitting times)" if exact else "reference calc_T",
                        "dt": DT, "nTimeSteps": NT, "nStepsODE": NODE,
                        "l2": "inputs larger than L2 (268 MB of points)"},
             "gpu_launches": 2 * args.steps, "clocks": clk.summary(), "launch": tuned,
             "work": {"kept_steps": int(cnt_h[0]), "fallback_steps": int(cnt_h[1]), "substeps": int(cnt_h[2]),
-                     "points": int(cnt_h[3])},
-            "roofline": {"bound": "fp32", "kernel": "k_integrate<2, tess I, float, ref>", "achieved": achieved,
+                     "points": int(cnt_h[3]), "crossings": int(cnt_h[_lib.CNT_CROSSINGS])},
+            "roofline": {"bound": "fp32", "kernel": f"k_integrate<2, tess I, float, {'exact' if exact else 'ref'}>",
+                         "achieved": achieved,
                          "peak": peaks["fp32_simt_tflops"], "unit": "TFLOP/s",
                          "frac": achieved / peaks["fp32_simt_tflops"],
                          "peak_source": "measured here: cuBLAS SGEMM 8192^3, TF32 off",
@@ -601,7 +613,10 @@ def bench_2d(args, torch, dev) -> dict:
                                        f"{C_CELL_2D}+2*{M_2D}+8 (algorithmic, before compensation)",
                          "kernel_ms": kern_ms, "algorithmic_flop_per_launch": flops,
                          "traffic": TRAFFIC_2D_BYTES_PER_LAUNCH},
-            "error_vs_fp64_oracle": {"max_abs": err, "points_checked": 4 * npt, "tolerance": 1e-5}}
+            "error_vs_fp64_oracle": {"max_abs": err, "points_checked": 4 * npt, "tolerance": 1e-5,
+                                     "oracle": "exact scheme (oracle/cpab_oracle_exact.c)" if exact
+                                     else "reference scheme (calc_T restated)",
+                                     "max_abs_vs_ref_scheme_nODE_1e4": err_fine}}
 
 
 def remap_ssd_c3(torch, dev, theta, src, dst, reps: int = 10) -> dict:
@@ -798,8 +813,8 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if args.workload != "batched_1d":
-        line = {"batched_2d_nc64": bench_2d, "remap_ssd": bench_remap, "mcmc_c3": bench_mcmc_c3}[args.workload](
-            args, torch, dev)
+        line = {"batched_2d_nc64": bench_2d, "remap_ssd": bench_remap, "mcmc_c3": bench_mcmc_c3,
+                "exact_2d_nc64": lambda a, t, d: bench_2d(a, t, d, exact=True)}[args.workload](args, torch, dev)
         if rank == 0:
             print(json.dumps(line), flush=True)
         return
@@ -1070,12 +1085,13 @@ def main():
                 line["plain_vs_batched_2d"] = plain_vs_batched_2d(torch, dev)
             except Exception as ex:  # reported, never fatal
                 line["plain_vs_batched_2d"] = {"error": repr(ex)}
-            try:
-                line["batched_2d_ref_f32"] = bench_2d(argparse.Namespace(steps=3, warmup=3), torch, dev)
-                for k in ("metric", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "data"):
-                    line["batched_2d_ref_f32"].pop(k, None)
-            except Exception as ex:
-                line["batched_2d_ref_f32"] = {"error": repr(ex)}
+            for key, ex_flag in (("batched_2d_ref_f32", False), ("batched_2d_exact_f32", True)):
+                try:
+                    line[key] = bench_2d(argparse.Namespace(steps=3, warmup=3), torch, dev, exact=ex_flag)
+                    for k in ("metric", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "data"):
+                        line[key].pop(k, None)
+                except Exception as ex:
+                    line[key] = {"error": repr(ex)}
             try:
                 line["other_configs"] = other_configs(torch, dev)
             except Exception as ex:
