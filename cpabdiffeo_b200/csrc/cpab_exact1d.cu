@@ -228,8 +228,14 @@ size_t exact1d_smem_bytes(int nC, int tile_pts, int sort, int prec)
     return b;
 }
 
+// Resident CTAs of 256 threads the register allocation must allow per SM
+// (a build-time choice: 1 leaves registers to the compiler).
+#ifndef CPAB_EXACT1D_MIN_BLOCKS
+#define CPAB_EXACT1D_MIN_BLOCKS 1
+#endif
+
 template <typename Real>
-__global__ void __launch_bounds__(256) k_exact1d(IntegrateArgs a)
+__global__ void __launch_bounds__(256, CPAB_EXACT1D_MIN_BLOCKS) k_exact1d(IntegrateArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nC = a.t.nC;
