@@ -878,15 +878,30 @@ def main():
     # on the same buffers, timed with events on the launching stream
     tables = sp.tables_from_theta(theta, DT, 1)
     ws = torch.empty(int(sp._ctx.lib.cpab_batched_workspace_bytes(args.theta)), dtype=torch.uint8, device=dev)
-    kt = []
-    for _ in range(5):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        sp.calc_T_batched(tables, pts, out, offsets=offsets, workspace=ws, scheme=_lib.SCHEME_EXACT, **p)
-        b.record(stream)
-        kt.append((a, b))
-    torch.cuda.synchronize()
-    kern_ms = float(np.median([a.elapsed_time(b) for a, b in kt]))
+
+    def kernel_ms(offs, n_uniform=0, reps=5):
+        kt = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            if offs is None:
+                sp.calc_T_batched(tables, pts[:n_uniform * args.theta], out[:n_uniform * args.theta],
+                                  scheme=_lib.SCHEME_EXACT, **p)
+            else:
+                sp.calc_T_batched(tables, pts, out, offsets=offs, workspace=ws, scheme=_lib.SCHEME_EXACT, **p)
+            b.record(stream)
+            kt.append((a, b))
+        torch.cuda.synchronize()
+        return float(np.median([a.elapsed_time(b) for a, b in kt]))
+
+    kern_ms = kernel_ms(offsets)
+    # load balance of the ragged batch: the same instances with equal point counts (same total up to
+    # rounding) in a uniform launch
+    n_eq = n_total // args.theta
+    uniform_ms = kernel_ms(None, n_uniform=n_eq)
+    load_balance = {"ragged_points_per_s": n_total / (kern_ms * 1e-3),
+                    "uniform_points_per_s": n_eq * args.theta / (uniform_ms * 1e-3),
+                    "achieved_over_ideal": (n_total / kern_ms) / (n_eq * args.theta / uniform_ms)}
 
     # end to end through the public API, host buffers (pinned), copies inside the timed region
     pts_pin = torch.from_numpy(pts_h).pin_memory()
@@ -1005,6 +1020,7 @@ def main():
             "gpu_launches": 3 * args.steps,
             "clocks": clk.summary(),
             "work": {"cell_visits": int(cnt_h[0]), "points": int(cnt_h[3]), "failed": int(cnt_h[4])},
+            "load_balance": load_balance,
             "fp64": {"value": n_total * world / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64,
                      "precision": "f64 points and arithmetic"},
             "ref_scheme_gpu": {"points_per_s": n_total * world / (ms_ref * 1e-3), "ms_per_step": ms_ref,

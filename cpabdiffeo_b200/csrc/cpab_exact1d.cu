@@ -233,6 +233,10 @@ size_t exact1d_smem_bytes(int nC, int tile_pts, int sort, int prec)
 #ifndef CPAB_EXACT1D_MIN_BLOCKS
 #define CPAB_EXACT1D_MIN_BLOCKS 1
 #endif
+// Tile order of a CTA: strided over the batch (0) or one contiguous range (1).
+#ifndef CPAB_EXACT1D_CONTIGUOUS
+#define CPAB_EXACT1D_CONTIGUOUS 0
+#endif
 
 template <typename Real>
 __global__ void __launch_bounds__(256, CPAB_EXACT1D_MIN_BLOCKS) k_exact1d(IntegrateArgs a)
@@ -268,8 +272,17 @@ __global__ void __launch_bounds__(256, CPAB_EXACT1D_MIN_BLOCKS) k_exact1d(Integr
     e.step = 1.0 / (double)nC;
     // the reference gives up after nC crossings
     const int cap = nC;
+#if CPAB_EXACT1D_CONTIGUOUS
+    // each CTA takes a contiguous range of tiles, so consecutive tiles mostly
+    // belong to the same instance and its tables are built once per range
+    const int64_t per = (ntiles + gridDim.x - 1) / gridDim.x;
+    const int64_t t_first = (int64_t)blockIdx.x * per, t_end = min(ntiles, t_first + per);
+    for (int64_t tile = t_first; tile < t_end; ++tile) {
+        if (((tile - t_first) & 7) == 0 && cta_cancelled(a.cancel, a.counters)) break;
+#else
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         if ((((tile - blockIdx.x) / gridDim.x) & 7) == 0 && cta_cancelled(a.cancel, a.counters)) break;
+#endif
         if (threadIdx.x == 0) {
             s_tile = decode_tile(a.batch, tile);
             s_claim = 0;

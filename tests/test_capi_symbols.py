@@ -55,8 +55,12 @@ def test_ctx_create_validation():
     # pts and out overlap -> ALIAS (reference raises, cpab/cpaNd/_CpaCalcs.py:388)
     assert lib.cpab_calc_T(h, 8, 8, 4096, 4096 + 64, 10, 0, 0, 0.02, 50, 100, None, None) == 4
     assert b"same memory" in lib.cpab_last_error_string(h)
-    assert lib.cpab_calc_T(h, 8, 8, 16, 16, 10, 0, 2, 0.02, 50, 100, None, None) == 10  # exact needs 1D
+    # the 2D/3D exact scheme needs the facet tables a context gets on a device
+    assert lib.cpab_calc_T(h, 8, 8, 16, 16, 10, 0, 2, 0.02, 50, 100, None, None) == 10
+    assert b"facet" in lib.cpab_last_error_string(h)
     assert lib.cpab_set_launch(h, 48, 0, 0) == 1
+    assert lib.cpab_set_max_ctas(h, -1) == 1
+    assert lib.cpab_set_max_ctas(h, 37) == 0 and lib.cpab_set_max_ctas(h, 0) == 0
     assert lib.cpab_ctx_destroy(h) == 0
 
 
