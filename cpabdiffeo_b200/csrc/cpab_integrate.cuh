@@ -3,6 +3,8 @@
 // (calc_T) and the fused registration likelihood.
 #pragma once
 
+#include <math_constants.h>
+
 #include "cpab_device.cuh"
 
 namespace cpab {
@@ -313,91 +315,109 @@ __device__ __forceinline__ int lookup_d(const Tess &t, const double *p, float)
     return fast_cell<DIM, TESS>(t, x);
 }
 
-// out = expm(t A)[p; 1]: x(t) = p + sum_k t^k/k! u_k, u_1 = L p + b,
-// u_k = L u_{k-1}, until the terms fall below the rounding of the sum.
+// The flow inside a cell over a time t <= h (one sub-step) as a Taylor
+// polynomial of fixed degree kExactDeg: x(t) = p + sum_{k=1..K} t^k/k! u_k,
+// u_1 = L p + b, u_k = L u_{k-1} (A = [L | b], read from global memory: the
+// code runs rarely and must not hold the matrix in registers).  The omitted
+// terms are below (t |L|)^K / (K+1)! of the first; exact_substep_cross
+// checks that this is below the rounding of FP64 (t |L| below ~0.1 at
+// K = 10; a sub-step of 2e-4 allows |L| up to ~500) and otherwise keeps the
+// reference scheme's sub-step end.
+constexpr int kExactDeg = 10;
+
 template <int DIM>
-__device__ __noinline__ void flow_taylor(const double *__restrict__ A, const double *p, double t, double *out)
+__device__ __forceinline__ void affine_lin(const double *__restrict__ A, const double *u, double *out)
 {
-    double u[DIM], x[DIM];
 #pragma unroll
     for (int r = 0; r < DIM; ++r) {
-        double v = __ldg(A + r * (DIM + 1) + DIM);
+        double v = 0.0;
 #pragma unroll
-        for (int m = 0; m < DIM; ++m) v = fma(__ldg(A + r * (DIM + 1) + m), p[m], v);
-        u[r] = t * v;
-        x[r] = p[r] + u[r];
+        for (int m = 0; m < DIM; ++m) v = fma(__ldg(A + r * (DIM + 1) + m), u[m], v);
+        out[r] = v;
+    }
+}
+
+template <int DIM>
+__device__ __forceinline__ void velocity(const double *__restrict__ A, const double *p, double *v)
+{
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) {
+        double s = __ldg(A + r * (DIM + 1) + DIM);
+#pragma unroll
+        for (int m = 0; m < DIM; ++m) s = fma(__ldg(A + r * (DIM + 1) + m), p[m], s);
+        v[r] = s;
+    }
+}
+
+// out = expm(t A)[p; 1] (out may alias p); false when the last term is not
+// below FP64 rounding of the displacement's first term
+template <int DIM>
+__device__ __forceinline__ bool flow_taylor(const double *__restrict__ A, const double *p, double t, double *out)
+{
+    double u[DIM], x[DIM];
+    velocity<DIM>(A, p, u);
+    double coef = t, first = 0.0, last = 0.0;
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) {
+        x[r] = fma(coef, u[r], p[r]);
+        first = fmax(first, fabs(coef * u[r]));
     }
 #pragma unroll 1
-    for (int k = 2; k <= 40; ++k) {
-        double nu[DIM], big = 0.0, xm = 0.0;
-#pragma unroll
-        for (int r = 0; r < DIM; ++r) {
-            double v = 0.0;
-#pragma unroll
-            for (int m = 0; m < DIM; ++m) v = fma(__ldg(A + r * (DIM + 1) + m), u[m], v);
-            nu[r] = v * (t / k);
-        }
+    for (int k = 2; k <= kExactDeg; ++k) {
+        double nu[DIM];
+        affine_lin<DIM>(A, u, nu);
+        coef *= t / k;
+        last = 0.0;
 #pragma unroll
         for (int r = 0; r < DIM; ++r) {
             u[r] = nu[r];
-            x[r] += u[r];
-            big = fmax(big, fabs(u[r]));
-            xm = fmax(xm, fabs(x[r]));
+            x[r] = fma(coef, u[r], x[r]);
+            last = fmax(last, fabs(coef * u[r]));
         }
-        if (!(big > 1e-18 * (xm + 1e-300))) break;
     }
 #pragma unroll
     for (int r = 0; r < DIM; ++r) out[r] = x[r];
+    return last <= 1e-17 * first;
 }
 
 // First root in [0, s] of g(t) = F . x(t) + F[DIM] along the flow of A from
-// p, given g(0) = g0 < 0 < g(s): the Taylor coefficients of g
-// (c_k = F . u_k / k!) and a safeguarded Newton iteration on that polynomial.
+// p, given g(0) = g0 < 0 < g(s): the Taylor coefficients of g,
+// c_k = F . u_k / k!, and a safeguarded Newton iteration on that polynomial.
+// Returns NaN when the degree does not resolve g to FP64 rounding over [0, s].
 template <int DIM>
-__device__ __noinline__ double facet_hit_time(const double *__restrict__ A, const double *__restrict__ F,
-                                              const double *p, double s, double g0)
+__device__ __forceinline__ double facet_hit_time(const double *__restrict__ A, const double *__restrict__ F,
+                                                 const double *p, double s, double g0)
 {
-    constexpr int KMAX = 24;
-    double c[KMAX + 1];
+    double c[kExactDeg + 1];
     c[0] = g0;
-    double u[DIM], fact = 1.0, sk = 1.0, scale = fabs(g0);
-    int K = 1;
+    double u[DIM], Fn[DIM];
 #pragma unroll
-    for (int r = 0; r < DIM; ++r) {
-        double v = __ldg(A + r * (DIM + 1) + DIM);
-#pragma unroll
-        for (int m = 0; m < DIM; ++m) v = fma(__ldg(A + r * (DIM + 1) + m), p[m], v);
-        u[r] = v;
-    }
+    for (int r = 0; r < DIM; ++r) Fn[r] = __ldg(F + r);
+    velocity<DIM>(A, p, u);
+    double inv_fact = 1.0;
 #pragma unroll 1
-    for (int k = 1; k <= KMAX; ++k) {
+    for (int k = 1; k <= kExactDeg; ++k) {
         if (k > 1) {
             double nu[DIM];
-#pragma unroll
-            for (int r = 0; r < DIM; ++r) {
-                double v = 0.0;
-#pragma unroll
-                for (int m = 0; m < DIM; ++m) v = fma(__ldg(A + r * (DIM + 1) + m), u[m], v);
-                nu[r] = v;
-            }
+            affine_lin<DIM>(A, u, nu);
 #pragma unroll
             for (int r = 0; r < DIM; ++r) u[r] = nu[r];
         }
-        fact *= k;
-        sk *= s;
+        inv_fact /= k;
         double d = 0.0;
 #pragma unroll
-        for (int r = 0; r < DIM; ++r) d = fma(__ldg(F + r), u[r], d);
-        c[k] = d / fact;
-        K = k;
-        const double term = fabs(c[k]) * sk;
-        scale = fmax(scale, term);
-        if (k >= 2 && !(term > 1e-18 * scale)) break;
+        for (int r = 0; r < DIM; ++r) d = fma(Fn[r], u[r], d);
+        c[k] = d * inv_fact;
     }
-    auto P = [&](double t, double &dP) {
-        double v = c[K], dv = 0.0;
+    // the last term over [0, s] against the first (FP64 rounding)
+    double sK = 1.0;
 #pragma unroll 1
-        for (int k = K - 1; k >= 0; --k) {
+    for (int k = 0; k < kExactDeg; ++k) sK *= s;
+    if (!(fabs(c[kExactDeg]) * sK <= 1e-17 * (fabs(g0) + fabs(c[1]) * s))) return CUDART_NAN;
+    auto P = [&](double t, double &dP) {
+        double v = c[kExactDeg], dv = 0.0;
+#pragma unroll 1
+        for (int k = kExactDeg - 1; k >= 0; --k) {
             dv = fma(dv, t, v);
             v = fma(v, t, c[k]);
         }
@@ -431,8 +451,8 @@ __device__ __noinline__ double facet_hit_time(const double *__restrict__ A, cons
 // the cap, q is the end point of the flow in the current cell (as in the
 // reference scheme, which keeps its sub-step's end wherever it lands).
 template <int DIM, int TESS, typename Real>
-__device__ __noinline__ int exact_substep_cross(const Tess &t, ExactCross &ex, int c, const PState<DIM, Real> &st,
-                                                PState<DIM, Real> &q)
+__device__ __forceinline__ int exact_substep_cross(const Tess &t, ExactCross &ex, int c,
+                                                   const PState<DIM, Real> &st, PState<DIM, Real> &q)
 {
     constexpr int NH = DIM + 1, NE = DIM * NH;
     double p[DIM], y[DIM];
@@ -441,7 +461,8 @@ __device__ __noinline__ int exact_substep_cross(const Tess &t, ExactCross &ex, i
     double s = ex.h;
 #pragma unroll 1
     for (int crossings = 0;;) {
-        if (lookup_d<DIM, TESS>(t, y, Real(0)) == c) {
+        // (the caller found q outside c; later ends are looked up here)
+        if (crossings > 0 && lookup_d<DIM, TESS>(t, y, Real(0)) == c) {
             q.set(y);
             return c;
         }
@@ -480,7 +501,12 @@ __device__ __noinline__ int exact_substep_cross(const Tess &t, ExactCross &ex, i
             q.set(p);
             return c;
         }
-        flow_taylor<DIM>(ex.A + (size_t)c * NE, p, s, y);
+        if (!flow_taylor<DIM>(ex.A + (size_t)c * NE, p, s, y)) {
+            // the neighbour's flow is too fast for the polynomial over the
+            // rest of the sub-step: the reference scheme's sub-step end
+            ++ex.unresolved;
+            return cell_of<DIM, TESS>(t, q);
+        }
     }
 }
 

@@ -88,7 +88,7 @@ struct ArraySnk {
 };
 
 template <int DIM, int TESS, typename Real, int SCHEME>
-__global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
+__device__ __forceinline__ void integrate_body(const IntegrateArgs &a)
 {
     constexpr int NE = DIM * (DIM + 1);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -173,6 +173,24 @@ __global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
             if (c_unres) atomicAdd(a.counters + CNT_FAILED, c_unres);
         }
     }
+}
+
+template <int DIM, int TESS, typename Real, int SCHEME>
+__global__ void __launch_bounds__(256) k_integrate(IntegrateArgs a)
+{
+    integrate_body<DIM, TESS, Real, SCHEME>(a);
+}
+
+// The exact scheme's exit resolution (FP64, rare) would otherwise set the
+// register count of the whole kernel; the bound keeps CPAB_EXACT_MIN_BLOCKS
+// CTAs of 256 threads resident per SM.
+#ifndef CPAB_EXACT_MIN_BLOCKS
+#define CPAB_EXACT_MIN_BLOCKS 3
+#endif
+template <int DIM, int TESS, typename Real>
+__global__ void __launch_bounds__(256, CPAB_EXACT_MIN_BLOCKS) k_integrate_exact(IntegrateArgs a)
+{
+    integrate_body<DIM, TESS, Real, SCHEME_EXACT>(a);
 }
 
 // ------------------------------------------------------------ trajectory
@@ -457,7 +475,9 @@ static cudaError_t launch_integrate_t(const IntegrateArgs &a, const LaunchCfg &c
     constexpr int NE = DIM * (DIM + 1);
     size_t smem = (size_t)(1 + TableLayout<Real>::kTParts) * a.t.nC * NE * sizeof(Real);
     if (a.sort) smem += ((size_t)a.t.nC + 2 * (size_t)a.batch.tile_pts) * sizeof(int);
-    auto kern = k_integrate<DIM, TESS, Real, SCHEME>;
+    void (*kern)(IntegrateArgs);
+    if constexpr (SCHEME == SCHEME_EXACT) kern = k_integrate_exact<DIM, TESS, Real>;
+    else kern = k_integrate<DIM, TESS, Real, SCHEME>;
     if (smem > kSmemOptInAbove) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
