@@ -207,6 +207,24 @@ __device__ __forceinline__ void advance(bool fast, const PState<DIM, double> &s,
         exact_midpoint<DIM>(q.p, A, h);
     }
 }
+// Paired FP32 arithmetic (sm_100's FFMA2 / FADD2: two lanes of float math per
+// instruction, each rounded as its scalar twin) for the (x, y) coordinates:
+// the column-major cell matrix gives column k as the pair (M[0][k], M[1][k]).
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
+// hi + lo += d for coordinates 0 and 1 at once (PState::add, twice)
+template <int DIM>
+__device__ __forceinline__ void add_pair(PState<DIM, float> &q, float2 d)
+{
+    const float2 hi = make_float2(q.hi[0], q.hi[1]), lo = make_float2(q.lo[0], q.lo[1]);
+    const float2 sm = __fadd2_rn(hi, d);
+    const float2 l2 = __fadd2_rn(lo, __fadd2_rn(d, neg2(__fadd2_rn(sm, neg2(hi)))));
+    const float2 x = __fadd2_rn(sm, l2);
+    q.hi[0] = sm.x; q.hi[1] = sm.y;
+    q.lo[0] = l2.x; q.lo[1] = l2.y;
+    q.x[0] = x.x; q.x[1] = x.y;
+}
+
 template <int DIM>
 __device__ __forceinline__ void advance(bool fast, const PState<DIM, float> &s, const float *A, const float *T,
                                         const float *, float, PState<DIM, float> &q)
@@ -215,10 +233,24 @@ __device__ __forceinline__ void advance(bool fast, const PState<DIM, float> &s, 
     float m[NE], d[DIM];
     // d = (T - I)[x; 1] for a closed-form step, (S - I)[x; 1] for a sub-step
     load_cell<DIM>(fast ? T : A, m);
-    cm_affine<DIM>(d, m, s.x);
     q = s;
+    if constexpr (DIM == 1) {
+        cm_affine<DIM>(d, m, s.x);
+        q.add(0, d[0]);
+    } else {
+        // rows 0 and 1 as one pair: the same fmaf sequence as cm_affine per row
+        float2 d01 = make_float2(m[DIM * DIM], m[DIM * DIM + 1]);
 #pragma unroll
-    for (int r = 0; r < DIM; ++r) q.add(r, d[r]);
+        for (int k = 0; k < DIM; ++k)
+            d01 = __ffma2_rn(make_float2(m[k * DIM], m[k * DIM + 1]), make_float2(s.x[k], s.x[k]), d01);
+        add_pair<DIM>(q, d01);
+        if constexpr (DIM == 3) {
+            float d2 = m[DIM * DIM + 2];
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) d2 = fmaf(m[k * DIM + 2], s.x[k], d2);
+            q.add(2, d2);
+        }
+    }
 }
 
 // ------------------------------------------------------------ exact scheme (2D/3D)

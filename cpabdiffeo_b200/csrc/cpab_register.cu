@@ -107,6 +107,8 @@ __device__ __forceinline__ Real bilinear(const float *img, int H, int W, double 
 // rounding toward -inf; taps combined in float as taps_combine<float>.
 // Split in issue (the four loads) and combine so that a thread can keep the
 // taps of several pixels in flight.
+__device__ __forceinline__ float2 neg2f(float2 a) { return make_float2(-a.x, -a.y); }
+
 struct TapsF {
     float v[4];
     float wx, wy;
@@ -115,12 +117,16 @@ struct TapsF {
 
 __device__ __forceinline__ void tapsf_issue(const float *img, int H, int W, float px, float py, TapsF &t)
 {
+    // x and y as one pair (sm_100's FADD2; each lane rounds as its scalar twin)
     constexpr float kRound = 12582912.0f;  // 1.5 * 2^23
-    const float sx = __fadd_rd(px, kRound), sy = __fadd_rd(py, kRound);
-    const float fx0 = sx - kRound, fy0 = sy - kRound;  // floor(px), floor(py) for |p| < 2^22
+    const float2 p2 = make_float2(px, py);
+    const float2 s2 = __fadd2_rd(p2, make_float2(kRound, kRound));
+    const float2 f2 = __fadd2_rn(s2, make_float2(-kRound, -kRound));  // floor(px), floor(py) for |p| < 2^22
+    const float sx = s2.x, sy = s2.y, fx0 = f2.x, fy0 = f2.y;
     t.in = fx0 > -2.0f && fx0 < (float)W + 1.0f && fy0 > -2.0f && fy0 < (float)H + 1.0f;  // false for NaN
-    t.wx = px - fx0;
-    t.wy = py - fy0;
+    const float2 w2 = __fadd2_rn(p2, make_float2(-fx0, -fy0));
+    t.wx = w2.x;
+    t.wy = w2.y;
     const int c0 = t.in ? __float_as_int(sx) - 0x4B400000 : -2;
     const int r0 = t.in ? __float_as_int(sy) - 0x4B400000 : -2;
     if ((unsigned)c0 < (unsigned)(W - 1) && (unsigned)r0 < (unsigned)(H - 1)) {
@@ -141,9 +147,10 @@ __device__ __forceinline__ void tapsf_issue(const float *img, int H, int W, floa
 __device__ __forceinline__ float tapsf_combine(const TapsF &t)
 {
     if (!t.in) return 0.0f;
-    const float top = fmaf(t.wx, t.v[1] - t.v[0], t.v[0]);
-    const float bot = fmaf(t.wx, t.v[3] - t.v[2], t.v[2]);
-    return fmaf(t.wy, bot - top, top);
+    // top and bottom rows as one pair: fmaf(wx, v1 - v0, v0), fmaf(wx, v3 - v2, v2)
+    const float2 lo = make_float2(t.v[0], t.v[2]);
+    const float2 tb = __ffma2_rn(make_float2(t.wx, t.wx), __fadd2_rn(make_float2(t.v[1], t.v[3]), neg2f(lo)), lo);
+    return fmaf(t.wy, tb.y - tb.x, tb.x);
 }
 
 __device__ __forceinline__ float bilinear_f(const float *img, int H, int W, float px, float py)
@@ -158,8 +165,11 @@ template <typename MapT, bool FCOORD>
 __device__ __forceinline__ MapT remap_sample(const RemapArgs &a, const float *src, MapT mx, MapT my)
 {
     if (FCOORD)
-        return (MapT)bilinear_f(src, a.H, a.W, fmaf((float)mx, (float)a.sx, (float)a.ox),
-                                fmaf((float)my, (float)a.sy, (float)a.oy));
+    {
+        const float2 p = __ffma2_rn(make_float2((float)mx, (float)my), make_float2((float)a.sx, (float)a.sy),
+                                    make_float2((float)a.ox, (float)a.oy));
+        return (MapT)bilinear_f(src, a.H, a.W, p.x, p.y);
+    }
     return bilinear<MapT>(src, a.H, a.W, (double)mx * a.sx + a.ox, (double)my * a.sy + a.oy);
 }
 
@@ -284,8 +294,10 @@ __global__ void __launch_bounds__(256, 4) k_remap_ssd_bulk(RemapArgs a)
                     if (j < n) {
                         MapT mx, my;
                         load_pair(m + 2 * j, mx, my);
-                        tapsf_issue(src, a.H, a.W, fmaf((float)mx, (float)a.sx, (float)a.ox),
-                                    fmaf((float)my, (float)a.sy, (float)a.oy), t[u]);
+                        const float2 pp = __ffma2_rn(make_float2((float)mx, (float)my),
+                                                     make_float2((float)a.sx, (float)a.sy),
+                                                     make_float2((float)a.ox, (float)a.oy));
+                        tapsf_issue(src, a.H, a.W, pp.x, pp.y, t[u]);
                     }
                 }
 #pragma unroll
