@@ -274,9 +274,17 @@ CPAB_HD int fast_cell_2d_tri(const Tess &t, const float *p)
     if (p[0] > 0.0f && p[0] < t.fhi[0] && p[1] > 0.0f && p[1] < t.fhi[1]) {
         // strictly inside the domain (the common case): the clamps below are
         // no-ops and none of the boundary rules applies -- same result
+#ifdef __CUDA_ARCH__
+        // both axes as one pair (FMUL2 / FADD2, each lane rounded as its scalar twin)
+        const float2 uw = __fmul2_rn(make_float2(p[0], p[1]), make_float2(t.finv_inc[0], t.finv_inc[1]));
+        const float kx = floorf(uw.x), ky = floorf(uw.y);
+        const float2 xy = __fadd2_rn(uw, make_float2(-kx, -ky));
+        const float x = xy.x, y = xy.y;
+#else
         const float u = p[0] * t.finv_inc[0], w = p[1] * t.finv_inc[1];
         const float kx = floorf(u), ky = floorf(w);
         const float x = u - kx, y = w - ky;
+#endif
         const int c = ((int)fminf(kx, (float)(t.nC0 - 1)) + (int)fminf(ky, (float)(t.nC1 - 1)) * t.nC0) * 4;
         const float omx = 1.0f - x;
         return c + ((x < y) ? ((omx < y) ? 2 : 3) : ((omx < y) ? 1 : 0));
