@@ -1,6 +1,5 @@
 // cpab_capi_register.cu -- C ABI of the remap / registration-likelihood
 // kernels (declared in include/cpab_b200.h).
-#include <algorithm>
 #include <cmath>
 
 #include "cpab_ctx.h"
@@ -54,14 +53,10 @@ int check_images(cpab_ctx *ctx, int N, int H, int W)
 
 extern "C" {
 
-// tile partials per image: the linear tiles of the plain and bulk paths or
-// the 2D tiles of the window path, whichever is more
-int64_t remap_tiles(int H, int W) { return std::max(tiles_of(H, W, kRemapTilePx), remap_window_tiles(H, W)); }
-
 size_t cpab_remap_workspace_bytes(int N, int H, int W)
 {
     if (N < 0 || H < 1 || W < 1) return 0;
-    return ws_layout(N, remap_tiles(H, W)).total;
+    return ws_layout(N, tiles_of(H, W, kRemapTilePx)).total;
 }
 
 int cpab_remap_ssd(cpab_ctx *ctx, const void *map, int map_precision, const float *src, const float *dst, int N,
@@ -81,7 +76,8 @@ int cpab_remap_ssd(cpab_ctx *ctx, const void *map, int map_precision, const floa
         return fail(ctx, CPAB_BAD_ARG, "pixel mapping is not finite");
     CPAB_CHECK_ALIGN(ctx, {map, map_precision == CPAB_F64 ? 8u : 4u, "map"}, {src, 4, "src"}, {dst, 4, "dst"},
                      {warped, 4, "warped"}, {ll, 8, "ll"}, {workspace, 8, "workspace"});
-    const WsLayout L = ws_layout(N, remap_tiles(H, W));
+    const int64_t tpi = tiles_of(H, W, kRemapTilePx);
+    const WsLayout L = ws_layout(N, tpi);
     RemapArgs a;
     memset(&a, 0, sizeof(a));
     a.map = map;

@@ -20,7 +20,6 @@
 // chunks (cpab_reduce.cuh finish_tile_chunks), added per image in index
 // order by the last tile to finish, so the sum does not depend on the tile
 // size either.  A result is therefore the same alone and inside any batch.
-#include <climits>
 #include <cmath>
 
 #include <math_constants.h>
@@ -344,143 +343,6 @@ __global__ void __launch_bounds__(256, 4) k_remap_ssd_bulk(RemapArgs a)
     }
 }
 
-// Window path (float maps with float coordinates): output tiles of
-// kWinTY x kWinTX pixels.  A first pass stages the tile's map in shared
-// memory and takes the bounding box of its bilinear footprints; the source
-// window under that box -- zero outside the image, like the taps -- is then
-// loaded into shared memory once, coalesced, and every pixel takes its four
-// taps from there: no bounds tests and no global gathers per pixel.  A tile
-// whose footprint is larger than kWinCap floats (a strongly contracting map)
-// samples the image in global memory instead.  Per-pixel arithmetic equals
-// the other paths' (taps, weights and the combination, the SSD term); the
-// sum follows this tiling, in a fixed order.
-constexpr int kWinTY = 32, kWinTX = 64, kWinCap = 6144;
-constexpr int kWinPer = kWinTY * kWinTX / 256;  // pixels per thread
-
-int64_t remap_window_tiles(int H, int W)
-{
-    return (int64_t)((H + kWinTY - 1) / kWinTY) * ((W + kWinTX - 1) / kWinTX);
-}
-
-__global__ void __launch_bounds__(256, 4) k_remap_ssd_win(RemapArgs a)
-{
-    __shared__ __align__(16) float2 s_map[kWinTY * kWinTX];
-    __shared__ float s_win[kWinCap];
-    __shared__ int s_box[8][4];
-    __shared__ int s_win_geo[4];  // x0, y0, width, fits
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int tx_n = (a.W + kWinTX - 1) / kWinTX, ty_n = (a.H + kWinTY - 1) / kWinTY;
-    const int tpi = tx_n * ty_n;
-    const int64_t ntiles = (int64_t)tpi * a.N, npx = (int64_t)a.H * a.W;
-    const double k = -0.5 / (a.sigma * a.sigma);
-    const float sx = (float)a.sx, sy = (float)a.sy, ox = (float)a.ox, oy = (float)a.oy;
-    const float2 *gmap = static_cast<const float2 *>(a.map);
-    constexpr float kRound = 12582912.0f;  // 1.5 * 2^23
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const int inst = (int)(tile / tpi);
-        const int t_in = (int)(tile - (int64_t)inst * tpi);
-        const int ty0 = (t_in / tx_n) * kWinTY, tx0 = (t_in % tx_n) * kWinTX;
-        const float *src = a.src + (int64_t)inst * npx;
-        // pass 1: the map into shared memory, the footprints' bounding box
-        int bx0 = INT_MAX, by0 = INT_MAX, bx1 = INT_MIN, by1 = INT_MIN;
-#pragma unroll
-        for (int u = 0; u < kWinPer; ++u) {
-            const int i = u * 256 + tid, r = ty0 + i / kWinTX, c = tx0 + i % kWinTX;
-            float2 m = make_float2(0.f, 0.f);
-            if (r < a.H && c < a.W) {
-                m = gmap[(int64_t)inst * npx + (int64_t)r * a.W + c];
-                const float2 p = __ffma2_rn(m, make_float2(sx, sy), make_float2(ox, oy));
-                const float2 f = __fadd2_rn(__fadd2_rd(p, make_float2(kRound, kRound)), make_float2(-kRound, -kRound));
-                if (f.x > -2.0f && f.x < (float)a.W + 1.0f && f.y > -2.0f && f.y < (float)a.H + 1.0f) {
-                    bx0 = min(bx0, (int)f.x);
-                    bx1 = max(bx1, (int)f.x);
-                    by0 = min(by0, (int)f.y);
-                    by1 = max(by1, (int)f.y);
-                }
-            }
-            s_map[i] = m;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            bx0 = min(bx0, __shfl_xor_sync(FULL, bx0, o));
-            by0 = min(by0, __shfl_xor_sync(FULL, by0, o));
-            bx1 = max(bx1, __shfl_xor_sync(FULL, bx1, o));
-            by1 = max(by1, __shfl_xor_sync(FULL, by1, o));
-        }
-        if (lane == 0) {
-            s_box[warp][0] = bx0;
-            s_box[warp][1] = by0;
-            s_box[warp][2] = bx1;
-            s_box[warp][3] = by1;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            int x0 = INT_MAX, y0 = INT_MAX, x1 = INT_MIN, y1 = INT_MIN;
-            for (int w = 0; w < 8; ++w) {
-                x0 = min(x0, s_box[w][0]);
-                y0 = min(y0, s_box[w][1]);
-                x1 = max(x1, s_box[w][2]);
-                y1 = max(y1, s_box[w][3]);
-            }
-            const int ww = x1 - x0 + 2, wh = y1 - y0 + 2;  // taps c0..c0+1, r0..r0+1
-            const bool fits = x1 >= x0 && (int64_t)ww * wh <= kWinCap;
-            s_win_geo[0] = x0;
-            s_win_geo[1] = y0;
-            s_win_geo[2] = fits ? ww : 0;
-            s_win_geo[3] = fits ? wh : 0;
-        }
-        __syncthreads();
-        const int wx0 = s_win_geo[0], wy0 = s_win_geo[1], ww = s_win_geo[2], wh = s_win_geo[3];
-        // pass 2: the source window, row by row (a warp per row, lanes along it)
-        for (int rr = warp; rr < wh; rr += 8) {
-            const int r = wy0 + rr;
-            for (int cc = lane; cc < ww; cc += 32) {
-                const int c = wx0 + cc;
-                s_win[rr * ww + cc] = (r >= 0 && r < a.H && c >= 0 && c < a.W) ? __ldg(src + (int64_t)r * a.W + c)
-                                                                                 : 0.0f;
-            }
-        }
-        __syncthreads();
-        // pass 3: sample, compare, sum (pixels in the thread's fixed order)
-        double acc = 0.0;
-#pragma unroll
-        for (int u = 0; u < kWinPer; ++u) {
-            const int i = u * 256 + tid, r = ty0 + i / kWinTX, c = tx0 + i % kWinTX;
-            if (r >= a.H || c >= a.W) continue;
-            const float2 p = __ffma2_rn(s_map[i], make_float2(sx, sy), make_float2(ox, oy));
-            float w;
-            if (ww > 0) {
-                const float2 s2 = __fadd2_rd(p, make_float2(kRound, kRound));
-                const float2 f = __fadd2_rn(s2, make_float2(-kRound, -kRound));
-                const bool in = f.x > -2.0f && f.x < (float)a.W + 1.0f && f.y > -2.0f && f.y < (float)a.H + 1.0f;
-                const float2 wxy = __fadd2_rn(p, make_float2(-f.x, -f.y));
-                w = 0.0f;
-                if (in) {
-                    const int c0 = __float_as_int(s2.x) - 0x4B400000, r0 = __float_as_int(s2.y) - 0x4B400000;
-                    const float *q = s_win + (r0 - wy0) * ww + (c0 - wx0);
-                    const float2 lo = make_float2(q[0], q[ww]);
-                    const float2 tb = __ffma2_rn(make_float2(wxy.x, wxy.x),
-                                                 __fadd2_rn(make_float2(q[1], q[ww + 1]), neg2f(lo)), lo);
-                    w = fmaf(wxy.y, tb.y - tb.x, tb.x);
-                }
-            } else {
-                w = bilinear_f(src, a.H, a.W, p.x, p.y);
-            }
-            const int64_t off = (int64_t)inst * npx + (int64_t)r * a.W + c;
-            if (a.warped) a.warped[off] = w;
-            if (a.dst) {
-                const double e = (double)w - (double)__ldg(a.dst + off);
-                acc += e * e * k;
-            }
-        }
-        // the tile's partial; its barrier also releases s_map and s_win for the next tile
-        if (a.dst)
-            store_tile_partial(acc, 0, tile, a.partials);
-        else
-            __syncthreads();
-    }
-}
-
 template <typename MapT, bool FCOORD>
 static cudaError_t launch_remap_bulk(const RemapArgs &a, cudaStream_t s)
 {
@@ -531,20 +393,9 @@ cudaError_t launch_remap_ssd(const RemapArgs &a, int map_prec, cudaStream_t s)
                       (reinterpret_cast<uintptr_t>(a.map) % 16 == 0) &&
                       (!a.dst || reinterpret_cast<uintptr_t>(a.dst) % 16 == 0);
     cudaError_t e;
-    int tpi = (int)((npx + a.tile_px - 1) / a.tile_px);
-    if (fcoord) {
-        // float maps with exact float coordinates: the window path, any alignment
-        const int64_t ntiles = remap_window_tiles(a.H, a.W) * a.N;
-        LaunchCfg cfg;
-        cfg.block = 256;
-        int64_t grid = persistent_grid(k_remap_ssd_win, cfg, 0);
-        if (grid > ntiles) grid = ntiles;
-        k_remap_ssd_win<<<(unsigned)grid, 256, 0, s>>>(a);
-        e = cudaGetLastError();
-        tpi = (int)remap_window_tiles(a.H, a.W);
-    } else if (bulk) {
+    if (bulk) {
         if (map_prec == PREC_F64) e = launch_remap_bulk<double, false>(a, s);
-        else e = launch_remap_bulk<float, false>(a, s);
+        else e = fcoord ? launch_remap_bulk<float, true>(a, s) : launch_remap_bulk<float, false>(a, s);
     } else {
         dim3 grid((unsigned)((npx + a.tile_px - 1) / a.tile_px), (unsigned)a.N);
         if (map_prec == PREC_F64) k_remap_ssd<double, false><<<grid, 256, 0, s>>>(a);
@@ -554,6 +405,7 @@ cudaError_t launch_remap_ssd(const RemapArgs &a, int map_prec, cudaStream_t s)
     }
     if (e != cudaSuccess || !a.dst) return e;
     // per-image sums of the tile partials, in tile order
+    const int tpi = (int)((npx + a.tile_px - 1) / a.tile_px);
     k_sum_partials<<<(a.N + 127) / 128, 128, 0, s>>>(a.partials, tpi, a.N, a.ll);
     return cudaGetLastError();
 }

@@ -42,9 +42,6 @@ struct RegisterArgs {
 };
 
 cudaError_t launch_remap_ssd(const RemapArgs &a, int map_prec, cudaStream_t s);
-// Output tiles of the window path (float maps with float coordinates); the
-// partials workspace needs max(this, linear tiles) entries per image.
-int64_t remap_window_tiles(int H, int W);
 // Dynamic shared memory of k_register_ll: the tables and one double2 point slot per tile pixel.
 size_t register_smem_bytes(int nC, int tile_px, int prec);
 cudaError_t launch_register_ll(const RegisterArgs &a, int prec, const LaunchCfg &cfg, cudaStream_t s);
