@@ -323,6 +323,15 @@ __device__ void stage_exact_substeps(const double *gA, const double *gT, int nC,
 // What a lane needs to resolve an exit: the instance's signed A (global,
 // row-major [nC, DIM*(DIM+1)]), the facet tables, the sub-step length and
 // the lane's counters.
+// Parked exits a warp resolves together, and the votes the oldest may wait
+// (integrate_range).
+#ifndef CPAB_EXACT_CROSS_BATCH
+#define CPAB_EXACT_CROSS_BATCH 16
+#endif
+#ifndef CPAB_EXACT_CROSS_WAIT
+#define CPAB_EXACT_CROSS_WAIT 96
+#endif
+
 struct ExactCross {
     const double *A;
     const double *F;
@@ -348,108 +357,153 @@ __device__ __forceinline__ int lookup_d(const Tess &t, const double *p, float)
 }
 
 // The flow inside a cell over a time t <= h (one sub-step) as a Taylor
-// polynomial of fixed degree kExactDeg: x(t) = p + sum_{k=1..K} t^k/k! u_k,
-// u_1 = L p + b, u_k = L u_{k-1} (A = [L | b], read from global memory: the
-// code runs rarely and must not hold the matrix in registers).  The omitted
-// terms are below (t |L|)^K / (K+1)! of the first; exact_substep_cross
-// checks that this is below the rounding of FP64 (t |L| below ~0.1 at
-// K = 10; a sub-step of 2e-4 allows |L| up to ~500) and otherwise keeps the
-// reference scheme's sub-step end.
+// polynomial: x(t) = p + sum_{k>=1} w_k, w_k = t^k/k! u_k, u_1 = L p + b,
+// u_k = L u_{k-1} (A = [L | b], loaded into registers once per call).  The
+// series stops at the first degree K whose omitted terms are provably below
+// FP64 rounding of the first: with r = t |L| / (K+1) < 1 (|L| the max row
+// sum), |w_{K+j}| <= |w_K| r^j, so the rest sums to at most |w_K| r/(1-r).
+// At sub-step lengths (t |L| ~ 1e-3) that is K = 6 or 7; kExactDeg caps it,
+// and a flow the cap does not resolve (t |L| above ~0.1) is reported so that
+// exact_substep_cross keeps the reference scheme's sub-step end.
 constexpr int kExactDeg = 10;
+constexpr double kTaylorTol = 1e-17;
 
 template <int DIM>
-__device__ __forceinline__ void affine_lin(const double *__restrict__ A, const double *u, double *out)
+__device__ __forceinline__ void load_affine(const double *__restrict__ A, double *Ar, double &lnorm)
+{
+    lnorm = 0.0;
+#pragma unroll
+    for (int r = 0; r < DIM; ++r) {
+        double rs = 0.0;
+#pragma unroll
+        for (int m = 0; m <= DIM; ++m) {
+            Ar[r * (DIM + 1) + m] = __ldg(A + r * (DIM + 1) + m);
+            if (m < DIM) rs += fabs(Ar[r * (DIM + 1) + m]);
+        }
+        lnorm = fmax(lnorm, rs);
+    }
+}
+
+template <int DIM>
+__device__ __forceinline__ void affine_lin(const double *Ar, const double *u, double *out)
 {
 #pragma unroll
     for (int r = 0; r < DIM; ++r) {
         double v = 0.0;
 #pragma unroll
-        for (int m = 0; m < DIM; ++m) v = fma(__ldg(A + r * (DIM + 1) + m), u[m], v);
+        for (int m = 0; m < DIM; ++m) v = fma(Ar[r * (DIM + 1) + m], u[m], v);
         out[r] = v;
     }
 }
 
 template <int DIM>
-__device__ __forceinline__ void velocity(const double *__restrict__ A, const double *p, double *v)
+__device__ __forceinline__ void velocity(const double *Ar, const double *p, double *v)
 {
 #pragma unroll
     for (int r = 0; r < DIM; ++r) {
-        double s = __ldg(A + r * (DIM + 1) + DIM);
+        double s = Ar[r * (DIM + 1) + DIM];
 #pragma unroll
-        for (int m = 0; m < DIM; ++m) s = fma(__ldg(A + r * (DIM + 1) + m), p[m], s);
+        for (int m = 0; m < DIM; ++m) s = fma(Ar[r * (DIM + 1) + m], p[m], s);
         v[r] = s;
     }
 }
 
-// out = expm(t A)[p; 1] (out may alias p); false when the last term is not
-// below FP64 rounding of the displacement's first term
+// out = expm(t A)[p; 1] (out may alias p); false when kExactDeg terms do
+// not bring the omitted rest below FP64 rounding of the first term
 template <int DIM>
 __device__ __forceinline__ bool flow_taylor(const double *__restrict__ A, const double *p, double t, double *out)
 {
+    double Ar[DIM * (DIM + 1)], lnorm;
+    load_affine<DIM>(A, Ar, lnorm);
     double u[DIM], x[DIM];
-    velocity<DIM>(A, p, u);
-    double coef = t, first = 0.0, last = 0.0;
+    velocity<DIM>(Ar, p, u);
+    double coef = t, first = 0.0;
 #pragma unroll
     for (int r = 0; r < DIM; ++r) {
         x[r] = fma(coef, u[r], p[r]);
         first = fmax(first, fabs(coef * u[r]));
     }
+    const double tl = fabs(t) * lnorm;
+    bool ok = false;
 #pragma unroll 1
     for (int k = 2; k <= kExactDeg; ++k) {
         double nu[DIM];
-        affine_lin<DIM>(A, u, nu);
+        affine_lin<DIM>(Ar, u, nu);
         coef *= t / k;
-        last = 0.0;
+        double wk = 0.0;
 #pragma unroll
         for (int r = 0; r < DIM; ++r) {
             u[r] = nu[r];
             x[r] = fma(coef, u[r], x[r]);
-            last = fmax(last, fabs(coef * u[r]));
+            wk = fmax(wk, fabs(coef * u[r]));
+        }
+        const double rr = tl / (k + 1);
+        if (rr < 0.5 && wk * rr <= kTaylorTol * (1.0 - rr) * first) {
+            ok = true;
+            break;
         }
     }
 #pragma unroll
     for (int r = 0; r < DIM; ++r) out[r] = x[r];
-    return last <= 1e-17 * first;
+    return ok || first == 0.0;
 }
 
 // First root in [0, s] of g(t) = F . x(t) + F[DIM] along the flow of A from
 // p, given g(0) = g0 < 0 < g(s): the Taylor coefficients of g,
-// c_k = F . u_k / k!, and a safeguarded Newton iteration on that polynomial.
-// Returns NaN when the degree does not resolve g to FP64 rounding over [0, s].
+// c_k = F . u_k / k!, up to the degree whose omitted rest is below FP64
+// rounding of g over [0, s] (the bound of flow_taylor times |F|_1), and a
+// safeguarded Newton iteration on that polynomial.  Returns NaN when
+// kExactDeg terms do not resolve g to that rounding.
 template <int DIM>
 __device__ __forceinline__ double facet_hit_time(const double *__restrict__ A, const double *__restrict__ F,
                                                  const double *p, double s, double g0)
 {
+    double Ar[DIM * (DIM + 1)], lnorm;
+    load_affine<DIM>(A, Ar, lnorm);
     double c[kExactDeg + 1];
     c[0] = g0;
-    double u[DIM], Fn[DIM];
+    double u[DIM], Fn[DIM], f1 = 0.0;
 #pragma unroll
-    for (int r = 0; r < DIM; ++r) Fn[r] = __ldg(F + r);
-    velocity<DIM>(A, p, u);
-    double inv_fact = 1.0;
+    for (int r = 0; r < DIM; ++r) {
+        Fn[r] = __ldg(F + r);
+        f1 += fabs(Fn[r]);
+    }
+    velocity<DIM>(Ar, p, u);
+    const double sl = s * lnorm;
+    double inv_fact = 1.0, sk = 1.0, scale = 0.0;
+    int K = 0;
 #pragma unroll 1
     for (int k = 1; k <= kExactDeg; ++k) {
         if (k > 1) {
             double nu[DIM];
-            affine_lin<DIM>(A, u, nu);
+            affine_lin<DIM>(Ar, u, nu);
 #pragma unroll
             for (int r = 0; r < DIM; ++r) u[r] = nu[r];
         }
         inv_fact /= k;
-        double d = 0.0;
+        sk *= s;
+        double d = 0.0, un = 0.0;
 #pragma unroll
-        for (int r = 0; r < DIM; ++r) d = fma(Fn[r], u[r], d);
+        for (int r = 0; r < DIM; ++r) {
+            d = fma(Fn[r], u[r], d);
+            un = fmax(un, fabs(u[r]));
+        }
         c[k] = d * inv_fact;
+        if (k == 1) {
+            scale = fabs(g0) + fabs(c[1]) * s;
+        } else {
+            const double rr = sl / (k + 1);
+            if (rr < 0.5 && f1 * un * inv_fact * sk * rr <= kTaylorTol * (1.0 - rr) * scale) {
+                K = k;
+                break;
+            }
+        }
     }
-    // the last term over [0, s] against the first (FP64 rounding)
-    double sK = 1.0;
-#pragma unroll 1
-    for (int k = 0; k < kExactDeg; ++k) sK *= s;
-    if (!(fabs(c[kExactDeg]) * sK <= 1e-17 * (fabs(g0) + fabs(c[1]) * s))) return CUDART_NAN;
+    if (K == 0) return CUDART_NAN;
     auto P = [&](double t, double &dP) {
-        double v = c[kExactDeg], dv = 0.0;
+        double v = c[K], dv = 0.0;
 #pragma unroll 1
-        for (int k = kExactDeg - 1; k >= 0; --k) {
+        for (int k = K - 1; k >= 0; --k) {
             dv = fma(dv, t, v);
             v = fma(v, t, c[k]);
         }
@@ -627,11 +681,21 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
     // finishes after the first idles for the second; points finish about once
     // in a hundred units)
     constexpr int kUnits = sizeof(Real) == 4 ? 2 : 1;
+    // EXACT: a sub-step that ends outside its cell parks the lane with that
+    // end (pend, qp) instead of resolving the exit at once: resolving takes
+    // about as long as a hundred units, and done alone it leaves the other 31
+    // lanes idle.  The warp resolves all parked lanes together once
+    // kCrossBatch of them wait, every active lane waits, or the oldest has
+    // waited kCrossWait votes.  Each point's arithmetic is unchanged.
+    constexpr int kCrossBatch = CPAB_EXACT_CROSS_BATCH, kCrossWait = CPAB_EXACT_CROSS_WAIT;
+    bool pend = false;
+    PState<DIM, Real> qp;
+    int pend_votes = 0;
     while (__any_sync(FULL, active)) {
         bool fin = false;
 #pragma unroll
         for (int u = 0; u < kUnits; ++u) {
-            if (active && !fin) {
+            if (active && !fin && !pend) {
                 const bool fast = (SCHEME == SCHEME_REF || SCHEME == SCHEME_EXACT) && sub_left == 0;
                 PState<DIM, Real> q;
                 if (SCHEME == SCHEME_EXACT)
@@ -639,8 +703,11 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
                 else
                     advance<DIM>(fast, st, sA + c * NE, sT + c * NE, nullptr, h, q);
                 int cq = cell_of<DIM, TESS>(t, q);
-                if (SCHEME == SCHEME_EXACT && !fast && cq != c)
-                    cq = exact_substep_cross<DIM, TESS, Real>(t, *ex, c, st, q);
+                if (SCHEME == SCHEME_EXACT && !fast && cq != c) {
+                    pend = true;
+                    qp = q;
+                    continue;
+                }
                 if (fast && cq != c) {
                     // the end point left the cell: redo the step with nStepsODE sub-steps from p
                     sub_left = nODE;
@@ -661,6 +728,28 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
                 if (fin) {
                     snk.put(idx, st);
                     ++c_pts;
+                }
+            }
+        }
+        if (SCHEME == SCHEME_EXACT) {
+            const unsigned pm = __ballot_sync(FULL, pend);
+            if (pm) {
+                const unsigned am = __ballot_sync(FULL, active);
+                if (__popc(pm) >= kCrossBatch || pm == am || ++pend_votes > kCrossWait) {
+                    pend_votes = 0;
+                    if (pend) {
+                        c = exact_substep_cross<DIM, TESS, Real>(t, *ex, c, st, qp);
+                        st = qp;
+                        pend = false;
+                        --sub_left;
+                        ++c_sub;
+                        if (sub_left == 0) --steps_left;
+                        fin = steps_left == 0;
+                        if (fin) {
+                            snk.put(idx, st);
+                            ++c_pts;
+                        }
+                    }
                 }
             }
         }
