@@ -228,13 +228,19 @@ size_t exact1d_smem_bytes(int nC, int tile_pts, int sort, int prec)
     return b;
 }
 
-// Resident CTAs of 256 threads the register allocation must allow per SM.
-// Measured on the batched 1D workload (88 M points, 4096 instances): 5 CTAs
-// (48 registers) 2.09 ms against 2.51 ms at the compiler's own choice; a
-// contiguous range of tiles per CTA (one table build per instance and CTA)
-// was slower than the strided order kept here (3.10 / 2.36 ms).
+// Resident CTAs of 256 threads the register allocation must allow per SM,
+// and the tiles a CTA takes in a row.  Measured on the batched 1D workload
+// (88 M points, 4096 instances), same box: 6 CTAs (40 registers) in groups
+// of 2 tiles 1.98 ms; 6 CTAs, single tiles 2.02 ms; 5 CTAs (48 registers)
+// 2.05 ms in groups of 2, 2.09 ms in groups of 4, 2.17 ms single; the
+// compiler's own register choice (96) 2.51 ms.  A contiguous range of tiles
+// per CTA (one table build per instance and CTA) was slower (3.10 ms):
+// instances differ in cost, and strided groups spread them over the CTAs.
 #ifndef CPAB_EXACT1D_MIN_BLOCKS
-#define CPAB_EXACT1D_MIN_BLOCKS 5
+#define CPAB_EXACT1D_MIN_BLOCKS 6
+#endif
+#ifndef CPAB_EXACT1D_TILE_GROUP
+#define CPAB_EXACT1D_TILE_GROUP 2
 #endif
 
 template <typename Real>
@@ -273,8 +279,15 @@ __global__ void __launch_bounds__(256, CPAB_EXACT1D_MIN_BLOCKS) k_exact1d(Integr
     e.step = 1.0 / (double)nC;
     // the reference gives up after nC crossings
     const int cap = nC;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        if ((((tile - blockIdx.x) / gridDim.x) & 7) == 0 && cta_cancelled(a.cancel, a.counters)) break;
+    // CTAs take groups of G consecutive tiles, strided over the grid (the
+    // tiles of a group mostly share an instance, so its tables are built once)
+    constexpr int G = CPAB_EXACT1D_TILE_GROUP;
+    for (int64_t it = 0;; ++it) {
+        const int64_t grp = (int64_t)blockIdx.x + (it / G) * gridDim.x;
+        const int64_t tile = grp * G + it % G;
+        if (grp * G >= ntiles) break;
+        if (tile >= ntiles) continue;
+        if ((it & 7) == 0 && cta_cancelled(a.cancel, a.counters)) break;
         if (threadIdx.x == 0) {
             s_tile = decode_tile(a.batch, tile);
             s_claim = 0;

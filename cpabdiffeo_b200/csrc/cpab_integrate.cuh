@@ -367,6 +367,10 @@ __device__ __forceinline__ int lookup_d(const Tess &t, const double *p, float)
 // exact_substep_cross keeps the reference scheme's sub-step end.
 constexpr int kExactDeg = 10;
 constexpr double kTaylorTol = 1e-17;
+// 1/k for the Taylor recurrences (a product instead of an FP64 division per term)
+static __constant__ double kInvInt[kExactDeg + 2] = {0.0,       1.0,       1.0 / 2,  1.0 / 3,
+                                                     1.0 / 4,   1.0 / 5,   1.0 / 6,  1.0 / 7,
+                                                     1.0 / 8,   1.0 / 9,   1.0 / 10, 1.0 / 11};
 
 template <int DIM>
 __device__ __forceinline__ void load_affine(const double *__restrict__ A, double *Ar, double &lnorm)
@@ -429,7 +433,7 @@ __device__ __forceinline__ bool flow_taylor(const double *__restrict__ A, const 
     for (int k = 2; k <= kExactDeg; ++k) {
         double nu[DIM];
         affine_lin<DIM>(Ar, u, nu);
-        coef *= t / k;
+        coef *= t * kInvInt[k];
         double wk = 0.0;
 #pragma unroll
         for (int r = 0; r < DIM; ++r) {
@@ -437,7 +441,7 @@ __device__ __forceinline__ bool flow_taylor(const double *__restrict__ A, const 
             x[r] = fma(coef, u[r], x[r]);
             wk = fmax(wk, fabs(coef * u[r]));
         }
-        const double rr = tl / (k + 1);
+        const double rr = tl * kInvInt[k + 1];
         if (rr < 0.5 && wk * rr <= kTaylorTol * (1.0 - rr) * first) {
             ok = true;
             break;
@@ -480,7 +484,7 @@ __device__ __forceinline__ double facet_hit_time(const double *__restrict__ A, c
 #pragma unroll
             for (int r = 0; r < DIM; ++r) u[r] = nu[r];
         }
-        inv_fact /= k;
+        inv_fact *= kInvInt[k];
         sk *= s;
         double d = 0.0, un = 0.0;
 #pragma unroll
@@ -492,7 +496,7 @@ __device__ __forceinline__ double facet_hit_time(const double *__restrict__ A, c
         if (k == 1) {
             scale = fabs(g0) + fabs(c[1]) * s;
         } else {
-            const double rr = sl / (k + 1);
+            const double rr = sl * kInvInt[k + 1];
             if (rr < 0.5 && f1 * un * inv_fact * sk * rr <= kTaylorTol * (1.0 - rr) * scale) {
                 K = k;
                 break;
@@ -522,7 +526,10 @@ __device__ __forceinline__ double facet_hit_time(const double *__restrict__ A, c
         if (g == 0) return t;
         double tn = t - g / dP;
         if (!(tn > lo && tn < hi)) tn = 0.5 * (lo + hi);
-        if (fabs(tn - t) <= 2e-16 * fabs(t) || hi - lo <= 2e-16 * hi) return tn;
+        // converged within about two ulps (4.5e-16 relative is at least two
+        // ulps in every binade: a tolerance under one ulp never ends an
+        // iteration that alternates between neighbouring doubles)
+        if (fabs(tn - t) <= 4.5e-16 * fabs(t) || hi - lo <= 4.5e-16 * hi) return tn;
         t = tn;
     }
     return 0.5 * (lo + hi);
@@ -681,15 +688,16 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
     // finishes after the first idles for the second; points finish about once
     // in a hundred units)
     constexpr int kUnits = sizeof(Real) == 4 ? 2 : 1;
-    // EXACT: a sub-step that ends outside its cell parks the lane with that
-    // end (pend, qp) instead of resolving the exit at once: resolving takes
-    // about as long as a hundred units, and done alone it leaves the other 31
-    // lanes idle.  The warp resolves all parked lanes together once
-    // kCrossBatch of them wait, every active lane waits, or the oldest has
-    // waited kCrossWait votes.  Each point's arithmetic is unchanged.
+    // EXACT: a sub-step that ends outside its cell parks the lane (pend)
+    // instead of resolving the exit at once: resolving takes about as long as
+    // a hundred units, and done alone it leaves the other 31 lanes idle.  The
+    // warp resolves all parked lanes together once kCrossBatch of them wait,
+    // every active lane waits, or the oldest has waited kCrossWait votes; a
+    // parked lane keeps only the sub-step's start and recomputes its end then
+    // (same arithmetic, fewer registers held).  Each point's arithmetic is
+    // unchanged.
     constexpr int kCrossBatch = CPAB_EXACT_CROSS_BATCH, kCrossWait = CPAB_EXACT_CROSS_WAIT;
     bool pend = false;
-    PState<DIM, Real> qp;
     int pend_votes = 0;
     while (__any_sync(FULL, active)) {
         bool fin = false;
@@ -705,7 +713,6 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
                 int cq = cell_of<DIM, TESS>(t, q);
                 if (SCHEME == SCHEME_EXACT && !fast && cq != c) {
                     pend = true;
-                    qp = q;
                     continue;
                 }
                 if (fast && cq != c) {
@@ -738,6 +745,9 @@ __device__ __forceinline__ void integrate_range(const Tess &t, int nT, int nODE,
                 if (__popc(pm) >= kCrossBatch || pm == am || ++pend_votes > kCrossWait) {
                     pend_votes = 0;
                     if (pend) {
+                        // the parked sub-step's end, recomputed with the same arithmetic
+                        PState<DIM, Real> qp;
+                        advance_exact<DIM>(false, st, sA + c * NE, sT + c * NE, qp);
                         c = exact_substep_cross<DIM, TESS, Real>(t, *ex, c, st, qp);
                         st = qp;
                         pend = false;

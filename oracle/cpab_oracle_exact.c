@@ -206,7 +206,8 @@ static double facet_root(int dim, const double *A, const double *F, const double
         const double dg = facet_dg(dim, F, A, y);
         double tn = t - g / dg;
         if (!(tn > lo && tn < hi)) tn = 0.5 * (lo + hi);
-        if (fabs(tn - t) <= 2e-16 * fmax(fabs(t), 1e-300) || hi - lo <= 2e-16 * hi) return tn;
+        /* within about two ulps (4.5e-16 is at least two ulps in every binade) */
+        if (fabs(tn - t) <= 4.5e-16 * fmax(fabs(t), 1e-300) || hi - lo <= 4.5e-16 * hi) return tn;
         t = tn;
     }
     return 0.5 * (lo + hi);
