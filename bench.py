@@ -63,13 +63,14 @@ def parse():
     ap.add_argument("--serve-sustained-seconds", type=float, default=10.0,
                     help="seconds of arrivals at 80%% of the measured serving capacity; 0 skips that run")
     ap.add_argument("--workload", default="batched_1d",
-                    choices=["batched_1d", "batched_2d_nc64", "exact_2d_nc64", "remap_ssd", "mcmc_c3"],
+                    choices=["batched_1d", "batched_2d_nc64", "exact_2d_nc64", "remap_ssd", "mcmc_c3", "serving"],
                     help="batched_1d: the headline (1D nC=100, 4096 theta, ragged); batched_2d_nc64: the reference "
                          "scheme in FP32 on 2D tess I 4x4 (nC=64), 4096 theta x 8192 points, for the "
                          "integration kernel's FP32 roofline; exact_2d_nc64: the same through the exact scheme "
                          "(facet hitting times); remap_ssd: remap + SSD of 256 pairs of 256x256 "
                          "images through FP32 maps, for its HBM roofline; mcmc_c3: 256-chain MCMC registration of "
-                         "256x256 FP32 image pairs, for the fused likelihood kernel's roofline")
+                         "256x256 FP32 image pairs, for the fused likelihood kernel's roofline; serving: only the "
+                         "serving legs (capacity, 200 req/s, sustained, 2000 req/s), one JSON line")
     return ap.parse_args()
 
 
@@ -225,11 +226,15 @@ def measured_peaks(torch) -> dict:
 
 # DRAM bytes per launch measured with ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum, one captured launch of the timed region):
-#  * k_exact1d on the 2048-theta case (42.7 M points): 300.4 MB, 7.03 B/point,
+#  * k_exact1d on the 2048-theta case (42.7 M points): 303.4 MB, 7.10 B/point,
 #    scaled to a launch by the points it processes;
 #  * k_integrate on the 2D 4096 x 8192-point workload: 587.9 MB per launch;
 #  * k_remap_ssd_bulk on 256 pairs of 256^2 images: 273.4 MB per launch.
-TRAFFIC_EXACT1D_BYTES_PER_POINT = 300.43e6 / 42737756
+TRAFFIC_EXACT1D_BYTES_PER_POINT = 303.38e6 / 42737756
+# Pipe utilisation of k_exact1d from the same capture (ncu, % of each pipe's
+# peak over the active cycles; FMA-heavy over the elapsed cycles).
+PIPES_EXACT1D = {"fp64_pct": 22.0, "fp32_fma_pct": 18.2, "fp32_fma_heavy_pct_elapsed": 30.5, "alu_pct": 31.5,
+                 "issue_active_pct": 73.1, "source": "ncu --set full, one launch of the 2048-theta case"}
 TRAFFIC_2D_BYTES_PER_LAUNCH = 587.94e6
 TRAFFIC_REMAP_BYTES_PER_LAUNCH = 273.43e6
 
@@ -772,16 +777,17 @@ def spawn_ranks(n: int) -> int:
 
 def serving_legs(args, dev) -> dict:
     """The serving mix: the capacity one GPU has for it (service times per
-    request type), the mix at 200 req/s, at 80 % of that capacity for
+    request type: the device-time bound, and the rate the server's job caps
+    sustain), the mix at 200 req/s, at 80 % of the lower capacity for
     --serve-sustained-seconds, and at the configuration's 2000 req/s for
     --serve-seconds (above capacity: the server keeps serving transforms while
     registrations queue)."""
     from cpabdiffeo_b200.serving_load import capacity_estimate, make_requests, run_load
     mix = ("1D/2D/3D, nC in {16,64,256,1024}, 1e3-4e6 pts, 10% 200-step registrations (side 64-1024)")
     out = {"serving_capacity": capacity_estimate(device=dev)}
-    reqs = make_requests(200.0, 2.0, seed=5)
-    out["serving_200hz"] = dict(run_load(reqs, device=dev), arrival_rate_hz=200.0, arrivals_s=2.0)
-    cap = out["serving_capacity"]["capacity_req_per_s"]
+    reqs = make_requests(200.0, 4.0, seed=5)
+    out["serving_200hz"] = dict(run_load(reqs, device=dev), arrival_rate_hz=200.0, arrivals_s=4.0)
+    cap = min(out["serving_capacity"]["capacity_req_per_s"], out["serving_capacity"]["capacity_with_job_caps"])
     if args.serve_sustained_seconds > 0:
         rate = 0.8 * cap
         reqs = make_requests(rate, args.serve_sustained_seconds, seed=6)
@@ -814,7 +820,8 @@ def main():
     dev = torch.device("cuda", local)
     if args.workload != "batched_1d":
         line = {"batched_2d_nc64": bench_2d, "remap_ssd": bench_remap, "mcmc_c3": bench_mcmc_c3,
-                "exact_2d_nc64": lambda a, t, d: bench_2d(a, t, d, exact=True)}[args.workload](args, torch, dev)
+                "exact_2d_nc64": lambda a, t, d: bench_2d(a, t, d, exact=True),
+                "serving": lambda a, t, d: serving_legs(a, d)}[args.workload](args, torch, dev)
         if rank == 0:
             print(json.dumps(line), flush=True)
         return
@@ -1039,6 +1046,7 @@ def main():
                             "kernel_ms": kern_ms, "step_ms_events": step_ms,
                             "traffic": TRAFFIC_EXACT1D_BYTES_PER_POINT * n_total,
                             "traffic_note": "ncu DRAM bytes of one launch on the 2048-theta case, scaled by points",
+                            "pipes_ncu": PIPES_EXACT1D,
                             "algorithmic_flop_per_launch": flops,
                             "hbm_achieved_gbs": 2 * pts_h.nbytes / (kern_ms * 1e-3) / 1e9,
                             "hbm_peak_gbs": peaks.get("hbm_gbs")}

@@ -55,7 +55,11 @@ class BatchedMetropolis:
         else:
             if prop_std is None:
                 raise ValueError("prop_std is needed for the random-walk proposal")
-            self.prop_std = torch.as_tensor(np.asarray(prop_std, dtype=np.float64), device=dev).contiguous()
+            if isinstance(prop_std, torch.Tensor) and prop_std.is_cuda:
+                # already resident (a server shares one per space): no host copy, no stream sync
+                self.prop_std = prop_std.to(device=dev, dtype=torch.float64).contiguous()
+            else:
+                self.prop_std = torch.as_tensor(np.asarray(prop_std, dtype=np.float64), device=dev).contiguous()
         self.scale = float(scale)
         self.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
         self.rule = {"reference": 0, "standard": 1}[rule]

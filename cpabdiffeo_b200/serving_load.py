@@ -59,45 +59,77 @@ def make_requests(rate_hz: float, duration_s: float, seed: int = 4, max_points: 
     return out
 
 
+WARM_BURST = 4
+
+
 def warm_up(srv: CpabServer, requests) -> int:
     """Serve, untimed, one small request of every transform shape in `requests`,
-    the largest transform payload in full, and one short registration job
-    (long enough to capture its CUDA graph), then forget them: the spaces,
-    the kernels of every variant (loaded on first launch), the pinned host
-    buffer pool and the graph path are ready before the timed arrivals.
-    Returns the number of warm-up requests."""
+    a burst of WARM_BURST copies of the largest transform payload, and
+    max_jobs short registration jobs on the largest image pair (long enough
+    to capture their CUDA graphs), then forget them, after
+    CpabServer.reserve for the largest point dimension and image side of
+    `requests`: the spaces, the kernels of every variant (loaded on first
+    launch), the device and pinned host buffers and the graph path are ready
+    before the timed arrivals.  Returns the number of warm-up requests."""
     seen, warm = set(), []
     big = max((r for _, r in requests if isinstance(r, TransformRequest)),
               key=lambda r: np.asarray(r.pts).shape[0], default=None)
     if big is not None:
-        warm.append(TransformRequest(big.dim, big.nCs, big.theta, big.pts, tess=big.tess, scheme=big.scheme))
+        warm.extend(TransformRequest(big.dim, big.nCs, big.theta, big.pts, tess=big.tess, scheme=big.scheme)
+                    for _ in range(WARM_BURST))
     for _, r in requests:
         if isinstance(r, TransformRequest):
             key = (r.dim, tuple(r.nCs), r.tess, r.scheme)
             if key not in seen:
                 seen.add(key)
                 warm.append(TransformRequest(r.dim, r.nCs, r.theta, r.pts[:1024], tess=r.tess, scheme=r.scheme))
-        elif "registration" not in seen:
-            seen.add("registration")
-            warm.append(RegistrationRequest(r.src[:64, :64].copy(), r.dst[:64, :64].copy(),
-                                            n_steps=2 * srv.mcmc_slice, seed=1, nCs=r.nCs, tess=r.tess))
+    regs = [r for _, r in requests if isinstance(r, RegistrationRequest)]
+    if regs:
+        # one job per job stream, on the largest image pair: every stream's
+        # allocations and graph capture happen here
+        big_reg = max(regs, key=lambda r: np.size(r.src))
+        warm.extend(RegistrationRequest(big_reg.src, big_reg.dst, n_steps=2 * srv.mcmc_slice, seed=1 + j,
+                                        nCs=big_reg.nCs, tess=big_reg.tess) for j in range(srv.max_jobs))
+    sides = [int(max(np.shape(r.src))) for r in regs]
+    trs = [r for _, r in requests if isinstance(r, TransformRequest)]
+    srv.reserve(dims=max((r.dim for r in trs), default=1), image_side=max(sides, default=0),
+                largest_request_values=max((np.asarray(r.pts).size for r in trs), default=0))
     for q in warm:
         srv.submit(q)
     srv.run_until_idle()
+    srv.spread_lane_buffers()
     torch.cuda.synchronize()
     srv.done.clear()
+    srv.host_seconds = dict.fromkeys(srv.host_seconds, 0.0)
+    srv.host_max_seconds = dict.fromkeys(srv.host_max_seconds, 0.0)
     return len(warm)
 
 
-def run_load(requests, device=None, time_limit_s: float = 120.0, grace_s: float | None = None) -> dict:
+def run_load(requests, device=None, time_limit_s: float = 120.0, grace_s: float | None = None,
+             server_kwargs: dict | None = None) -> dict:
     """Replay `requests` in real time.  With grace_s None the server drains
     (every request is served); otherwise the run stops grace_s after the
     last arrival and reports what was served by then (an overloaded server
-    never drains), with the requests still queued or running."""
-    srv = CpabServer(device=device)
+    never drains), with the requests still queued or running.
+    server_kwargs: CpabServer's scheduling parameters (max_jobs, ...)."""
+    srv = CpabServer(device=device, **(server_kwargs or {}))
     # spaces, kernels and graph capture warmed by one small request of each shape (not timed)
     n_warm = warm_up(srv, requests)
     gc.collect()                                   # garbage of earlier work is not collected inside the window
+    # the request stream and the warmed server move out of the cyclic
+    # collector's reach (as a latency-sensitive Python server freezes its
+    # start-up heap), so a collection inside the window scans only what the
+    # window creates; the pauses it still takes are recorded
+    gc.freeze()
+    pauses = []
+    t_gc = [0.0]
+
+    def on_gc(phase, info):
+        if phase == "start":
+            t_gc[0] = time.perf_counter()
+        else:
+            pauses.append(time.perf_counter() - t_gc[0])
+    gc.callbacks.append(on_gc)
     t0 = time.perf_counter()
     i = 0
     while i < len(requests) or not srv.idle():
@@ -111,10 +143,16 @@ def run_load(requests, device=None, time_limit_s: float = 120.0, grace_s: float 
         if grace_s is not None and i == len(requests) and now > (requests[-1][0] if requests else 0.0) + grace_s:
             break
     wall = time.perf_counter() - t0
+    gc.callbacks.remove(on_gc)
+    gc.unfreeze()
+    # work still queued or running (an overloaded window) finishes before the
+    # server and its device buffers are dropped
+    torch.cuda.synchronize(srv.device)
     lat = np.asarray([r.t_done - r.t_submit for r in srv.done.values()])
     pts = sum(int(np.asarray(r.req.pts).shape[0]) for r in srv.done.values() if isinstance(r.req, TransformRequest))
     n_reg = sum(1 for r in srv.done.values() if isinstance(r.req, RegistrationRequest))
     lat_t = np.asarray([r.t_done - r.t_submit for r in srv.done.values() if isinstance(r.req, TransformRequest)])
+    srv.close()
     return {
         "requests_submitted": len(requests), "requests_done": len(srv.done), "registrations_done": n_reg,
         "wall_s": wall, "req_per_s": len(srv.done) / wall, "points_per_s": pts / wall,
@@ -125,29 +163,40 @@ def run_load(requests, device=None, time_limit_s: float = 120.0, grace_s: float 
         "warm_up_requests": n_warm,
         "left_unserved": len(requests) - len(srv.done),
         "left_registrations": sum(1 for _, q in requests if isinstance(q, RegistrationRequest)) - n_reg,
+        "host_seconds": {k: round(v, 3) for k, v in srv.host_seconds.items()},
+        "host_max_call_ms": {k: round(v * 1e3, 2) for k, v in srv.host_max_seconds.items()},
+        "gc_pauses": len(pauses), "gc_max_ms": round(max(pauses, default=0.0) * 1e3, 2),
     }
 
 
-def capacity_estimate(device=None, reg_sides=(128, 512, 1024), reg_steps: int = 40) -> dict:
+def capacity_estimate(device=None, reg_sides=(128, 512, 1024), reg_steps: int = 40,
+                      server_kwargs: dict | None = None) -> dict:
     """Requests per second one GPU can serve of the mix, from measured service
     times of each request type served alone (host work, copies and kernels,
-    one request at a time -- concurrent service overlaps host and device work,
-    so the server can do somewhat better).
+    one request at a time).
 
     Transforms: for each (dim, grid) of the mix, the service time of 1e3 and
     1e6 points gives t(n) = o + n / r; the mix's payload is log-uniform in
     [1e3, 4e6] (mean (4e6 - 1e3) / ln 4000).  Registrations: the per-step time
     at a few image sides gives t(side) = a + b side^2; sides are uniform in
-    [64, 1024] and each job takes 200 steps.  Capacity = 1 / (0.9 E[t_transform]
-    + 0.1 E[t_registration])."""
-    srv = CpabServer(device=device)
+    [64, 1024] and each job takes 200 steps -- once with the whole GPU and
+    once capped as the server runs them (job_sm_fraction of the SMs).
+      capacity_req_per_s = 1 / (0.9 E[t_transform] + 0.1 E[t_registration, whole GPU]):
+        the device-time bound of the mix, one request at a time;
+      capacity_with_job_caps = min(max_jobs / (0.1 E[t_registration, capped]),
+                                   (1 - u) / (0.9 E[t_transform])), u = max_jobs * job_sm_fraction:
+        the rate the server's scheduling sustains (max_jobs capped jobs at
+        once, transforms on the SMs the jobs leave)."""
+    kw = dict(server_kwargs or {})
+    srv = CpabServer(device=device, **kw)
+    whole = CpabServer(device=device, **dict(kw, job_sm_fraction=1.0))
     rng = np.random.default_rng(11)
 
-    def serve(req) -> float:
+    def serve(server, req) -> float:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        srv.submit(req)
-        srv.run_until_idle()
+        server.submit(req)
+        server.run_until_idle()
         torch.cuda.synchronize()
         return time.perf_counter() - t0
 
@@ -159,28 +208,41 @@ def capacity_estimate(device=None, reg_sides=(128, 512, 1024), reg_steps: int = 
             theta = prior.sample(1, rng)[0]
             small = rng.uniform(0, 1, (1000, dim)).astype(np.float32)
             big = rng.uniform(0, 1, (1_000_000, dim)).astype(np.float32)
-            serve(TransformRequest(dim, nCs, theta, small, tess=tess))          # warm the space and kernels
-            ts = min(serve(TransformRequest(dim, nCs, theta, small, tess=tess)) for _ in range(3))
-            tb = min(serve(TransformRequest(dim, nCs, theta, big, tess=tess)) for _ in range(2))
+            serve(srv, TransformRequest(dim, nCs, theta, small, tess=tess))     # warm the space and kernels
+            ts = min(serve(srv, TransformRequest(dim, nCs, theta, small, tess=tess)) for _ in range(3))
+            tb = min(serve(srv, TransformRequest(dim, nCs, theta, big, tess=tess)) for _ in range(2))
             r = (1_000_000 - 1000) / max(tb - ts, 1e-9)
             o = max(ts - 1000 / r, 0.0)
             per_cfg[f"{dim}d_{'x'.join(map(str, nCs))}_{tess}"] = {"overhead_ms": o * 1e3, "points_per_s": r,
                                                                  "mean_ms": (o + mean_n / r) * 1e3}
     t_tr = float(np.mean([v["mean_ms"] for v in per_cfg.values()])) * 1e-3
-    per_step = {}
-    for side in reg_sides:
-        src = gaussian_filter(rng.uniform(0, 1, (side, side)).astype(np.float32), 8.0)
-        dst = np.roll(src, 2, axis=1)
-        serve(RegistrationRequest(src, dst, n_steps=2 * srv.mcmc_slice, seed=1))  # warm (graph capture)
-        t = serve(RegistrationRequest(src, dst, n_steps=reg_steps, seed=2))
-        per_step[side] = t / reg_steps
-    sides = np.array(sorted(per_step))
-    b, a = np.polyfit(sides.astype(float) ** 2, [per_step[s] for s in sides], 1)
     e_side2 = (1024 ** 3 - 63 ** 3) / (3 * (1024 - 63))       # E[side^2], side uniform on 64..1024
-    t_reg = 200 * (a + b * e_side2)
+
+    def registration(server):
+        per_step = {}
+        for side in reg_sides:
+            src = gaussian_filter(rng.uniform(0, 1, (side, side)).astype(np.float32), 8.0)
+            dst = np.roll(src, 2, axis=1)
+            serve(server, RegistrationRequest(src, dst, n_steps=2 * server.mcmc_slice, seed=1))  # warm (graph)
+            per_step[side] = serve(server, RegistrationRequest(src, dst, n_steps=reg_steps, seed=2)) / reg_steps
+        sides = np.array(sorted(per_step))
+        b, a = np.polyfit(sides.astype(float) ** 2, [per_step[s] for s in sides], 1)
+        return 200 * (a + b * e_side2), {int(s): v * 1e3 for s, v in per_step.items()}
+
+    t_reg, steps_whole = registration(whole)
+    t_reg_cap, steps_cap = registration(srv)
+    srv.close()
+    whole.close()
     mean_t = 0.9 * t_tr + 0.1 * t_reg
+    sms = torch.cuda.get_device_properties(srv.device).multi_processor_count
+    u = min(1.0, srv.max_jobs * srv.job_max_ctas / sms)
+    r_reg = srv.max_jobs / (0.1 * t_reg_cap)
+    r_tr = (1.0 - u) / (0.9 * t_tr) if u < 1.0 else float("inf")
     return {"transform_mean_ms": t_tr * 1e3, "registration_mean_ms": t_reg * 1e3,
-            "registration_step_ms": {int(s): v * 1e3 for s, v in per_step.items()},
+            "registration_mean_ms_capped": t_reg_cap * 1e3,
+            "registration_step_ms": steps_whole, "registration_step_ms_capped": steps_cap,
             "mean_service_ms": mean_t * 1e3, "capacity_req_per_s": 1.0 / mean_t,
+            "capacity_with_job_caps": min(r_reg, r_tr),
+            "job_caps": {"max_jobs": srv.max_jobs, "ctas_per_job": srv.job_max_ctas, "sm_share_of_jobs": u},
             "device_seconds_per_second_at_2000_req_per_s": 2000 * mean_t,
             "transforms": per_cfg}

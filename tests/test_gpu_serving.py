@@ -2,6 +2,8 @@
 mix (bit-exact: the kernels are per point / per image with fixed reduction
 order and per-job random streams), requests submitted while others run are
 admitted, and a tight memory budget still drains the queue."""
+import inspect
+
 import numpy as np
 import pytest
 import torch
@@ -46,10 +48,15 @@ def _same(a, b):
     return np.array_equal(a, b)
 
 
-def test_alone_equals_in_mix():
+@pytest.mark.parametrize("reserved", [False, True])
+def test_alone_equals_in_mix(reserved):
+    """reserved: the server's stream buffers, pinned pool and job image slots
+    are allocated up front (CpabServer.reserve) and reused across requests."""
     rng = np.random.default_rng(0)
     reqs = _mix(rng)
     srv = CpabServer(device=DEV)
+    if reserved:
+        srv.reserve(dims=3, image_side=40)
     first, late = reqs[:8], reqs[8:]
     ids = [srv.submit(r) for r in first]
     srv.step()                                  # work is on the GPU ...
@@ -100,10 +107,37 @@ def test_memory_budget_admission_drains():
 def test_load_runner_warms_every_shape_then_serves_all():
     """run_load serves one small request per shape untimed, forgets it, then
     replays the seeded arrivals; every timed request completes."""
-    from cpabdiffeo_b200.serving_load import make_requests, run_load
+    from cpabdiffeo_b200.serving_load import WARM_BURST, make_requests, run_load
     reqs = make_requests(40.0, 0.3, seed=8, max_points=2e4, reg_steps=12, max_side=96)
     r = run_load(reqs, device=torch.device(DEV), time_limit_s=60.0)
     shapes = {(q.dim, tuple(q.nCs), q.tess) for _, q in reqs if isinstance(q, TransformRequest)}
     has_reg = any(isinstance(q, RegistrationRequest) for _, q in reqs)
-    assert r["warm_up_requests"] == len(shapes) + int(has_reg) + 1  # + the largest payload once
+    max_jobs = inspect.signature(CpabServer.__init__).parameters["max_jobs"].default
+    assert r["warm_up_requests"] == len(shapes) + max_jobs * int(has_reg) + WARM_BURST
     assert r["requests_done"] == r["requests_submitted"] == len(reqs)
+
+
+def test_inflight_point_bound_admits_in_order_and_drains():
+    """Transforms are admitted in arrival order while at most
+    max_inflight_points are in flight; a registration queued behind held-back
+    transforms still starts; everything drains and the count returns to 0."""
+    rng = np.random.default_rng(3)
+    geo = build_space(1, (100,), "II")
+    theta = Prior.create(geo, 0.1, 1.0).sample(12, rng)
+    srv = CpabServer(device=DEV, max_inflight_points=20_000)
+    ids = [srv.submit(TransformRequest(1, (100,), theta[i], rng.uniform(0, 1, (8000, 1)).astype(np.float32)))
+           for i in range(12)]
+    src = gaussian_filter(rng.uniform(0, 1, (32, 32)).astype(np.float32), 3.0)
+    jid = srv.submit(RegistrationRequest(src, np.roll(src, 1, axis=1), n_steps=4, seed=5))
+    srv.step()
+    assert srv.tr_points == 16_000 and len(srv.waiting) == 10      # two transforms fit, ten wait
+    assert all(r.rid != jid for r in srv.waiting)                  # the job was not held back
+    peak = 0
+    while not srv.idle():
+        srv.step()
+        peak = max(peak, srv.tr_points)
+    assert len(srv.done) == 13 and srv.tr_points == 0 and srv.in_use == 0
+    assert peak <= 20_000
+    t_admit = [srv.done[i].t_admit for i in ids]
+    assert all(a <= b for a, b in zip(t_admit, t_admit[1:]))
+    assert set(srv.host_seconds) == {"retire", "admit", "launch", "jobs"}
