@@ -445,8 +445,15 @@ struct SlotSnk2 {
     }
 };
 
+// CPAB_REGISTER_MIN_BLOCKS: resident CTAs of 256 threads the register
+// allocation must allow per SM (unset: the compiler's own choice).
+#ifdef CPAB_REGISTER_MIN_BLOCKS
+#define CPAB_REGISTER_BOUNDS __launch_bounds__(256, CPAB_REGISTER_MIN_BLOCKS)
+#else
+#define CPAB_REGISTER_BOUNDS __launch_bounds__(256)
+#endif
 template <int TESS, typename Real>
-__global__ void __launch_bounds__(256) k_register_ll(RegisterArgs a)
+__global__ void CPAB_REGISTER_BOUNDS k_register_ll(RegisterArgs a)
 {
     constexpr int DIM = 2, NE = 6;
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -168,6 +168,7 @@ class CpabServer:
         self._spaces: dict = {}
         self._priors: dict = {}
         self.max_jobs = int(max_jobs)
+        self._finishing = 0                # jobs whose last slice is enqueued, not yet retired
         sms = torch.cuda.get_device_properties(self.device).multi_processor_count
         self.job_max_ctas = max(1, int(sms * job_sm_fraction))
         self.max_inflight_points = int(max_inflight_points)
@@ -372,7 +373,9 @@ class CpabServer:
         being admitted (in order) once max_inflight_points are in flight,
         without holding back the registrations behind them."""
         kept: deque[_Record] = deque()
-        jobs = len(self.jobs)
+        # finishing jobs (last slice enqueued, not retired) still hold their
+        # image slot and pinned buffers, so they count
+        jobs = len(self.jobs) + self._finishing
         tr_full = False
         started = False                    # one job start per iteration: the loop turns between starts
         while self.waiting:
@@ -589,6 +592,7 @@ class CpabServer:
                 self._note("job_slice", t_sl)
                 job["left"] -= k
                 if job["left"] == 0:
+                    self._finishing += 1
                     mh = job["mh"]
                     d = mh.theta.numel()
                     th_h = self._pinned_buf(d, torch.float64)
@@ -605,6 +609,7 @@ class CpabServer:
                         rec.result = dict(theta=th_h[:d].numpy().copy(), ll=float(ll_h[0]),
                                           accepted=int(acc_h[0]))
                         self._release_pinned(th_h, ll_h, acc_h, *pins)
+                        self._finishing -= 1
                         if slot is not None:
                             self._job_slots.append(slot)
                     self.inflight.append((ev, [job["rec"]], finalize))
