@@ -251,33 +251,46 @@ __global__ void __launch_bounds__(256, 4) k_remap_ssd_bulk(RemapArgs a)
     }
     __syncthreads();
     int issued0 = 0, issued1 = 0;  // copies thread 0 issued per stage (one phase each)
-    auto issue = [&](int64_t tile, int stage) {
+    // (image, tile within the image) of the current tile, advanced by the
+    // grid stride with one add and one compare instead of a 64-bit division
+    // per tile: stride = qG images + rG tiles
+    const int64_t qG = (int64_t)gridDim.x / tpi, rG = (int64_t)gridDim.x - qG * tpi;
+    auto advance = [&](int64_t &inst, int64_t &tin) {
+        tin += rG;
+        inst += qG;
+        if (tin >= tpi) {
+            tin -= tpi;
+            ++inst;
+        }
+    };
+    auto issue = [&](int64_t inst, int64_t tin, int stage) {
         if (stage) ++issued1; else ++issued0;
-        const int inst = (int)(tile / tpi);
-        const int64_t start = (tile - (int64_t)inst * tpi) * TP;
+        const int64_t start = tin * TP;
         const int n = (int)min((int64_t)TP, npx - start);
-        const int64_t off = (int64_t)inst * npx + start;
+        const int64_t off = inst * npx + start;
         const uint32_t mb = (uint32_t)n * 2u * (uint32_t)sizeof(MapT), db = a.dst ? (uint32_t)n * 4u : 0u;
         mbar_arrive_expect_tx(&s_bar[stage], mb + db);
         bulk_g2s(s_map0 + stage * 2 * TP, gmap + 2 * off, mb, &s_bar[stage]);
         if (db) bulk_g2s(s_dst0 + stage * TP, a.dst + off, db, &s_bar[stage]);
     };
-    if (threadIdx.x == 0 && (int64_t)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    int64_t inst = (int64_t)blockIdx.x / tpi, tin = (int64_t)blockIdx.x - inst * tpi;
+    if (threadIdx.x == 0 && (int64_t)blockIdx.x < ntiles) issue(inst, tin, 0);
     int it = 0;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
         const int stage = it & 1;
         const uint32_t parity = (uint32_t)(it >> 1) & 1u;
+        int64_t inst_n = inst, tin_n = tin;
+        advance(inst_n, tin_n);
         // s_dead was last written before the previous tile's closing barrier
         const bool dead = s_dead != 0;
         // the other stage was released by the previous iteration's closing barrier
-        if (threadIdx.x == 0 && !dead && tile + gridDim.x < ntiles) issue(tile + gridDim.x, stage ^ 1);
+        if (threadIdx.x == 0 && !dead && tile + gridDim.x < ntiles) issue(inst_n, tin_n, stage ^ 1);
         const bool ok = !dead && mbar_wait(&s_bar[stage], parity);
         if (!ok && !dead) s_dead = 1;
-        const int inst = (int)(tile / tpi);
-        const int64_t start = (tile - (int64_t)inst * tpi) * TP;
+        const int64_t start = tin * TP;
         const int n = (int)min((int64_t)TP, npx - start);
-        const int64_t off = (int64_t)inst * npx + start;
-        const float *src = a.src + (int64_t)inst * npx;
+        const int64_t off = inst * npx + start;
+        const float *src = a.src + inst * npx;
         float *warped = a.warped ? a.warped + off : nullptr;
         double acc = 0.0;
         if (ok && FCOORD) {
@@ -333,6 +346,8 @@ __global__ void __launch_bounds__(256, 4) k_remap_ssd_bulk(RemapArgs a)
             store_tile_partial(acc, it & 1, tile, a.partials);
         else
             __syncthreads();
+        inst = inst_n;
+        tin = tin_n;
     }
     // Without a give-up every copy this CTA issued was waited for above (the
     // last issue targets its last tile).  After one, wait (bounded) for the
