@@ -229,14 +229,14 @@ def measured_peaks(torch) -> dict:
 #  * k_exact1d on the 2048-theta case (42.7 M points): 303.4 MB, 7.10 B/point,
 #    scaled to a launch by the points it processes;
 #  * k_integrate on the 2D 4096 x 8192-point workload: 587.9 MB per launch;
-#  * k_remap_ssd_bulk on 256 pairs of 256^2 images: 273.4 MB per launch.
+#  * k_remap_ssd_bulk on 256 pairs of 256^2 images: 273.0 MB per launch.
 TRAFFIC_EXACT1D_BYTES_PER_POINT = 303.38e6 / 42737756
 # Pipe utilisation of k_exact1d from the same capture (ncu, % of each pipe's
 # peak over the active cycles; FMA-heavy over the elapsed cycles).
 PIPES_EXACT1D = {"fp64_pct": 22.0, "fp32_fma_pct": 18.2, "fp32_fma_heavy_pct_elapsed": 30.5, "alu_pct": 31.5,
                  "issue_active_pct": 73.1, "source": "ncu --set full, one launch of the 2048-theta case"}
 TRAFFIC_2D_BYTES_PER_LAUNCH = 587.94e6
-TRAFFIC_REMAP_BYTES_PER_LAUNCH = 273.43e6
+TRAFFIC_REMAP_BYTES_PER_LAUNCH = 272.95e6
 
 # Closed-form segment cost model (FP64 operations): per cell visit the
 # crossing test and hitting time take 10 arithmetic operations plus one log,
