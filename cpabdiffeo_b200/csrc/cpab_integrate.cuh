@@ -358,7 +358,8 @@ __device__ __forceinline__ int lookup_d(const Tess &t, const double *p, float)
 
 // The flow inside a cell over a time t <= h (one sub-step) as a Taylor
 // polynomial: x(t) = p + sum_{k>=1} w_k, w_k = t^k/k! u_k, u_1 = L p + b,
-// u_k = L u_{k-1} (A = [L | b], loaded into registers once per call).  The
+// u_k = L u_{k-1} (A = [L | b], read through the read-only cache at each use:
+// held in registers it raised the kernel's spills, 37.3 against 36.1 ms).  The
 // series stops at the first degree K whose omitted terms are provably below
 // FP64 rounding of the first: with r = t |L| / (K+1) < 1 (|L| the max row
 // sum), |w_{K+j}| <= |w_K| r^j, so the rest sums to at most |w_K| r/(1-r).
@@ -373,41 +374,39 @@ static __constant__ double kInvInt[kExactDeg + 2] = {0.0,       1.0,       1.0 /
                                                      1.0 / 8,   1.0 / 9,   1.0 / 10, 1.0 / 11};
 
 template <int DIM>
-__device__ __forceinline__ void load_affine(const double *__restrict__ A, double *Ar, double &lnorm)
+__device__ __forceinline__ double affine_norm(const double *__restrict__ A)
 {
-    lnorm = 0.0;
+    double lnorm = 0.0;
 #pragma unroll
     for (int r = 0; r < DIM; ++r) {
         double rs = 0.0;
 #pragma unroll
-        for (int m = 0; m <= DIM; ++m) {
-            Ar[r * (DIM + 1) + m] = __ldg(A + r * (DIM + 1) + m);
-            if (m < DIM) rs += fabs(Ar[r * (DIM + 1) + m]);
-        }
+        for (int m = 0; m < DIM; ++m) rs += fabs(__ldg(A + r * (DIM + 1) + m));
         lnorm = fmax(lnorm, rs);
     }
+    return lnorm;
 }
 
 template <int DIM>
-__device__ __forceinline__ void affine_lin(const double *Ar, const double *u, double *out)
+__device__ __forceinline__ void affine_lin(const double *__restrict__ A, const double *u, double *out)
 {
 #pragma unroll
     for (int r = 0; r < DIM; ++r) {
         double v = 0.0;
 #pragma unroll
-        for (int m = 0; m < DIM; ++m) v = fma(Ar[r * (DIM + 1) + m], u[m], v);
+        for (int m = 0; m < DIM; ++m) v = fma(__ldg(A + r * (DIM + 1) + m), u[m], v);
         out[r] = v;
     }
 }
 
 template <int DIM>
-__device__ __forceinline__ void velocity(const double *Ar, const double *p, double *v)
+__device__ __forceinline__ void velocity(const double *__restrict__ A, const double *p, double *v)
 {
 #pragma unroll
     for (int r = 0; r < DIM; ++r) {
-        double s = Ar[r * (DIM + 1) + DIM];
+        double s = __ldg(A + r * (DIM + 1) + DIM);
 #pragma unroll
-        for (int m = 0; m < DIM; ++m) s = fma(Ar[r * (DIM + 1) + m], p[m], s);
+        for (int m = 0; m < DIM; ++m) s = fma(__ldg(A + r * (DIM + 1) + m), p[m], s);
         v[r] = s;
     }
 }
@@ -417,8 +416,8 @@ __device__ __forceinline__ void velocity(const double *Ar, const double *p, doub
 template <int DIM>
 __device__ __forceinline__ bool flow_taylor(const double *__restrict__ A, const double *p, double t, double *out)
 {
-    double Ar[DIM * (DIM + 1)], lnorm;
-    load_affine<DIM>(A, Ar, lnorm);
+    const double *Ar = A;  // global, read through __ldg
+    const double lnorm = affine_norm<DIM>(A);
     double u[DIM], x[DIM];
     velocity<DIM>(Ar, p, u);
     double coef = t, first = 0.0;
@@ -462,8 +461,8 @@ template <int DIM>
 __device__ __forceinline__ double facet_hit_time(const double *__restrict__ A, const double *__restrict__ F,
                                                  const double *p, double s, double g0)
 {
-    double Ar[DIM * (DIM + 1)], lnorm;
-    load_affine<DIM>(A, Ar, lnorm);
+    const double *Ar = A;  // global, read through __ldg
+    const double lnorm = affine_norm<DIM>(A);
     double c[kExactDeg + 1];
     c[0] = g0;
     double u[DIM], Fn[DIM], f1 = 0.0;
