@@ -179,8 +179,11 @@ def capacity_estimate(device=None, reg_sides=(128, 512, 1024), reg_steps: int = 
     1e6 points gives t(n) = o + n / r; the mix's payload is log-uniform in
     [1e3, 4e6] (mean (4e6 - 1e3) / ln 4000).  Registrations: the per-step time
     at a few image sides gives t(side) = a + b side^2; sides are uniform in
-    [64, 1024] and each job takes 200 steps -- once with the whole GPU and
-    once capped as the server runs them (job_sm_fraction of the SMs).
+    [64, 1024] and each job takes 200 steps plus its start (the per-step time
+    is the difference of a 3 x reg_steps and a reg_steps job, so the start --
+    staging, first eager slice, graph capture -- is measured apart) -- once
+    with the whole GPU and once capped as the server runs them
+    (job_sm_fraction of the SMs).
       capacity_req_per_s = 1 / (0.9 E[t_transform] + 0.1 E[t_registration, whole GPU]):
         the device-time bound of the mix, one request at a time;
       capacity_with_job_caps = min(max_jobs / (0.1 E[t_registration, capped]),
@@ -224,18 +227,25 @@ def capacity_estimate(device=None, reg_sides=(128, 512, 1024), reg_steps: int = 
     e_side2 = (1024 ** 3 - 63 ** 3) / (3 * (1024 - 63))       # E[side^2], side uniform on 64..1024
 
     def registration(server):
-        per_step = {}
+        # per-step time from two job lengths (the difference cancels the job's
+        # start: staging, first eager slice, graph capture), plus that start
+        per_step, start = {}, {}
         for side in reg_sides:
             src = gaussian_filter(rng.uniform(0, 1, (side, side)).astype(np.float32), 8.0)
             dst = np.roll(src, 2, axis=1)
             serve(server, RegistrationRequest(src, dst, n_steps=2 * server.mcmc_slice, seed=1))  # warm (graph)
-            per_step[side] = serve(server, RegistrationRequest(src, dst, n_steps=reg_steps, seed=2)) / reg_steps
+            t_short = serve(server, RegistrationRequest(src, dst, n_steps=reg_steps, seed=2))
+            t_long = serve(server, RegistrationRequest(src, dst, n_steps=3 * reg_steps, seed=3))
+            per_step[side] = max(t_long - t_short, 0.0) / (2 * reg_steps)
+            start[side] = max(t_short - reg_steps * per_step[side], 0.0)
         sides = np.array(sorted(per_step))
         b, a = np.polyfit(sides.astype(float) ** 2, [per_step[s] for s in sides], 1)
-        return 200 * (a + b * e_side2), {int(s): v * 1e3 for s, v in per_step.items()}
+        t_start = float(np.mean(list(start.values())))
+        return (t_start + 200 * (a + b * e_side2), {int(s): v * 1e3 for s, v in per_step.items()},
+                t_start * 1e3)
 
-    t_reg, steps_whole = registration(whole)
-    t_reg_cap, steps_cap = registration(srv)
+    t_reg, steps_whole, start_whole = registration(whole)
+    t_reg_cap, steps_cap, start_cap = registration(srv)
     srv.close()
     whole.close()
     mean_t = 0.9 * t_tr + 0.1 * t_reg
@@ -246,6 +256,7 @@ def capacity_estimate(device=None, reg_sides=(128, 512, 1024), reg_steps: int = 
     return {"transform_mean_ms": t_tr * 1e3, "registration_mean_ms": t_reg * 1e3,
             "registration_mean_ms_capped": t_reg_cap * 1e3,
             "registration_step_ms": steps_whole, "registration_step_ms_capped": steps_cap,
+            "registration_start_ms": start_whole, "registration_start_ms_capped": start_cap,
             "mean_service_ms": mean_t * 1e3, "capacity_req_per_s": 1.0 / mean_t,
             "capacity_with_job_caps": min(r_reg, r_tr),
             "job_caps": {"max_jobs": srv.max_jobs, "ctas_per_job": srv.job_max_ctas, "sm_share_of_jobs": u},
