@@ -380,11 +380,70 @@ __global__ void k_expm(const double *A, double *signedA, double *T, int64_t n_ce
     }
 }
 
-// A = B.theta (theta row-major [N, d], B row-major [D_A, d]) fused with the
-// per-cell expm: one thread per (instance, cell).  A is optional output.
+// Per (instance, cell) after A: the sign, dt, the expm and the stores.
 template <int DIM>
-__global__ void k_theta_to_trels(const double *B, const double *theta, int d, int nC, int N,
-                                 double dt, double sign, double *A, double *signedA, double *T)
+__device__ __forceinline__ void cell_tables(const double *a, int64_t g, double dt, double sign, double *A,
+                                            double *signedA, double *T)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    double M[NE], Tr[NE];
+#pragma unroll
+    for (int k = 0; k < NE; ++k) {
+        if (A) A[g * NE + k] = a[k];
+        const double s = sign < 0 ? -a[k] : a[k];
+        if (signedA) signedA[g * NE + k] = s;
+        M[k] = s * dt;
+    }
+    affine_expm<DIM>(M, Tr);
+#pragma unroll
+    for (int k = 0; k < NE; ++k) T[g * NE + k] = Tr[k];
+}
+
+// A = B.theta (theta row-major [N, d], B row-major [D_A, d], rows in (cell,
+// entry) order) fused with the per-cell expm.  A CTA takes 32 instances and
+// a strided share of the cells: the instances' theta staged once in shared
+// memory, transposed ([d][32]), then lane = instance and warp = cell, so a
+// warp's B loads are one broadcast address and its theta loads one
+// conflict-free row; each lane sums its dot products over j in order (the
+// same operations, hence the same A, as one thread per (instance, cell)).
+// Measured on 4096 theta x 100 cells (1D): the thread-per-(instance, cell)
+// form took 0.12 ms, its warps' B loads spanning 32 cache lines.
+constexpr int kThetaLanes = 32;
+template <int DIM>
+__global__ void __launch_bounds__(256) k_theta_to_trels(const double *B, const double *theta, int d, int nC, int N,
+                                                        int cell_groups, double dt, double sign, double *A,
+                                                        double *signedA, double *T)
+{
+    constexpr int NE = DIM * (DIM + 1);
+    extern __shared__ double s_thT[];  // [d][kThetaLanes]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int n0 = (blockIdx.x / cell_groups) * kThetaLanes, grp = blockIdx.x % cell_groups;
+    for (int e = threadIdx.x; e < kThetaLanes * d; e += blockDim.x) {
+        const int i = e / d, j = e - i * d;  // consecutive e: consecutive theta of one instance
+        s_thT[j * kThetaLanes + i] = (n0 + i < N) ? theta[(int64_t)(n0 + i) * d + j] : 0.0;
+    }
+    __syncthreads();
+    const int n = n0 + lane;
+    if (n >= N) return;  // no barrier follows
+    for (int c = grp * nw + warp; c < nC; c += cell_groups * nw) {
+        const double *Bc = B + (int64_t)c * NE * d;
+        double a[NE];
+#pragma unroll
+        for (int k = 0; k < NE; ++k) a[k] = 0.0;
+        for (int j = 0; j < d; ++j) {
+            const double tj = s_thT[j * kThetaLanes + lane];
+#pragma unroll
+            for (int k = 0; k < NE; ++k) a[k] = fma(__ldg(Bc + k * d + j), tj, a[k]);
+        }
+        cell_tables<DIM>(a, (int64_t)n * nC + c, dt, sign, A, signedA, T);
+    }
+}
+
+// The same with one thread per (instance, cell), for a d too large to stage
+// 32 instances' theta in shared memory.
+template <int DIM>
+__global__ void k_theta_to_trels_cell(const double *B, const double *theta, int d, int nC, int N,
+                                      double dt, double sign, double *A, double *signedA, double *T)
 {
     constexpr int NE = DIM * (DIM + 1);
     const int64_t total = (int64_t)N * nC;
@@ -393,7 +452,7 @@ __global__ void k_theta_to_trels(const double *B, const double *theta, int d, in
         const int n = (int)(g / nC), c = (int)(g - (int64_t)n * nC);
         const double *th = theta + (int64_t)n * d;
         const double *Bc = B + (int64_t)c * NE * d;
-        double a[NE], M[NE], Tr[NE];
+        double a[NE];
 #pragma unroll
         for (int k = 0; k < NE; ++k) a[k] = 0.0;
         for (int j = 0; j < d; ++j) {
@@ -401,16 +460,7 @@ __global__ void k_theta_to_trels(const double *B, const double *theta, int d, in
 #pragma unroll
             for (int k = 0; k < NE; ++k) a[k] = fma(Bc[k * d + j], tj, a[k]);
         }
-#pragma unroll
-        for (int k = 0; k < NE; ++k) {
-            if (A) A[g * NE + k] = a[k];
-            double s = sign < 0 ? -a[k] : a[k];
-            if (signedA) signedA[g * NE + k] = s;
-            M[k] = s * dt;
-        }
-        affine_expm<DIM>(M, Tr);
-#pragma unroll
-        for (int k = 0; k < NE; ++k) T[g * NE + k] = Tr[k];
+        cell_tables<DIM>(a, g, dt, sign, A, signedA, T);
     }
 }
 
@@ -589,15 +639,37 @@ cudaError_t launch_expm(int dim, const double *A, double *signedA, double *T, in
     return cudaGetLastError();
 }
 
+template <int DIM>
+static cudaError_t launch_theta_to_trels_t(const double *B, const double *theta, int d, int nC, int N, double dt,
+                                           double sign, double *A, double *signedA, double *T, cudaStream_t s)
+{
+    if (N <= 0 || nC <= 0) return cudaGetLastError();
+    const size_t smem = (size_t)kThetaLanes * d * sizeof(double);
+    if (smem <= 100 * 1024) {
+        if (smem > kSmemOptInAbove) {
+            cudaError_t e = cudaFuncSetAttribute(k_theta_to_trels<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        // about four CTAs per SM: the instance blocks times a split of the cells
+        const int blocks = (N + kThetaLanes - 1) / kThetaLanes;
+        const int max_groups = (nC + 7) / 8;  // 8 warps per CTA
+        const int want = (4 * num_sms() + blocks - 1) / blocks;
+        const int groups = std::max(1, std::min(want, max_groups));
+        k_theta_to_trels<DIM><<<blocks * groups, 256, smem, s>>>(B, theta, d, nC, N, groups, dt, sign, A, signedA, T);
+    } else {
+        const int g = grid_for((int64_t)N * nC, 128);
+        k_theta_to_trels_cell<DIM><<<g, 128, 0, s>>>(B, theta, d, nC, N, dt, sign, A, signedA, T);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_theta_to_trels(int dim, const double *B, const double *theta, int d, int nC, int N, double dt,
                                   double sign, double *A, double *signedA, double *T, cudaStream_t s)
 {
-    int64_t total = (int64_t)N * nC;
-    int g = grid_for(total, 128);
-    if (dim == 1) k_theta_to_trels<1><<<g, 128, 0, s>>>(B, theta, d, nC, N, dt, sign, A, signedA, T);
-    else if (dim == 2) k_theta_to_trels<2><<<g, 128, 0, s>>>(B, theta, d, nC, N, dt, sign, A, signedA, T);
-    else k_theta_to_trels<3><<<g, 128, 0, s>>>(B, theta, d, nC, N, dt, sign, A, signedA, T);
-    return cudaGetLastError();
+    if (dim == 1) return launch_theta_to_trels_t<1>(B, theta, d, nC, N, dt, sign, A, signedA, T, s);
+    if (dim == 2) return launch_theta_to_trels_t<2>(B, theta, d, nC, N, dt, sign, A, signedA, T, s);
+    return launch_theta_to_trels_t<3>(B, theta, d, nC, N, dt, sign, A, signedA, T, s);
 }
 
 }  // namespace cpab
