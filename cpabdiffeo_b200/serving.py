@@ -129,7 +129,9 @@ class CpabServer:
     the mix at 200 req/s, transform p99 39 ms against 200 ms with 8 jobs of
     25 % (which can occupy every SM), at the price of slower registrations;
     batches and the in-flight depth of 2^21 points bound the host work of one
-    iteration (measured transform p99 17-21 ms against 40-300 ms at 2^22).
+    iteration (measured transform p99 17-21 ms against 40-300 ms at 2^22;
+    with the lanes and reserve() below, 9.5-12 ms).  max_batch_requests:
+    requests per batch (the lanes' per-request buffers are sized for it).
     copy_threads: host threads that pack inputs into and unpack results out
     of the pinned buffers (numpy copies release the GIL); 0: min(8, cores)."""
 
